@@ -1,0 +1,165 @@
+"""TEST INFRASTRUCTURE ONLY -- ctypes access to the CPU oracle.
+
+Imported by tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline
+legs as the checker of the CUDA path.  The product never imports it.
+
+``liboracle.so`` is this directory's own C/C++ restatement of the reference
+algorithms.  ``_ref/`` holds the reference's own code compiled here (when its
+sources were available at build time); ``ref_available()`` says whether it is.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+_LIB = None
+_REF_SEEDED = None
+_REF_CERT = None
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_i64p = C.POINTER(C.c_int64)
+_cpp = C.POINTER(C.c_char_p)
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(t) if a is not None else None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = HERE / "liboracle.so"
+        if not path.exists():
+            raise RuntimeError(f"{path} missing: run `make -C oracle`")
+        L = C.CDLL(str(path))
+        L.sqo_pair.restype = C.c_double
+        L.sqo_pair.argtypes = [_dp, _dp, _dp]
+        L.sqo_pair_cached.restype = C.c_double
+        L.sqo_pair_cached.argtypes = [_dp, _dp, C.c_double, C.c_double, C.c_double, C.c_double, _dp, C.c_int]
+        L.sqo_boundary.restype = C.c_double
+        L.sqo_boundary.argtypes = [_dp, C.c_double, _dp]
+        L.sqo_total.restype = C.c_double
+        L.sqo_total.argtypes = [C.c_int, C.c_double, _dp, _dp, _i64p]
+        L.sqo_total_batch.restype = C.c_int
+        L.sqo_total_batch.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp, _i64p, C.c_int]
+        L.sqo_certified_side.restype = C.c_double
+        L.sqo_certified_side.argtypes = [C.c_int, _dp, _dp, _dp]
+        L.sqo_certify.restype = C.c_int
+        L.sqo_certify.argtypes = [C.c_int, C.c_int, _ip, _cpp, _cpp, _cpp, C.c_char_p, C.c_int,
+                                  C.c_char_p, C.c_int, _dp]
+        L.sqo_roundtrip.restype = None
+        L.sqo_roundtrip.argtypes = [C.c_char_p, C.c_char_p, C.c_int]
+        _LIB = L
+    return _LIB
+
+
+def ref_available() -> bool:
+    return (HERE / "_ref" / "libref_seeded.so").exists() and (HERE / "_ref" / "libref_certifier.so").exists()
+
+
+def ref_seeded():
+    global _REF_SEEDED
+    if _REF_SEEDED is None:
+        L = C.CDLL(str(HERE / "_ref" / "libref_seeded.so"))
+        L.ref_pair.restype = C.c_double
+        L.ref_pair.argtypes = [_dp, _dp, _dp]
+        L.ref_pair_smooth.restype = C.c_double
+        L.ref_pair_smooth.argtypes = [_dp, _dp, _dp]
+        L.ref_boundary.restype = C.c_double
+        L.ref_boundary.argtypes = [_dp, C.c_double, _dp]
+        L.ref_total_batch.restype = C.c_int
+        L.ref_total_batch.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp, C.c_int]
+        _REF_SEEDED = L
+    return _REF_SEEDED
+
+
+def ref_certifier():
+    global _REF_CERT
+    if _REF_CERT is None:
+        L = C.CDLL(str(HERE / "_ref" / "libref_certifier.so"))
+        L.ref_evaluate.restype = C.c_int
+        L.ref_evaluate.argtypes = [C.c_int, C.c_int, _ip, _cpp, _cpp, _cpp, C.c_char_p, C.c_int,
+                                   C.c_char_p, C.c_int, _dp]
+        L.ref_roundtrip.restype = None
+        L.ref_roundtrip.argtypes = [C.c_char_p, C.c_char_p, C.c_int]
+        _REF_CERT = L
+    return _REF_CERT
+
+
+# ---------------------------------------------------------------- energies
+def pair(p, q, grad=False):
+    p = np.ascontiguousarray(p, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    g = np.zeros(3) if grad else None
+    e = lib().sqo_pair(_ptr(p, _dp), _ptr(q, _dp), _ptr(g, _dp))
+    return (e, g) if grad else e
+
+
+def total_batch(xya, L, grad=True, threads=None):
+    """FP64 all-pairs energy (+ gradient, + candidate-pair counts) of a batch.
+
+    xya: (configs, n, 3) float64; L: (configs,).  Returns (energy, grad, cand)."""
+    xya = np.ascontiguousarray(xya, dtype=np.float64)
+    configs, n, _ = xya.shape
+    L = np.ascontiguousarray(np.broadcast_to(np.asarray(L, dtype=np.float64), (configs,)))
+    e = np.zeros(configs)
+    g = np.zeros_like(xya) if grad else None
+    cand = np.zeros(configs, dtype=np.int64)
+    threads = threads or os.cpu_count() or 1
+    lib().sqo_total_batch(configs, n, _ptr(xya, _dp), _ptr(L, _dp), _ptr(e, _dp), _ptr(g, _dp),
+                          _ptr(cand, _i64p), threads)
+    return e, g, cand
+
+
+def ref_total_batch(xya, L, grad=True, threads=None):
+    """The reference's own pair()/boundary() all-pairs energy (+ gradient)."""
+    xya = np.ascontiguousarray(xya, dtype=np.float64)
+    configs, n, _ = xya.shape
+    L = np.ascontiguousarray(np.broadcast_to(np.asarray(L, dtype=np.float64), (configs,)))
+    e = np.zeros(configs)
+    g = np.zeros_like(xya) if grad else None
+    threads = threads or os.cpu_count() or 1
+    used = ref_seeded().ref_total_batch(configs, n, _ptr(xya, _dp), _ptr(L, _dp), _ptr(e, _dp),
+                                        _ptr(g, _dp), threads)
+    return e, g, used
+
+
+def certified_side(xya):
+    xya = np.ascontiguousarray(xya, dtype=np.float64)
+    n = xya.shape[0]
+    best = np.zeros_like(xya)
+    lam = C.c_double(0)
+    L = lib().sqo_certified_side(n, _ptr(xya, _dp), _ptr(best, _dp), C.byref(lam))
+    return L, lam.value, best
+
+
+# ---------------------------------------------------------------- certifier
+def _rows_to_c(rows):
+    sid = np.array([int(r["square_id"]) for r in rows], dtype=np.int32)
+    enc = [[str(r[k]).encode() for r in rows] for k in ("x", "y", "angle")]
+    arrs = [(C.c_char_p * max(1, len(rows)))(*e) for e in enc]
+    return sid, arrs
+
+
+def certify(n, rows, which="oracle"):
+    """(ok, L_or_None, reason, score) for one packing, by the oracle
+    restatement (which="oracle") or the compiled reference ("ref")."""
+    sid, (xs, ys, as_) = _rows_to_c(rows)
+    Lbuf = C.create_string_buffer(128)
+    rbuf = C.create_string_buffer(256)
+    sc = C.c_double(0)
+    fn = lib().sqo_certify if which == "oracle" else ref_certifier().ref_evaluate
+    ok = fn(n, len(rows), _ptr(sid, _ip), xs, ys, as_, Lbuf, 128, rbuf, 256, C.byref(sc))
+    return bool(ok), (Lbuf.value.decode() if ok else None), rbuf.value.decode(), sc.value
+
+
+def roundtrip(s, which="oracle"):
+    out = C.create_string_buffer(64)
+    fn = lib().sqo_roundtrip if which == "oracle" else ref_certifier().ref_roundtrip
+    fn(str(s).encode(), out, 64)
+    return out.value.decode()

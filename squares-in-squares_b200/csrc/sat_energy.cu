@@ -1,0 +1,287 @@
+// FP32 cell-list SAT overlap + wall energy and gradient of many independent
+// configurations: one CTA per configuration.
+//
+// Per CTA (all in shared memory):
+//   1. load the n squares (coalesced 12-byte records), cos/sin, cell id on a
+//      G x G grid of cells with side >= sqrt(2.000001) (so every interacting
+//      pair sits in the same or adjacent cells), per-cell counts;
+//   2. exclusive scan of the counts, counting-sort scatter, then each cell's
+//      few entries ordered by square index (deterministic pair order);
+//   3. every square visits its own cell (later entries) and the four
+//      "forward" cells (E, NE, N, SE) -- each unordered pair exactly once --
+//      and accumulates the pair energy, both squares' gradients (shared
+//      float atomics for the partner) and its wall term;
+//   4. warp-shuffle + shared reduction of the energy and candidate count,
+//      coalesced store of the gradient.
+// Reference: total_cached (seeded.cu:148-162) is the all-pairs O(n^2) form
+// of the same energy; the legacy FP32 path's 16x16 cell grid of width 2
+// (packing.cu:22-47) is the reference's own cell-list idea.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "common.cuh"
+#include "sat_pair.cuh"
+
+namespace sqs {
+
+constexpr int kSatMaxN = 1024;
+constexpr float kCellMin = 1.41422f;  // > sqrt(2.000001) = 1.4142139
+
+__host__ __device__ inline int sat_grid_cap(int n) {
+    // Cell grid side cap: about sqrt(2n) cells per side, at most 45 (L = 64).
+    int g = (int)sqrtf(2.0f * (float)n);
+    return g < 1 ? 1 : (g > 45 ? 45 : g);
+}
+
+__host__ __device__ inline size_t sat_smem_bytes(int n) {
+    const int G = sat_grid_cap(n);
+    size_t b = 0;
+    b += (size_t)n * 16;                  // stash (x, y, c, s), reused as gradient accumulators
+    b += (size_t)n * 16;                  // cell-sorted (x, y, c, s)
+    b += (size_t)n * 4;                   // sorted -> original index (short) + cell (short)
+    b += (size_t)n * 4;                   // original -> (cell, rank) (short, short)
+    b += (size_t)(G * G + 1) * 4;         // cell counts / starts
+    b += 64;                              // reduction scratch
+    return (b + 15) & ~(size_t)15;
+}
+
+template <int T>
+__global__ void __launch_bounds__(T) sat_energy_kernel(int n, const float* __restrict__ xya,
+                                                        const float* __restrict__ side,
+                                                        float* __restrict__ energy,
+                                                        float* __restrict__ grad,
+                                                        uint32_t* __restrict__ cand) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int cfg = blockIdx.x;
+    const int tid = threadIdx.x;
+    const int Gcap = sat_grid_cap(n);
+    float4* stash = reinterpret_cast<float4*>(smem);
+    float4* sorted = stash + n;
+    short2* sorted_meta = reinterpret_cast<short2*>(sorted + n);   // (orig, cell)
+    short2* orig_meta = sorted_meta + n;                           // (cell, rank)
+    int* cells = reinterpret_cast<int*>(orig_meta + n);            // G*G + 1
+    float* red = reinterpret_cast<float*>(cells + Gcap * Gcap + 1);
+    float* gacc = reinterpret_cast<float*>(stash);                 // 3n floats, after phase 2
+
+    const float L = side[cfg];
+    int G = (int)(L / kCellMin);
+    G = G < 1 ? 1 : (G > Gcap ? Gcap : G);
+    const float inv_cell = (float)G / L;
+    const int ncell = G * G;
+
+    for (int c = tid; c <= ncell; c += T) cells[c] = 0;
+    __syncthreads();
+
+    // 1. load, trig, cell binning
+    const float* src = xya + (size_t)cfg * 3 * n;
+    for (int i = tid; i < n; i += T) {
+        const float x = src[3 * i], y = src[3 * i + 1], a = src[3 * i + 2];
+        float s, c;
+        sincosf(a, &s, &c);
+        int cx = (int)floorf(x * inv_cell), cy = (int)floorf(y * inv_cell);
+        cx = cx < 0 ? 0 : (cx >= G ? G - 1 : cx);
+        cy = cy < 0 ? 0 : (cy >= G ? G - 1 : cy);
+        const int cell = cy * G + cx;
+        const int rank = atomicAdd(&cells[cell], 1);
+        stash[i] = make_float4(x, y, c, s);
+        orig_meta[i] = make_short2((short)cell, (short)rank);
+    }
+    __syncthreads();
+
+    // 2. exclusive scan over ncell counts (single warp; ncell <= 2025)
+    if (tid < 32) {
+        const int per = (ncell + 31) / 32;
+        const int lo = tid * per, hi = min(lo + per, ncell);
+        int sum = 0;
+        for (int c = lo; c < hi; ++c) sum += cells[c];
+        int incl = sum;
+        for (int o = 1; o < 32; o <<= 1) {
+            int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (tid >= o) incl += v;
+        }
+        int run = incl - sum;
+        for (int c = lo; c < hi; ++c) {
+            int k = cells[c];
+            cells[c] = run;
+            run += k;
+        }
+        if (tid == 31) cells[ncell] = incl;
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += T) {
+        const short2 m = orig_meta[i];
+        const int pos = cells[m.x] + m.y;
+        sorted[pos] = stash[i];
+        sorted_meta[pos] = make_short2((short)i, m.x);
+    }
+    __syncthreads();
+    // order each cell's entries by original index (cells hold a few squares)
+    for (int c = tid; c < ncell; c += T) {
+        const int a = cells[c], b = cells[c + 1];
+        for (int u = a + 1; u < b; ++u) {
+            const float4 kv = sorted[u];
+            const short2 km = sorted_meta[u];
+            int w = u - 1;
+            while (w >= a && sorted_meta[w].x > km.x) {
+                sorted[w + 1] = sorted[w];
+                sorted_meta[w + 1] = sorted_meta[w];
+                --w;
+            }
+            sorted[w + 1] = kv;
+            sorted_meta[w + 1] = km;
+        }
+    }
+    for (int k = tid; k < 3 * n; k += T) gacc[k] = 0.f;
+    __syncthreads();
+
+    // 3. pairs over the half stencil + walls
+    float e_loc = 0.f;
+    uint32_t cand_loc = 0;
+    for (int p = tid; p < n; p += T) {
+        const float4 P = sorted[p];
+        const short2 pm = sorted_meta[p];
+        const int cell = pm.y, cx = cell % G, cy = cell / G;
+        float gx = 0.f, gy = 0.f, ga = 0.f;
+        e_loc += wall_energy_grad(P.x, P.y, P.z, P.w, L, gx, gy, ga);
+#pragma unroll 1
+        for (int k = 0; k < 5; ++k) {
+            int qa, qb;
+            if (k == 0) {
+                qa = p + 1;
+                qb = cells[cell + 1];
+            } else {
+                const int ox = (k == 1 || k == 2 || k == 4) ? 1 : 0;   // E, NE, SE
+                const int oy = (k == 2) ? 1 : (k == 3 ? 1 : (k == 4 ? -1 : 0));
+                const int nx = cx + ox, ny = cy + oy;
+                if (nx >= G || ny < 0 || ny >= G) continue;
+                const int nc = ny * G + nx;
+                qa = cells[nc];
+                qb = cells[nc + 1];
+            }
+            for (int q = qa; q < qb; ++q) {
+                const float4 Q = sorted[q];
+                const float dx = Q.x - P.x, dy = Q.y - P.y;
+                const float d2 = dx * dx + dy * dy;
+                if (d2 >= kPairCut2) continue;
+                cand_loc += d2 < 2.0f;
+                PairGrad g;
+                if (sat_pair_grad(dx, dy, P.z, P.w, Q.z, Q.w, g)) {
+                    e_loc += g.e;
+                    gx += g.px;
+                    gy += g.py;
+                    ga += g.pa;
+                    const int j = sorted_meta[q].x;
+                    atomicAdd(&gacc[3 * j], g.qx);
+                    atomicAdd(&gacc[3 * j + 1], g.qy);
+                    atomicAdd(&gacc[3 * j + 2], g.qa);
+                }
+            }
+        }
+        const int i = pm.x;
+        atomicAdd(&gacc[3 * i], gx);
+        atomicAdd(&gacc[3 * i + 1], gy);
+        atomicAdd(&gacc[3 * i + 2], ga);
+    }
+
+    // 4. reductions and stores
+    for (int o = 16; o > 0; o >>= 1) {
+        e_loc += __shfl_xor_sync(0xffffffffu, e_loc, o);
+        cand_loc += __shfl_xor_sync(0xffffffffu, cand_loc, o);
+    }
+    constexpr int W = T / 32;
+    if ((tid & 31) == 0) {
+        red[tid >> 5] = e_loc;
+        reinterpret_cast<uint32_t*>(red)[W + (tid >> 5)] = cand_loc;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        float e = 0.f;
+        uint32_t cc = 0;
+        for (int w = 0; w < W; ++w) {
+            e += red[w];
+            cc += reinterpret_cast<uint32_t*>(red)[W + w];
+        }
+        energy[cfg] = e;
+        if (cand) cand[cfg] = cc;
+    }
+    if (grad) {
+        float* dst = grad + (size_t)cfg * 3 * n;
+        for (int k = tid; k < 3 * n; k += T) dst[k] = gacc[k];
+    }
+}
+
+template <int T>
+static int launch(sqs_ctx* ctx, int configs, int n, const float* xya, const float* side,
+                  float* energy, float* grad, uint32_t* cand) {
+    const size_t smem = sat_smem_bytes(n);
+    static bool attr_set[64] = {false};
+    const int dev = ctx->device & 63;
+    if (!attr_set[dev]) {
+        SQS_CUDA(cudaFuncSetAttribute(sat_energy_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      96 * 1024));
+        attr_set[dev] = true;
+    }
+    sat_energy_kernel<T><<<configs, T, smem, ctx->stream>>>(n, xya, side, energy, grad, cand);
+    SQS_CUDA(cudaGetLastError());
+    ctx->launches += 1;
+    return SQS_OK;
+}
+
+int sat_energy_launch(sqs_ctx* ctx, int configs, int n, const float* xya, const float* side,
+                      float* energy, float* grad, uint32_t* cand, int threads) {
+    SQS_REQUIRE(configs >= 0 && configs <= (1 << 30), "configs %d out of range", configs);
+    SQS_REQUIRE(n >= 1 && n <= kSatMaxN, "n %d out of 1..%d", n, kSatMaxN);
+    SQS_REQUIRE(xya && side && energy, "null device pointer");
+    if (configs == 0) return SQS_OK;
+    if (threads == 0) threads = n <= 256 ? 64 : 128;
+    switch (threads) {
+        case 32: return launch<32>(ctx, configs, n, xya, side, energy, grad, cand);
+        case 64: return launch<64>(ctx, configs, n, xya, side, energy, grad, cand);
+        case 128: return launch<128>(ctx, configs, n, xya, side, energy, grad, cand);
+        case 256: return launch<256>(ctx, configs, n, xya, side, energy, grad, cand);
+        default: break;
+    }
+    SQS_REQUIRE(false, "threads %d not in {32, 64, 128, 256}", threads);
+}
+
+}  // namespace sqs
+
+extern "C" int sqs_sat_energy(sqs_ctx* ctx, int configs, int n, const float* xya, const float* side,
+                              float* energy, float* grad, uint32_t* cand, int threads) {
+    if (int r = sqs::enter(ctx)) return r;
+    return sqs::sat_energy_launch(ctx, configs, n, xya, side, energy, grad, cand, threads);
+}
+
+extern "C" int sqs_sat_energy_host(sqs_ctx* ctx, int configs, int n, const float* xya,
+                                   const float* side, float* energy, float* grad, uint32_t* cand) {
+    if (int r = sqs::enter(ctx)) return r;
+    SQS_REQUIRE(configs >= 0 && n >= 1 && n <= sqs::kSatMaxN, "configs/n out of range");
+    SQS_REQUIRE(xya && side && energy, "null host pointer");
+    if (configs == 0) return SQS_OK;
+    const size_t sb = (size_t)configs * n * 3 * sizeof(float);
+    if (int r = ctx->d_in.reserve(sb)) return r;
+    if (int r = ctx->d_side.reserve((size_t)configs * sizeof(float))) return r;
+    if (int r = ctx->d_out.reserve((size_t)configs * sizeof(float))) return r;
+    if (grad)
+        if (int r = ctx->d_grad.reserve(sb)) return r;
+    if (cand)
+        if (int r = ctx->d_cand.reserve((size_t)configs * sizeof(uint32_t))) return r;
+    SQS_CUDA(cudaMemcpyAsync(ctx->d_in.p, xya, sb, cudaMemcpyHostToDevice, ctx->stream));
+    SQS_CUDA(cudaMemcpyAsync(ctx->d_side.p, side, (size_t)configs * sizeof(float),
+                             cudaMemcpyHostToDevice, ctx->stream));
+    int r = sqs::sat_energy_launch(ctx, configs, n, (const float*)ctx->d_in.p, (const float*)ctx->d_side.p,
+                                   (float*)ctx->d_out.p, grad ? (float*)ctx->d_grad.p : nullptr,
+                                   cand ? (uint32_t*)ctx->d_cand.p : nullptr, 0);
+    if (r) return r;
+    SQS_CUDA(cudaMemcpyAsync(energy, ctx->d_out.p, (size_t)configs * sizeof(float),
+                             cudaMemcpyDeviceToHost, ctx->stream));
+    if (grad)
+        SQS_CUDA(cudaMemcpyAsync(grad, ctx->d_grad.p, sb, cudaMemcpyDeviceToHost, ctx->stream));
+    if (cand)
+        SQS_CUDA(cudaMemcpyAsync(cand, ctx->d_cand.p, (size_t)configs * sizeof(uint32_t),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+    SQS_CUDA(cudaStreamSynchronize(ctx->stream));
+    return SQS_OK;
+}

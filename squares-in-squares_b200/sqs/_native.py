@@ -1,0 +1,187 @@
+"""ctypes binding of libsqs.so (the C ABI declared in include/sqs.h).
+
+There is no fallback: if the library is missing or no sm_100 device is
+visible, the calls raise.  No PyTorch is involved; arrays are numpy.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libsqs.so"
+
+_vp = C.c_void_p
+_fp = C.POINTER(C.c_float)
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_u32p = C.POINTER(C.c_uint32)
+_u64p = C.POINTER(C.c_uint64)
+_i64p = C.POINTER(C.c_int64)
+_cpp = C.POINTER(C.c_char_p)
+
+
+class SQSError(RuntimeError):
+    """A libsqs call returned a negative status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"libsqs error {code}: {message}")
+        self.code = code
+
+
+# name -> (restype, argtypes)
+SIGNATURES: dict[str, tuple] = {
+    "sqs_version": (C.c_char_p, []),
+    "sqs_last_error": (C.c_char_p, []),
+    "sqs_device_count": (C.c_int, []),
+    "sqs_ctx_create": (C.c_int, [C.c_int, C.POINTER(_vp)]),
+    "sqs_ctx_destroy": (C.c_int, [_vp]),
+    "sqs_ctx_device_info": (C.c_int, [_vp, C.c_char_p, C.c_int, _ip]),
+    "sqs_dev_alloc": (C.c_int, [_vp, C.c_size_t, C.POINTER(_vp)]),
+    "sqs_dev_free": (C.c_int, [_vp, _vp]),
+    "sqs_copy_h2d": (C.c_int, [_vp, _vp, _vp, C.c_size_t]),
+    "sqs_copy_d2h": (C.c_int, [_vp, _vp, _vp, C.c_size_t]),
+    "sqs_memset": (C.c_int, [_vp, _vp, C.c_int, C.c_size_t]),
+    "sqs_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(_vp)]),
+    "sqs_host_free": (C.c_int, [_vp]),
+    "sqs_sync": (C.c_int, [_vp]),
+    "sqs_event_record": (C.c_int, [_vp, C.c_int]),
+    "sqs_event_elapsed": (C.c_int, [_vp, C.c_int, C.c_int, _fp]),
+    "sqs_flush_l2": (C.c_int, [_vp]),
+    "sqs_launch_count": (C.c_int64, [_vp]),
+    "sqs_sat_energy": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_int]),
+    "sqs_sat_energy_host": (C.c_int, [_vp, C.c_int, C.c_int, _fp, _fp, _fp, _fp, _u32p]),
+}
+
+_LIB = None
+
+
+def lib():
+    """Load libsqs.so once (raises if it is missing)."""
+    global _LIB
+    if _LIB is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing; build it with "
+                               "`python squares-in-squares_b200/build.py`")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def check(rc: int) -> int:
+    if rc < 0:
+        raise SQSError(rc, lib().sqs_last_error().decode(errors="replace"))
+    return rc
+
+
+def ptr(a: np.ndarray | None, t=_vp):
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "arrays passed to libsqs must be C-contiguous"
+    return a.ctypes.data_as(t)
+
+
+class DeviceArray:
+    """A device buffer owned by a Context (numpy-like shape/dtype metadata)."""
+
+    def __init__(self, ctx: "Context", shape, dtype):
+        self.ctx = ctx
+        self.shape = tuple(int(s) for s in np.atleast_1d(shape))
+        self.dtype = np.dtype(dtype)
+        self.nbytes = int(np.prod(self.shape)) * self.dtype.itemsize
+        p = _vp()
+        check(lib().sqs_dev_alloc(ctx.handle, max(1, self.nbytes), C.byref(p)))
+        self.ptr = p.value
+
+    def upload(self, host: np.ndarray):
+        host = np.ascontiguousarray(host, dtype=self.dtype)
+        assert host.nbytes == self.nbytes
+        check(lib().sqs_copy_h2d(self.ctx.handle, self.ptr, host.ctypes.data, self.nbytes))
+        return self
+
+    def download(self, out: np.ndarray | None = None) -> np.ndarray:
+        out = np.empty(self.shape, self.dtype) if out is None else out
+        check(lib().sqs_copy_d2h(self.ctx.handle, out.ctypes.data, self.ptr, self.nbytes))
+        self.ctx.sync()
+        return out
+
+    def free(self):
+        if self.ptr:
+            check(lib().sqs_dev_free(self.ctx.handle, self.ptr))
+            self.ptr = None
+
+
+class PinnedArray:
+    """Page-locked host array (numpy view) for timed transfers."""
+
+    def __init__(self, shape, dtype):
+        self.dtype = np.dtype(dtype)
+        self.shape = tuple(int(s) for s in np.atleast_1d(shape))
+        nbytes = int(np.prod(self.shape)) * self.dtype.itemsize
+        p = _vp()
+        check(lib().sqs_host_alloc(max(1, nbytes), C.byref(p)))
+        self._p = p.value
+        buf = (C.c_char * max(1, nbytes)).from_address(self._p)
+        self.array = np.frombuffer(buf, dtype=self.dtype, count=int(np.prod(self.shape))).reshape(self.shape)
+
+    def free(self):
+        if self._p:
+            self.array = None
+            check(lib().sqs_host_free(self._p))
+            self._p = None
+
+
+class Context:
+    """One CUDA device + stream (sqs_ctx)."""
+
+    def __init__(self, device: int = 0):
+        h = _vp()
+        check(lib().sqs_ctx_create(device, C.byref(h)))
+        self.handle = h.value
+        self.device = device
+
+    def close(self):
+        if self.handle:
+            lib().sqs_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def info(self):
+        buf = C.create_string_buffer(256)
+        sm = C.c_int(0)
+        check(lib().sqs_ctx_device_info(self.handle, buf, 256, C.byref(sm)))
+        return buf.value.decode(), sm.value
+
+    def sync(self):
+        check(lib().sqs_sync(self.handle))
+
+    def record(self, slot: int):
+        check(lib().sqs_event_record(self.handle, slot))
+
+    def elapsed(self, a: int, b: int) -> float:
+        ms = C.c_float(0)
+        check(lib().sqs_event_elapsed(self.handle, a, b, C.byref(ms)))
+        return ms.value
+
+    def flush_l2(self):
+        check(lib().sqs_flush_l2(self.handle))
+
+    def launches(self) -> int:
+        return int(lib().sqs_launch_count(self.handle))
+
+    def alloc(self, shape, dtype) -> DeviceArray:
+        return DeviceArray(self, shape, dtype)
+
+
+def device_count() -> int:
+    return int(lib().sqs_device_count())
