@@ -2,15 +2,18 @@
 // configurations: one CTA per configuration.
 //
 // Per CTA (all in shared memory):
-//   1. load the n squares (coalesced 12-byte records), cos/sin, cell id on a
-//      G x G grid of cells with side >= sqrt(2.000001) (so every interacting
-//      pair sits in the same or adjacent cells), per-cell counts;
-//   2. exclusive scan of the counts, counting-sort scatter, then each cell's
-//      few entries ordered by square index (deterministic pair order);
-//   3. every square visits its own cell (later entries) and the four
-//      "forward" cells (E, NE, N, SE) -- each unordered pair exactly once --
-//      and accumulates the pair energy, both squares' gradients (shared
-//      float atomics for the partner) and its wall term;
+//   1. load the n squares (coalesced 12-byte records), cos/sin, wall term,
+//      cell id on a G x G grid of cells with side >= sqrt(2.000001) (so every
+//      interacting pair sits in the same or adjacent cells), per-cell counts;
+//   2. exclusive scan of the counts, counting-sort scatter, each cell's few
+//      entries ordered by square index (deterministic pair order);
+//   3. broad phase: every square scans two contiguous ranges of the
+//      cell-sorted array -- the rest of its own cell plus the east cell, and
+//      the three cells of the row above -- which visits each unordered
+//      neighbour pair exactly once.  Pairs inside the cut-off are appended
+//      to a per-warp queue (ballot + popc), and every time 32 are queued the
+//      whole warp evaluates them (narrow phase at full SIMT width), adding
+//      both squares' gradients with shared-memory atomics;
 //   4. warp-shuffle + shared reduction of the energy and candidate count,
 //      coalesced store of the gradient.
 // Reference: total_cached (seeded.cu:148-162) is the all-pairs O(n^2) form
@@ -28,6 +31,7 @@ namespace sqs {
 
 constexpr int kSatMaxN = 1024;
 constexpr float kCellMin = 1.41422f;  // > sqrt(2.000001) = 1.4142139
+constexpr int kQueue = 64;            // per-warp pair queue entries
 
 __host__ __device__ inline int sat_grid_cap(int n) {
     // Cell grid side cap: about sqrt(2n) cells per side, at most 45 (L = 64).
@@ -35,15 +39,17 @@ __host__ __device__ inline int sat_grid_cap(int n) {
     return g < 1 ? 1 : (g > 45 ? 45 : g);
 }
 
-__host__ __device__ inline size_t sat_smem_bytes(int n) {
+__host__ __device__ inline size_t sat_smem_bytes(int n, int threads) {
     const int G = sat_grid_cap(n);
     size_t b = 0;
-    b += (size_t)n * 16;                  // stash (x, y, c, s), reused as gradient accumulators
-    b += (size_t)n * 16;                  // cell-sorted (x, y, c, s)
-    b += (size_t)n * 4;                   // sorted -> original index (short) + cell (short)
-    b += (size_t)n * 4;                   // original -> (cell, rank) (short, short)
-    b += (size_t)(G * G + 1) * 4;         // cell counts / starts
-    b += 64;                              // reduction scratch
+    b += (size_t)n * 16;                      // stash (x, y, c, s) by original index
+    b += (size_t)n * 16;                      // cell-sorted (x, y, c, s)
+    b += (size_t)n * 12;                      // gradient accumulators by original index
+    b += (size_t)n * 4;                       // sorted -> (original index, cell)
+    b += (size_t)n * 4;                       // original -> (cell, rank)
+    b += (size_t)(G * G + 1) * 4;             // cell counts / starts
+    b += (size_t)(threads / 32) * kQueue * 4; // warp pair queues
+    b += 64;                                  // reduction scratch
     return (b + 15) & ~(size_t)15;
 }
 
@@ -54,16 +60,18 @@ __global__ void __launch_bounds__(T) sat_energy_kernel(int n, const float* __res
                                                         float* __restrict__ grad,
                                                         uint32_t* __restrict__ cand) {
     extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int W = T / 32;
     const int cfg = blockIdx.x;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int Gcap = sat_grid_cap(n);
     float4* stash = reinterpret_cast<float4*>(smem);
     float4* sorted = stash + n;
-    short2* sorted_meta = reinterpret_cast<short2*>(sorted + n);   // (orig, cell)
-    short2* orig_meta = sorted_meta + n;                           // (cell, rank)
-    int* cells = reinterpret_cast<int*>(orig_meta + n);            // G*G + 1
-    float* red = reinterpret_cast<float*>(cells + Gcap * Gcap + 1);
-    float* gacc = reinterpret_cast<float*>(stash);                 // 3n floats, after phase 2
+    float* gacc = reinterpret_cast<float*>(sorted + n);
+    short2* sorted_meta = reinterpret_cast<short2*>(gacc + 3 * n);  // (orig, cell)
+    short2* orig_meta = sorted_meta + n;                            // (cell, rank)
+    int* cells = reinterpret_cast<int*>(orig_meta + n);             // G*G + 1
+    uint32_t* queues = reinterpret_cast<uint32_t*>(cells + Gcap * Gcap + 1);
+    float* red = reinterpret_cast<float*>(queues + W * kQueue);
 
     const float L = side[cfg];
     int G = (int)(L / kCellMin);
@@ -74,12 +82,18 @@ __global__ void __launch_bounds__(T) sat_energy_kernel(int n, const float* __res
     for (int c = tid; c <= ncell; c += T) cells[c] = 0;
     __syncthreads();
 
-    // 1. load, trig, cell binning
+    // 1. load, trig, walls, cell binning
+    float e_loc = 0.f;
     const float* src = xya + (size_t)cfg * 3 * n;
     for (int i = tid; i < n; i += T) {
         const float x = src[3 * i], y = src[3 * i + 1], a = src[3 * i + 2];
         float s, c;
         sincosf(a, &s, &c);
+        float gx = 0.f, gy = 0.f, ga = 0.f;
+        e_loc += wall_energy_grad(x, y, c, s, L, gx, gy, ga);
+        gacc[3 * i] = gx;
+        gacc[3 * i + 1] = gy;
+        gacc[3 * i + 2] = ga;
         int cx = (int)floorf(x * inv_cell), cy = (int)floorf(y * inv_cell);
         cx = cx < 0 ? 0 : (cx >= G ? G - 1 : cx);
         cy = cy < 0 ? 0 : (cy >= G ? G - 1 : cy);
@@ -90,7 +104,7 @@ __global__ void __launch_bounds__(T) sat_energy_kernel(int n, const float* __res
     }
     __syncthreads();
 
-    // 2. exclusive scan over ncell counts (single warp; ncell <= 2025)
+    // 2. exclusive scan over ncell counts (one warp; ncell <= 2025)
     if (tid < 32) {
         const int per = (ncell + 31) / 32;
         const int lo = tid * per, hi = min(lo + per, ncell);
@@ -133,67 +147,84 @@ __global__ void __launch_bounds__(T) sat_energy_kernel(int n, const float* __res
             sorted_meta[w + 1] = km;
         }
     }
-    for (int k = tid; k < 3 * n; k += T) gacc[k] = 0.f;
     __syncthreads();
 
-    // 3. pairs over the half stencil + walls
-    float e_loc = 0.f;
+    // 3. broad phase into warp queues, narrow phase 32 pairs at a time
     uint32_t cand_loc = 0;
-    for (int p = tid; p < n; p += T) {
-        const float4 P = sorted[p];
-        const short2 pm = sorted_meta[p];
-        const int cell = pm.y, cx = cell % G, cy = cell / G;
-        float gx = 0.f, gy = 0.f, ga = 0.f;
-        e_loc += wall_energy_grad(P.x, P.y, P.z, P.w, L, gx, gy, ga);
-#pragma unroll 1
-        for (int k = 0; k < 5; ++k) {
-            int qa, qb;
-            if (k == 0) {
-                qa = p + 1;
-                qb = cells[cell + 1];
-            } else {
-                const int ox = (k == 1 || k == 2 || k == 4) ? 1 : 0;   // E, NE, SE
-                const int oy = (k == 2) ? 1 : (k == 3 ? 1 : (k == 4 ? -1 : 0));
-                const int nx = cx + ox, ny = cy + oy;
-                if (nx >= G || ny < 0 || ny >= G) continue;
-                const int nc = ny * G + nx;
-                qa = cells[nc];
-                qb = cells[nc + 1];
+    uint32_t* queue = queues + warp * kQueue;
+    int qn = 0;  // warp-uniform queue length
+    auto narrow = [&](uint32_t entry) {
+        const int p = (int)(entry & 0xffffu), q = (int)(entry >> 16);
+        const float4 P = sorted[p], Q = sorted[q];
+        PairGrad g;
+        if (sat_pair_grad(Q.x - P.x, Q.y - P.y, P.z, P.w, Q.z, Q.w, g)) {
+            e_loc += g.e;
+            const int i = sorted_meta[p].x, j = sorted_meta[q].x;
+            atomicAdd(&gacc[3 * i], g.px);
+            atomicAdd(&gacc[3 * i + 1], g.py);
+            atomicAdd(&gacc[3 * i + 2], g.pa);
+            atomicAdd(&gacc[3 * j], g.qx);
+            atomicAdd(&gacc[3 * j + 1], g.qy);
+            atomicAdd(&gacc[3 * j + 2], g.qa);
+        }
+    };
+    for (int base = warp * 32; base < n; base += T) {
+        const int p = base + lane;
+        int a1 = 0, len1 = 0, a2 = 0, len = 0;
+        float px = 0.f, py = 0.f;
+        if (p < n) {
+            const float4 P = sorted[p];
+            px = P.x;
+            py = P.y;
+            const int cell = sorted_meta[p].y, cy = cell / G, cx = cell - cy * G;
+            // own cell after p, then the east cell (same row, contiguous)
+            a1 = p + 1;
+            len1 = cells[cy * G + min(cx + 2, G)] - a1;
+            // the row above: cells cx-1 .. cx+1
+            int len2 = 0;
+            if (cy + 1 < G) {
+                a2 = cells[(cy + 1) * G + max(cx - 1, 0)];
+                len2 = cells[(cy + 1) * G + min(cx + 2, G)] - a2;
             }
-            for (int q = qa; q < qb; ++q) {
+            len = len1 + len2;
+        }
+        const int maxlen = __reduce_max_sync(0xffffffffu, len);
+        for (int t = 0; t < maxlen; ++t) {
+            bool pass = false;
+            int q = 0;
+            if (t < len) {
+                q = t < len1 ? a1 + t : a2 + (t - len1);
                 const float4 Q = sorted[q];
-                const float dx = Q.x - P.x, dy = Q.y - P.y;
+                const float dx = Q.x - px, dy = Q.y - py;
                 const float d2 = dx * dx + dy * dy;
-                if (d2 >= kPairCut2) continue;
+                pass = d2 < kPairCut2;
                 cand_loc += d2 < 2.0f;
-                PairGrad g;
-                if (sat_pair_grad(dx, dy, P.z, P.w, Q.z, Q.w, g)) {
-                    e_loc += g.e;
-                    gx += g.px;
-                    gy += g.py;
-                    ga += g.pa;
-                    const int j = sorted_meta[q].x;
-                    atomicAdd(&gacc[3 * j], g.qx);
-                    atomicAdd(&gacc[3 * j + 1], g.qy);
-                    atomicAdd(&gacc[3 * j + 2], g.qa);
-                }
+            }
+            const uint32_t m = __ballot_sync(0xffffffffu, pass);
+            if (pass) queue[qn + __popc(m & ((1u << lane) - 1u))] = (uint32_t)p | ((uint32_t)q << 16);
+            qn += __popc(m);
+            if (qn >= 32) {
+                __syncwarp();
+                narrow(queue[lane]);
+                __syncwarp();
+                if (lane < qn - 32) queue[lane] = queue[32 + lane];
+                __syncwarp();
+                qn -= 32;
             }
         }
-        const int i = pm.x;
-        atomicAdd(&gacc[3 * i], gx);
-        atomicAdd(&gacc[3 * i + 1], gy);
-        atomicAdd(&gacc[3 * i + 2], ga);
     }
+    __syncwarp();
+    if (lane < qn) narrow(queue[lane]);
+    __syncthreads();
 
     // 4. reductions and stores
     for (int o = 16; o > 0; o >>= 1) {
         e_loc += __shfl_xor_sync(0xffffffffu, e_loc, o);
         cand_loc += __shfl_xor_sync(0xffffffffu, cand_loc, o);
     }
-    constexpr int W = T / 32;
-    if ((tid & 31) == 0) {
-        red[tid >> 5] = e_loc;
-        reinterpret_cast<uint32_t*>(red)[W + (tid >> 5)] = cand_loc;
+    if (lane == 0) {
+        red[warp] = e_loc;
+        reinterpret_cast<uint32_t*>(red)[W + warp] = cand_loc;
     }
     __syncthreads();
     if (tid == 0) {
@@ -215,7 +246,7 @@ __global__ void __launch_bounds__(T) sat_energy_kernel(int n, const float* __res
 template <int T>
 static int launch(sqs_ctx* ctx, int configs, int n, const float* xya, const float* side,
                   float* energy, float* grad, uint32_t* cand) {
-    const size_t smem = sat_smem_bytes(n);
+    const size_t smem = sat_smem_bytes(n, T);
     static bool attr_set[64] = {false};
     const int dev = ctx->device & 63;
     if (!attr_set[dev]) {

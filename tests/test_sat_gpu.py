@@ -68,9 +68,12 @@ def test_cta_widths_agree(ctx, oracle, threads):
 
 def test_aligned_ties_follow_reference_gradient(ctx, oracle):
     # Axis-aligned overlapping grids: every overlapping pair has tied axes;
-    # the gradient must follow the reference's own-axis-first choice.
+    # the gradient must follow the reference's own-axis-first choice.  The
+    # pitches are dyadic so FP32 differences are exact and the ties are real
+    # ties in both precisions (with a pitch like 0.9, FP32 rounding of dx vs
+    # dy decides between two axes 1e-8 apart, a genuine kink of the energy).
     from sqs.workloads import grid_state
-    states = np.stack([grid_state(49, pitch=p) for p in (0.9, 0.95, 0.999, 1.0)])
+    states = np.stack([grid_state(49, pitch=p) for p in (0.75, 0.875, 0.9375, 1.0)])
     out, x32, s32 = _run(ctx, states, 6.5)
     _check(oracle, out, x32, s32)
 
