@@ -86,6 +86,31 @@ int sqs_sat_energy(sqs_ctx* ctx, int configs, int n, const float* xya, const flo
 int sqs_sat_energy_host(sqs_ctx* ctx, int configs, int n, const float* xya, const float* side,
                         float* energy, float* grad, uint32_t* cand);
 
+/* ---------------------------------------------------- interval certifier */
+#define SQS_CERT_ROUNDTRIP 1 /* re-read every literal through a double first */
+
+typedef struct sqs_verdict {
+    int32_t ok;        /* 1 accepted, 0 rejected                              */
+    int32_t n;
+    double score;      /* max(0, L/sqrt(n) - 1), or the grid penalty if rejected */
+    char L[80];        /* side to 50 decimals when accepted, else ""           */
+    char reason[112];  /* "ok" or the reference certifier's rejection reason    */
+} sqs_verdict;
+
+/* Certify `count` packings.  Packing p has n_of[p] expected squares and rows
+ * row_start[p] .. row_start[p+1]-1; row r has square id square_id[r] (NULL:
+ * the row's position within its packing) and three decimal literals x, y,
+ * angle (radians) at text[lit_off[3r+k] .. lit_off[3r+k+1]), k = 0, 1, 2.
+ * Every verdict, reason, score and 50-decimal side equals the reference
+ * certifier's evaluate_single_puzzle (certifier.cpp:738-912) on the same
+ * strings; SQS_CERT_ROUNDTRIP applies its --roundtrip literal transform
+ * (certifier.cpp:914-929, main :1002-1006) first.  Replaces the `certifier`
+ * process (certifier.cpp:933-1077) and the Python gate core.certify /
+ * core.evaluate (core.py:52-62) for whole batches. */
+int sqs_certify_batch(sqs_ctx* ctx, int count, const int32_t* n_of, const int64_t* row_start,
+                      const int32_t* square_id, const char* text, const int64_t* lit_off, int flags,
+                      sqs_verdict* out);
+
 #ifdef __cplusplus
 }
 #endif

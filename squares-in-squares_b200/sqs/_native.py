@@ -30,6 +30,12 @@ class SQSError(RuntimeError):
         self.code = code
 
 
+class Verdict(C.Structure):
+    """sqs_verdict (include/sqs.h)."""
+    _fields_ = [("ok", C.c_int32), ("n", C.c_int32), ("score", C.c_double),
+                ("L", C.c_char * 80), ("reason", C.c_char * 112)]
+
+
 # name -> (restype, argtypes)
 SIGNATURES: dict[str, tuple] = {
     "sqs_version": (C.c_char_p, []),
@@ -52,6 +58,7 @@ SIGNATURES: dict[str, tuple] = {
     "sqs_launch_count": (C.c_int64, [_vp]),
     "sqs_sat_energy": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_int]),
     "sqs_sat_energy_host": (C.c_int, [_vp, C.c_int, C.c_int, _fp, _fp, _fp, _fp, _u32p]),
+    "sqs_certify_batch": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, C.c_char_p, _vp, C.c_int, C.POINTER(Verdict)]),
 }
 
 _LIB = None
