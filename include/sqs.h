@@ -111,6 +111,52 @@ int sqs_certify_batch(sqs_ctx* ctx, int count, const int32_t* n_of, const int64_
                       const int32_t* square_id, const char* text, const int64_t* lit_off, int flags,
                       sqs_verdict* out);
 
+/* ------------------------------------------------ annealing + polish */
+/* One anneal-and-certify job: parallel tempering of n unit squares in a
+ * container that shrinks after every new best state.  The job's whole
+ * trajectory is a function of its inputs and `seed` alone (counter-based
+ * RNG), so it is the same alone or batched with other jobs. */
+typedef struct sqs_job {
+    int32_t n;               /* squares, 1..1000                                  */
+    int32_t replicas;        /* temperature rungs, 1..64                          */
+    int32_t sweeps;          /* sweep budget; one sweep = n proposals per replica */
+    int32_t exchange_every;  /* sweeps between replica-exchange rounds           */
+    int32_t polish_iters;    /* FP64 gradient-polish iterations on the best state */
+    int32_t flags;           /* reserved, 0                                       */
+    double L0;               /* initial container side                            */
+    double tmin, tmax;       /* geometric temperature ladder                      */
+    double sigma_xy;         /* proposal std-dev of a centre coordinate           */
+    double sigma_a;          /* proposal std-dev of the angle (radians)           */
+    double shrink;           /* relative shrink of the side after each improvement*/
+    uint64_t seed;
+    const double* xya;       /* initial state, n rows of (x, y, angle), host      */
+} sqs_job;
+
+typedef struct sqs_job_result {
+    int32_t status;          /* 0 ok; < 0 job error (see reason)                  */
+    int32_t certified;       /* the interval certifier accepted the packing      */
+    int32_t shrinks, improvements, sweeps_done, replicas;
+    double L_cert;           /* FP64 dilation-certified side of the best state    */
+    double L_polished;       /* the same after the gradient polish                */
+    double dilation;         /* centre dilation under which the packing certified*/
+    double score;            /* max(0, L/sqrt(n) - 1) of the certified side       */
+    int64_t proposals, accepted, exchange_attempts, exchange_accepts;
+    double device_ms;        /* device time of this call (all jobs)               */
+    char L[80];              /* certified side, 50 decimals ("" if none)          */
+    char reason[112];
+} sqs_job_result;
+
+/* Anneal, polish and certify `njobs` jobs in persistent batched launches
+ * (one thread-block cluster per job, one warp per replica) and return each
+ * job's best packing in xya_out[j] (caller buffer of n*3 doubles; centres
+ * after the certifying dilation, angles in [0, pi/2)).  Replaces the
+ * reference's `packing` / `seeded` search programs (packing.cu:768-868,
+ * seeded.cu:831-983) and its certified_candidate dilation ladder
+ * (demo.py:25-40).  slice_sweeps > 0 runs the jobs in slices of that many
+ * sweeps (state kept resident in HBM between slices); 0 = one slice. */
+int sqs_anneal_batch(sqs_ctx* ctx, const sqs_job* jobs, int njobs, int slice_sweeps, double* const* xya_out,
+                     sqs_job_result* out);
+
 #ifdef __cplusplus
 }
 #endif

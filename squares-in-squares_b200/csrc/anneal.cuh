@@ -1,0 +1,60 @@
+// Device-side job records of the batched parallel-tempering annealer, shared
+// by the anneal and polish kernels and the host runtime (anneal_host.cu).
+#pragma once
+#include <cstdint>
+
+namespace sqs {
+namespace ann {
+
+constexpr int kMaxR = 64;            // replicas (temperature rungs) per job
+constexpr int kMaxRl = 32;           // replicas (warps) per CTA
+constexpr int kCellK = 12;           // slot capacity of one cell
+constexpr float kCellSide = 1.59f;   // >= sqrt(2.000001) + largest centre move (0.12 * sqrt 2)
+constexpr float kMaxStep = 0.12f;    // clamp of each proposal coordinate
+constexpr int kMaxN = 1000;
+
+// Per job, read-only while a slice runs.
+struct JobDev {
+    int32_t n, R, cs, Rl;             // squares, replicas, CTAs per job (cluster size), replicas per CTA
+    int32_t sweeps_total, exchange_every;
+    int32_t Gmax, polish_iters;       // cell grid side for the initial container; polish iterations
+    float sigma_xy, sigma_a, tmin, tmax;
+    float shrink, L0, pad0, pad1;
+    uint64_t seed;
+    int64_t pos_off;                  // float4 index of replica 0, square 0
+    int64_t best_off;                 // double index of the best state (n x 3)
+    int64_t scr_off;                  // float4 index of the job's quench scratch (2n)
+    int32_t quench_iters, pad2;       // gradient steps of the coldest replica per checkpoint
+};
+
+// Per job, advanced by every slice.
+struct JobMut {
+    float L;                          // current container side
+    int32_t sweep;                    // sweeps completed
+    int32_t xround;                   // exchange rounds completed
+    int32_t status;                   // 0 running, 1 finished, < 0 error
+    int32_t shrinks, improvements, pad0, pad1;
+    double best_L;                    // best FP64 dilation-certified side (1e30: none yet)
+    uint64_t proposals, accepted, xatt, xacc;
+    int32_t perm[kMaxR];              // rung (temperature index) of each replica
+    int64_t E[kMaxR];                 // energy of each replica, fixed point (kEScale units)
+};
+
+// Energies are accumulated as integers in units of 2^-40: every pair and
+// wall term is rounded once, so sums are exact and independent of the order
+// in which neighbours are visited (cell lists are rebuilt with atomics), and
+// the running energy of a replica never drifts from its full recomputation.
+constexpr float kEScale = 1099511627776.0f;  // 2^40
+
+enum : int32_t { kRunning = 0, kFinished = 1, kErrCells = -2, kErrInput = -3 };
+
+// Shared-memory bytes one replica needs: (x, y, cos, sin), angle, cell counts, cell slots.
+__host__ __device__ inline int64_t replica_smem_bytes(int n, int Gmax) {
+    int64_t b = (int64_t)n * 16 + (int64_t)n * 4;
+    b += ((int64_t)Gmax * Gmax + 3) & ~3LL;
+    b += (int64_t)Gmax * Gmax * kCellK * 2;
+    return (b + 15) & ~15LL;
+}
+
+}  // namespace ann
+}  // namespace sqs

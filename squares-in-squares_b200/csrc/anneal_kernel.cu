@@ -1,0 +1,645 @@
+// Batched parallel-tempering simulated annealing of unit squares in a
+// shrinking square container: one thread-block cluster per job, one warp per
+// replica, every replica's squares and cell list in shared memory.
+//
+// Reference semantics it re-designs (cuda/seeded.cu): the energy model
+// (pair_cached/boundary/total_cached :41-162), single-square Metropolis
+// moves (:501-546), replica exchange within a temperature ladder
+// (swap_replicas :791-817), the FP64 dilation-certified side of a candidate
+// best state (device_certified_side :175-226) and the host's shrink of the
+// container after every improvement (:919-938).  What is new:
+//   * FP32 moves and energies, with dE of a single-square move taken over the
+//     3x3 cell neighbourhood (O(1) per proposal instead of O(n));
+//   * lanes of the replica's warp split the neighbour candidates, a butterfly
+//     reduction leaves the same dE on every lane, so every lane takes the same
+//     Metropolis decision without a broadcast;
+//   * counter-based Philox keyed by (job seed, replica, proposal index): a
+//     job's trajectory does not depend on the batch, slot or CTA running it;
+//   * replica exchange swaps rungs (temperature indices), not states, and the
+//     whole ladder (up to 64 rungs) may span a cluster of CTAs, exchanged over
+//     distributed shared memory;
+//   * the shrink decision is taken on the device at every exchange point
+//     (no per-epoch device-to-host round trip).
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "anneal.cuh"
+#include "common.cuh"
+#include "philox.cuh"
+#include "sat_pair.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace sqs {
+namespace ann {
+
+constexpr float kHalfPiF = 1.57079632679489662f;
+
+struct Rep {  // one replica's shared-memory view
+    float4* sq;        // (x, y, cos a, sin a)
+    float* ang;        // a in [0, pi/2)
+    uint8_t* cnt;      // squares per cell
+    uint16_t* slot;    // cell c: slot[c * kCellK + k]
+};
+
+__device__ __forceinline__ Rep rep_view(unsigned char* base, int n, int Gmax) {
+    Rep r;
+    r.sq = reinterpret_cast<float4*>(base);
+    r.ang = reinterpret_cast<float*>(r.sq + n);
+    r.cnt = reinterpret_cast<uint8_t*>(r.ang + n);
+    r.slot = reinterpret_cast<uint16_t*>(r.cnt + ((Gmax * Gmax + 3) & ~3));
+    return r;
+}
+
+struct Grid {
+    int G;
+    float inv;  // G / L
+    __device__ __forceinline__ int cx(float x) const {
+        int c = (int)floorf(x * inv);
+        return c < 0 ? 0 : (c >= G ? G - 1 : c);
+    }
+};
+
+__device__ __forceinline__ Grid make_grid(float L, int Gmax) {
+    Grid g;
+    int G = (int)(L / kCellSide);
+    g.G = G < 1 ? 1 : (G > Gmax ? Gmax : G);
+    g.inv = (float)g.G / L;
+    return g;
+}
+
+__device__ __forceinline__ float wall_e(float x, float y, float c, float s, float L) {
+    return wall_energy(x, y, c, s, L);
+}
+
+// Build the cell list of one replica (warp).  Returns false on overflow (a
+// cell asked for more than kCellK slots); the list is then incomplete but
+// every count is clamped to kCellK and every slot holds a valid index, so no
+// later scan can leave the replica's arrays.
+__device__ bool build_cells(const Rep& R, int n, const Grid& g, int lane) {
+    const int ncell = g.G * g.G;
+    for (int c = lane; c < ncell; c += 32) R.cnt[c] = 0;
+    for (int k = lane; k < ncell * kCellK; k += 32) R.slot[k] = 0;
+    __syncwarp();
+    bool ok = true;
+    for (int i = lane; i < n; i += 32) {
+        const float4 p = R.sq[i];
+        const int c = g.cx(p.y) * g.G + g.cx(p.x);
+        const unsigned k = atomicAdd(reinterpret_cast<unsigned*>(R.cnt + (c & ~3)), 1u << (8 * (c & 3)));
+        const unsigned slot_k = (k >> (8 * (c & 3))) & 0xffu;
+        if (slot_k < (unsigned)kCellK) R.slot[c * kCellK + slot_k] = (uint16_t)i;
+        else ok = false;
+    }
+    __syncwarp();
+    ok = __all_sync(0xffffffffu, ok);
+    if (!ok) {
+        for (int c = lane; c < ncell; c += 32)
+            if (R.cnt[c] > kCellK) R.cnt[c] = (uint8_t)kCellK;
+        __syncwarp();
+    }
+    return ok;
+}
+
+// Visit the squares of the 3x3 cell block around (cx, cy): returns through
+// `fn(j)` for every candidate t = lane, lane + 32, ...
+template <typename Fn>
+__device__ __forceinline__ void for_block(const Rep& R, const Grid& g, int cx, int cy, int lane, Fn&& fn) {
+    int cnt = 0, cell = 0;
+    if (lane < 9) {
+        const int x = cx + lane % 3 - 1, y = cy + lane / 3 - 1;
+        if (x >= 0 && x < g.G && y >= 0 && y < g.G) {
+            cell = y * g.G + x;
+            cnt = R.cnt[cell];
+        }
+    }
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 16; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 8);
+    int ends[9], cells[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+        ends[c] = __shfl_sync(0xffffffffu, incl, c);
+        cells[c] = __shfl_sync(0xffffffffu, cell, c);
+    }
+    for (int t = lane; t < total; t += 32) {
+        int c = 0, start = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (t >= ends[k]) { c = k + 1; start = ends[k]; }
+        fn((int)R.slot[cells[c] * kCellK + (t - start)]);
+    }
+}
+
+__device__ __forceinline__ long long qe(float e) { return __float2ll_rn(e * kEScale); }
+
+__device__ __forceinline__ long long warp_sum_ll(long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double warp_max_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__device__ __forceinline__ double warp_min_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Full energy of one replica (walls + each neighbour pair once), fixed point.
+__device__ long long full_energy(const Rep& R, int n, const Grid& g, float L, int lane) {
+    long long e = 0;
+    for (int i = 0; i < n; ++i) {
+        const float4 P = R.sq[i];
+        if (lane == 0) e += qe(wall_e(P.x, P.y, P.z, P.w, L));
+        for_block(R, g, g.cx(P.x), g.cx(P.y), lane, [&](int j) {
+            if (j > i) {
+                const float4 Q = R.sq[j];
+                const float dx = Q.x - P.x, dy = Q.y - P.y;
+                if (dx * dx + dy * dy < kPairCut2) e += qe(sat_pair_energy(dx, dy, P.z, P.w, Q.z, Q.w));
+            }
+        });
+    }
+    return warp_sum_ll(e);
+}
+
+// FP64 dilation-certified side of a replica (device_certified_side,
+// seeded.cu:175-226): the smallest centre dilation lambda that opens a
+// tau = 2.6e-8 gap along the best axis of every close pair, rejection above
+// 1.008, side of the bounding box of the dilated squares.  Products are kept
+// unfused so the result rounds like the host oracle's.
+__device__ double cert_side(const Rep& R, int n, const Grid& g, int lane, double& lam_out, double& x0_out,
+                            double& y0_out) {
+    const double tau = 2.6e-8;
+    double lam = 1.0;
+    for (int i = lane; i < n; i += 32) {
+        const float4 P = R.sq[i];
+        const double xi = P.x, yi = P.y;
+        double si, ci;
+        sincos((double)R.ang[i], &si, &ci);
+        const int cx = g.cx(P.x), cy = g.cx(P.y);
+        for (int dy = -1; dy <= 1; ++dy) {
+            for (int dxc = -1; dxc <= 1; ++dxc) {
+                const int x = cx + dxc, y = cy + dy;
+                if (x < 0 || x >= g.G || y < 0 || y >= g.G) continue;
+                const int cell = y * g.G + x;
+                const int m = R.cnt[cell];
+                for (int k = 0; k < m; ++k) {
+                    const int j = R.slot[cell * kCellK + k];
+                    if (j <= i) continue;
+                    const double dx = __dsub_rn(xi, (double)R.sq[j].x), dyv = __dsub_rn(yi, (double)R.sq[j].y);
+                    if (__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dyv, dyv)) >= 2.05) continue;
+                    double sj, cj;
+                    sincos((double)R.ang[j], &sj, &cj);
+                    const double c12 = fabs(__dadd_rn(__dmul_rn(ci, cj), __dmul_rn(si, sj)));
+                    const double s12 = fabs(__dadd_rn(__dmul_rn(-si, cj), __dmul_rn(ci, sj)));
+                    const double r = __dadd_rn(0.5, __dmul_rn(0.5, __dadd_rn(c12, s12)));
+                    const double v1 = fabs(__dadd_rn(__dmul_rn(dx, ci), __dmul_rn(dyv, si)));
+                    const double v2 = fabs(__dadd_rn(__dmul_rn(-dx, si), __dmul_rn(dyv, ci)));
+                    const double v3 = fabs(__dadd_rn(__dmul_rn(dx, cj), __dmul_rn(dyv, sj)));
+                    const double v4 = fabs(__dadd_rn(__dmul_rn(-dx, sj), __dmul_rn(dyv, cj)));
+                    const double vmax = fmax(fmax(v1, v2), fmax(v3, v4));
+                    const double req = vmax > 1e-12 ? __ddiv_rn(__dadd_rn(r, tau), vmax) : 1e9;
+                    lam = fmax(lam, req);
+                }
+            }
+        }
+    }
+    lam = warp_max_d(lam);
+    lam_out = lam;
+    if (lam > 1.008) return 1e9;
+    double bx0 = 1e9, bx1 = -1e9, by0 = 1e9, by1 = -1e9;
+    for (int i = lane; i < n; i += 32) {
+        const float4 P = R.sq[i];
+        const double x = __dmul_rn((double)P.x, lam), y = __dmul_rn((double)P.y, lam);
+        double s, c;
+        sincos((double)R.ang[i], &s, &c);
+        const double r = __dmul_rn(0.5, __dadd_rn(fabs(c), fabs(s)));
+        bx0 = fmin(bx0, __dsub_rn(x, r));
+        bx1 = fmax(bx1, __dadd_rn(x, r));
+        by0 = fmin(by0, __dsub_rn(y, r));
+        by1 = fmax(by1, __dadd_rn(y, r));
+    }
+    bx0 = warp_min_d(bx0);
+    bx1 = warp_max_d(bx1);
+    by0 = warp_min_d(by0);
+    by1 = warp_max_d(by1);
+    x0_out = bx0;
+    y0_out = by0;
+    return fmax(__dsub_rn(bx1, bx0), __dsub_rn(by1, by0));
+}
+
+// Quench of one replica: Jacobi gradient descent on its overlap + wall
+// energy with a backtracking step (every square moves at once; gradients are
+// summed in fixed point, so the result does not depend on neighbour order).
+// The reference's analogue is the per-epoch polish (seeded.cu:621-713).
+__device__ long long quench(const Rep& R, int n, Grid& g, float L, int lane, int iters, float4* grad,
+                            float4* saved, long long E) {
+    float alpha = 0.05f;
+    for (int it = 0; it < iters && E > 0; ++it) {
+        for (int i = lane; i < n; i += 32) {
+            const float4 P = R.sq[i];
+            float wx = 0.f, wy = 0.f, wa = 0.f;
+            wall_energy_grad(P.x, P.y, P.z, P.w, L, wx, wy, wa);
+            long long qx = qe(wx), qy = qe(wy), qa = qe(wa);
+            const int cx = g.cx(P.x), cy = g.cx(P.y);
+            for (int dy = -1; dy <= 1; ++dy) {
+                for (int dxc = -1; dxc <= 1; ++dxc) {
+                    const int x = cx + dxc, y = cy + dy;
+                    if (x < 0 || x >= g.G || y < 0 || y >= g.G) continue;
+                    const int cell = y * g.G + x;
+                    const int m = R.cnt[cell];
+                    for (int k = 0; k < m; ++k) {
+                        const int j = R.slot[cell * kCellK + k];
+                        if (j == i) continue;
+                        const float4 Q = R.sq[j];
+                        const float ex = Q.x - P.x, ey = Q.y - P.y;
+                        if (ex * ex + ey * ey >= kPairCut2) continue;
+                        PairGrad pg;
+                        if (sat_pair_grad(ex, ey, P.z, P.w, Q.z, Q.w, pg)) {
+                            qx += qe(pg.px);
+                            qy += qe(pg.py);
+                            qa += qe(pg.pa);
+                        }
+                    }
+                }
+            }
+            grad[i] = make_float4((float)qx * (1.0f / kEScale), (float)qy * (1.0f / kEScale),
+                                  (float)qa * (1.0f / kEScale), 0.f);
+            saved[i] = make_float4(P.x, P.y, R.ang[i], 0.f);
+        }
+        __syncwarp();
+        for (int tries = 0; tries < 6; ++tries) {
+            for (int i = lane; i < n; i += 32) {
+                const float4 d = grad[i], o = saved[i];
+                const float sx = fminf(0.1f, fmaxf(-0.1f, alpha * d.x));
+                const float sy = fminf(0.1f, fmaxf(-0.1f, alpha * d.y));
+                float a = o.z - fminf(0.1f, fmaxf(-0.1f, alpha * d.z));
+                a = a - kHalfPiF * floorf(a * (1.0f / kHalfPiF));
+                if (!(a >= 0.f && a < kHalfPiF)) a = 0.f;
+                float sn, cs;
+                sincosf(a, &sn, &cs);
+                R.sq[i] = make_float4(o.x - sx, o.y - sy, cs, sn);
+                R.ang[i] = a;
+            }
+            __syncwarp();
+            const bool fits = build_cells(R, n, g, lane);
+            const long long En = fits ? full_energy(R, n, g, L, lane) : E;
+            if (fits && En < E) {
+                E = En;
+                alpha = fminf(alpha * 1.3f, 0.2f);
+                break;
+            }
+            alpha *= 0.3f;
+            if (tries == 5) {  // no improvement: restore the saved state
+                for (int i = lane; i < n; i += 32) {
+                    const float4 o = saved[i];
+                    float sn, cs;
+                    sincosf(o.z, &sn, &cs);
+                    R.sq[i] = make_float4(o.x, o.y, cs, sn);
+                    R.ang[i] = o.z;
+                }
+                __syncwarp();
+                build_cells(R, n, g, lane);
+                it = iters;
+            }
+        }
+    }
+    return E;
+}
+
+struct CtaShared {
+    JobDev jd;
+    JobMut jm;
+    float temps[kMaxR];
+    long long wE[kMaxRl];      // this CTA's replica energies at a checkpoint
+    double wL[kMaxRl];         // this CTA's candidate certified sides at a checkpoint
+    double wlam[kMaxRl], wx0[kMaxRl], wy0[kMaxRl];
+    int wbad[kMaxRl];          // cell-list overflow per warp
+    int decision_win;          // global replica index of the new best (-1: none)
+    int bad;                   // any overflow in the cluster
+    float newL;
+    unsigned long long props[kMaxRl], accs[kMaxRl];
+};
+
+__global__ void __launch_bounds__(1024) anneal_kernel(const int32_t* __restrict__ job_list,
+                                                      const JobDev* __restrict__ jdev, JobMut* __restrict__ jmut,
+                                                      float4* __restrict__ pos, double* __restrict__ best,
+                                                      int slice_sweeps) {
+    cg::cluster_group cluster = cg::this_cluster();
+    __shared__ CtaShared S;
+    extern __shared__ __align__(16) unsigned char dyn[];
+    const int rank = (int)cluster.block_rank();
+    const int job = job_list[blockIdx.x / cluster.num_blocks()];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    if (tid == 0) {
+        S.jd = jdev[job];
+        S.jm = jmut[job];
+    }
+    __syncthreads();
+    const JobDev& jd = S.jd;
+    if (S.jm.status != kRunning) return;  // identical in every CTA of the cluster
+    const int n = jd.n, R = jd.R, Rl = jd.Rl;
+    const int r = rank * Rl + w;  // global replica index of this warp
+    const bool active = w < Rl;
+    if (tid < R) {
+        const float lt = logf(jd.tmin), lh = logf(jd.tmax);
+        S.temps[tid] = R > 1 ? expf(lt + (lh - lt) * (float)tid / (float)(R - 1)) : jd.tmin;
+    }
+    const int64_t rb = replica_smem_bytes(n, jd.Gmax);
+    Rep rep = rep_view(dyn + (active ? w : 0) * rb, n, jd.Gmax);
+    float L = S.jm.L;
+    Grid g = make_grid(L, jd.Gmax);
+    const uint32_t k0 = (uint32_t)jd.seed, k1 = (uint32_t)(jd.seed >> 32);
+
+    // load the replica
+    if (active) {
+        const float4* src = pos + jd.pos_off + (int64_t)r * n;
+        for (int i = lane; i < n; i += 32) {
+            const float4 p = src[i];
+            float s, c;
+            sincosf(p.z, &s, &c);
+            rep.sq[i] = make_float4(p.x, p.y, c, s);
+            rep.ang[i] = p.z;
+        }
+        __syncwarp();
+        const bool ok = build_cells(rep, n, g, lane);
+        if (lane == 0) S.wbad[w] = !ok;
+    }
+    __syncthreads();
+    cluster.sync();
+    if (tid == 0) {
+        int bad = 0;
+        for (int q = 0; q < (int)cluster.num_blocks(); ++q) {
+            const CtaShared* o = cluster.map_shared_rank(&S, q);
+            for (int k = 0; k < Rl; ++k) bad |= o->wbad[k];
+        }
+        S.bad = bad;
+    }
+    cluster.sync();
+    if (S.bad) {
+        if (rank == 0 && tid == 0) jmut[job].status = kErrCells;
+        return;
+    }
+    long long E = 0;
+    if (active) {
+        E = S.jm.sweep == 0 ? full_energy(rep, n, g, L, lane) : S.jm.E[r];
+    }
+    unsigned long long props = 0, accs = 0;
+    float invT = active ? 1.0f / S.temps[S.jm.perm[r]] : 0.f;
+
+    const int sweep0 = S.jm.sweep;
+    const int sweep_end = min(jd.sweeps_total, sweep0 + slice_sweeps);
+    for (int sweep = sweep0; sweep < sweep_end; ++sweep) {
+        if (active) {
+            for (int k = 0; k < n; ++k) {
+                const uint64_t ev = (uint64_t)sweep * (uint64_t)n + (uint64_t)k;
+                U4 rr{0u, 0u, 0u, 0u};
+                if (lane < 2) rr = philox4x32_10(U4{(uint32_t)ev, (uint32_t)(ev >> 32), (uint32_t)r, (uint32_t)lane}, k0, k1);
+                const uint32_t a0 = __shfl_sync(0xffffffffu, rr.x, 0), a1 = __shfl_sync(0xffffffffu, rr.y, 0);
+                const uint32_t a2 = __shfl_sync(0xffffffffu, rr.z, 0), a3 = __shfl_sync(0xffffffffu, rr.w, 0);
+                const uint32_t b0 = __shfl_sync(0xffffffffu, rr.x, 1), b1 = __shfl_sync(0xffffffffu, rr.y, 1);
+                const int i = (int)(((uint64_t)a0 * (uint64_t)n) >> 32);
+                const float rad1 = sqrtf(-2.f * __logf(u01(a1)));
+                float sn1, cs1;
+                __sincosf(6.2831853f * u01(a2), &sn1, &cs1);
+                const float rad2 = sqrtf(-2.f * __logf(u01(a3)));
+                const float n2 = rad2 * __cosf(6.2831853f * u01(b0));
+                const float dx = fminf(kMaxStep, fmaxf(-kMaxStep, jd.sigma_xy * rad1 * cs1));
+                const float dy = fminf(kMaxStep, fmaxf(-kMaxStep, jd.sigma_xy * rad1 * sn1));
+                const float da = jd.sigma_a * n2;
+                const float4 P = rep.sq[i];
+                // keep centres in [0.5, L - 0.5] without ever moving a square
+                // further than the clamped step (it may start outside)
+                const float nx = fminf(fmaxf(P.x, L - 0.5f), fmaxf(fminf(P.x, 0.5f), P.x + dx));
+                const float ny = fminf(fmaxf(P.y, L - 0.5f), fmaxf(fminf(P.y, 0.5f), P.y + dy));
+                float na = rep.ang[i] + da;
+                na = na - kHalfPiF * floorf(na * (1.0f / kHalfPiF));
+                if (!(na >= 0.f && na < kHalfPiF)) na = 0.f;
+                float ns, nc;
+                sincosf(na, &ns, &nc);
+                const int ocx = g.cx(P.x), ocy = g.cx(P.y);
+                long long dq = 0;
+                if (lane == 0) dq = qe(wall_e(nx, ny, nc, ns, L)) - qe(wall_e(P.x, P.y, P.z, P.w, L));
+                for_block(rep, g, ocx, ocy, lane, [&](int j) {
+                    if (j == i) return;
+                    const float4 Q = rep.sq[j];
+                    const float ex = Q.x - nx, ey = Q.y - ny;
+                    if (ex * ex + ey * ey < kPairCut2) dq += qe(sat_pair_energy(ex, ey, nc, ns, Q.z, Q.w));
+                    const float fx = Q.x - P.x, fy = Q.y - P.y;
+                    if (fx * fx + fy * fy < kPairCut2) dq -= qe(sat_pair_energy(fx, fy, P.z, P.w, Q.z, Q.w));
+                });
+                dq = warp_sum_ll(dq);
+                const float de = (float)dq * (1.0f / kEScale);
+                bool acc = dq <= 0 || u01(b1) < __expf(-de * invT);
+                const int ncx = g.cx(nx), ncy = g.cx(ny);
+                const int oc = ocy * g.G + ocx, ncell = ncy * g.G + ncx;
+                if (acc && oc != ncell && rep.cnt[ncell] >= kCellK) acc = false;
+                ++props;
+                if (acc) {
+                    ++accs;
+                    E += dq;
+                    if (lane == 0) {
+                        rep.sq[i] = make_float4(nx, ny, nc, ns);
+                        rep.ang[i] = na;
+                        if (oc != ncell) {
+                            const int m = rep.cnt[oc];
+                            for (int q = 0; q < m; ++q) {
+                                if (rep.slot[oc * kCellK + q] == (uint16_t)i) {
+                                    rep.slot[oc * kCellK + q] = rep.slot[oc * kCellK + m - 1];
+                                    break;
+                                }
+                            }
+                            rep.cnt[oc] = (uint8_t)(m - 1);
+                            rep.slot[ncell * kCellK + rep.cnt[ncell]] = (uint16_t)i;
+                            rep.cnt[ncell] = (uint8_t)(rep.cnt[ncell] + 1);
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        // ---- checkpoint: best-state search, shrink, replica exchange.  Only at
+        // multiples of exchange_every (and at the end of the budget), so a
+        // job's trajectory does not depend on how it is sliced.
+        const bool xpoint = (sweep + 1) % jd.exchange_every == 0;
+        if (!xpoint && sweep + 1 != jd.sweeps_total) continue;
+        if (active) {
+            double Lc = 1e30, lam = 0, x0 = 0, y0 = 0;
+            // the replica on the coldest rung is quenched toward zero overlap
+            if (S.jm.perm[r] == 0 && jd.quench_iters > 0)
+                E = quench(rep, n, g, L, lane, jd.quench_iters, pos + jd.scr_off, pos + jd.scr_off + n, E);
+            // any state whose overlaps a dilation of at most 0.8% removes is a
+            // certified candidate (penetrations of depth d cost about d^2 each)
+            if (E < qe(1e-4f)) Lc = cert_side(rep, n, g, lane, lam, x0, y0);
+            if (lane == 0) {
+                S.wE[w] = E;
+                S.wL[w] = Lc;
+                S.wlam[w] = lam;
+                S.wx0[w] = x0;
+                S.wy0[w] = y0;
+            }
+        }
+        __syncthreads();
+        cluster.sync();
+        if (tid == 0) {
+            // every CTA takes the same decisions from the same gathered values
+            long long Eall[kMaxR];
+            double bestc = S.jm.best_L;
+            int win = -1;
+            for (int q = 0; q < (int)cluster.num_blocks(); ++q) {
+                const CtaShared* o = cluster.map_shared_rank(&S, q);
+                for (int k = 0; k < Rl; ++k) {
+                    Eall[q * Rl + k] = o->wE[k];
+                    if (o->wL[k] < bestc) {
+                        bestc = o->wL[k];
+                        win = q * Rl + k;
+                    }
+                }
+            }
+            S.decision_win = win;
+            S.newL = L;
+            if (win >= 0) {
+                S.jm.best_L = bestc;
+                S.jm.improvements += 1;
+                float nl = (float)(fmin((double)L, bestc) * (1.0 - (double)jd.shrink));
+                const float lb = sqrtf((float)n) + 1e-6f;
+                if (nl < lb) nl = lb;
+                if (nl < L) {
+                    S.newL = nl;
+                    S.jm.shrinks += 1;
+                }
+            }
+            // replica exchange between neighbouring rungs, alternating parity
+            if (xpoint) {
+                int holder[kMaxR];
+                for (int q = 0; q < R; ++q) holder[S.jm.perm[q]] = q;
+                const int par = S.jm.xround & 1;
+                for (int k = par; k + 1 < R; k += 2) {
+                    const int a = holder[k], b = holder[k + 1];
+                    const U4 u = philox4x32_10(U4{(uint32_t)S.jm.xround, (uint32_t)k, 0u, 0x7fffffffu}, k0, k1);
+                    const float d = (1.0f / S.temps[k] - 1.0f / S.temps[k + 1]) *
+                                    ((float)(Eall[a] - Eall[b]) * (1.0f / kEScale));
+                    S.jm.xatt += 1;
+                    if (d >= 0.f || u01(u.x) < expf(d)) {
+                        S.jm.xacc += 1;
+                        S.jm.perm[a] = k + 1;
+                        S.jm.perm[b] = k;
+                        holder[k] = b;
+                        holder[k + 1] = a;
+                    }
+                }
+                S.jm.xround += 1;
+            }
+        }
+        cluster.sync();
+        __syncthreads();
+        if (active) {
+            invT = 1.0f / S.temps[S.jm.perm[r]];
+            if (S.decision_win == r) {
+                // new best: dilated, translated to the origin, angles in [0, pi/2)
+                double* dst = best + jd.best_off;
+                const double lam = S.wlam[w], x0 = S.wx0[w], y0 = S.wy0[w];
+                for (int i = lane; i < n; i += 32) {
+                    dst[3 * i] = __dsub_rn(__dmul_rn((double)rep.sq[i].x, lam), x0);
+                    dst[3 * i + 1] = __dsub_rn(__dmul_rn((double)rep.sq[i].y, lam), y0);
+                    dst[3 * i + 2] = (double)rep.ang[i];
+                }
+            }
+        }
+        if (S.newL < L) {
+            const float f = S.newL / L;
+            L = S.newL;
+            g = make_grid(L, jd.Gmax);
+            if (active) {
+                for (int i = lane; i < n; i += 32) {
+                    rep.sq[i].x *= f;
+                    rep.sq[i].y *= f;
+                }
+                __syncwarp();
+                const bool ok = build_cells(rep, n, g, lane);
+                if (lane == 0) S.wbad[w] = !ok;
+                E = full_energy(rep, n, g, L, lane);
+            }
+            __syncthreads();
+            cluster.sync();
+            if (tid == 0) {
+                int bad = 0;
+                for (int q = 0; q < (int)cluster.num_blocks(); ++q) {
+                    const CtaShared* o = cluster.map_shared_rank(&S, q);
+                    for (int k = 0; k < Rl; ++k) bad |= o->wbad[k];
+                }
+                S.bad = bad;
+            }
+            cluster.sync();
+            if (S.bad) {
+                if (rank == 0 && tid == 0) jmut[job].status = kErrCells;
+                return;
+            }
+        }
+    }
+
+    // ---- write the slice back
+    if (active) {
+        float4* dst = pos + jd.pos_off + (int64_t)r * n;
+        for (int i = lane; i < n; i += 32) dst[i] = make_float4(rep.sq[i].x, rep.sq[i].y, rep.ang[i], 0.f);
+        if (lane == 0) {
+            jmut[job].E[r] = E;
+            atomicAdd(reinterpret_cast<unsigned long long*>(&jmut[job].proposals), props);
+            atomicAdd(reinterpret_cast<unsigned long long*>(&jmut[job].accepted), accs);
+        }
+    }
+    if (rank == 0 && tid == 0) {
+        JobMut& m = jmut[job];
+        m.L = L;
+        m.sweep = sweep_end;
+        m.xround = S.jm.xround;
+        m.status = sweep_end >= jd.sweeps_total ? kFinished : kRunning;
+        m.shrinks = S.jm.shrinks;
+        m.improvements = S.jm.improvements;
+        m.best_L = S.jm.best_L;
+        m.xatt = S.jm.xatt;
+        m.xacc = S.jm.xacc;
+        for (int q = 0; q < R; ++q) m.perm[q] = S.jm.perm[q];
+    }
+}
+
+int launch_anneal(cudaStream_t stream, int njobs, int cs, int Rl, size_t smem, const int32_t* job_list,
+                  const JobDev* jdev, JobMut* jmut, float4* pos, double* best, int slice) {
+    static bool attr_done[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!attr_done[dev & 63]) {
+        SQS_CUDA(cudaFuncSetAttribute(anneal_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      232448 - (int)sizeof(CtaShared)));
+        SQS_CUDA(cudaFuncSetAttribute(anneal_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        attr_done[dev & 63] = true;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(njobs * cs), 1, 1);
+    cfg.blockDim = dim3((unsigned)(Rl * 32), 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    SQS_CUDA(cudaLaunchKernelEx(&cfg, anneal_kernel, job_list, jdev, jmut, pos, best, slice));
+    return SQS_OK;
+}
+
+}  // namespace ann
+}  // namespace sqs

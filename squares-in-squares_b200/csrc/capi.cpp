@@ -112,6 +112,7 @@ int sqs_ctx_destroy(sqs_ctx* ctx) {
     ctx->d_grad.release();
     ctx->d_cand.release();
     ctx->d_misc.release();
+    ctx->d_anneal.release();
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SQS_OK;

@@ -63,7 +63,7 @@ struct sqs_ctx {
     size_t flush_bytes = 0;
     int64_t launches = 0;
     // staging for the host-pointer entry points
-    sqs::DevBuf d_in, d_side, d_out, d_grad, d_cand, d_misc;
+    sqs::DevBuf d_in, d_side, d_out, d_grad, d_cand, d_misc, d_anneal;
 };
 
 namespace sqs {

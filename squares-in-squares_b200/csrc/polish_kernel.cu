@@ -1,0 +1,259 @@
+// FP64 gradient polish of every job's best state, one CTA per job.
+//
+// The reference polishes every chain after every epoch with PRP+ conjugate
+// gradient and a 5-step backtracking search on the squared-penetration
+// energy at the chain's target side (seeded.cu:621-713, gradient
+// pair_cached_smooth :67-90 and the smooth wall derivative :640-645).  Here
+// the polish runs once per job on its best FP64 state: compress the state by
+// a factor (1 - delta) into a side L (1 - delta), descend the same energy
+// with a backtracking line search until it vanishes, and keep the result if
+// its dilation-certified side (device_certified_side, seeded.cu:175-226) is
+// smaller; delta shrinks after every failure.  Pairs are evaluated all
+// against all (n <= 1000, one CTA): every thread owns squares and loops over
+// all partners, so gradients need no atomics and reductions have a fixed
+// order (the result is deterministic).
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "anneal.cuh"
+#include "common.cuh"
+
+namespace sqs {
+namespace ann {
+
+constexpr int kPT = 256;  // threads per polish CTA
+
+size_t polish_smem_bytes(int n) { return (size_t)n * (4 * 24 + 16) + 64; }
+
+__device__ __forceinline__ double sgn_s(double x) { return fabs(x) > 1e-6 ? (x >= 0.0 ? 1.0 : -1.0) : 0.0; }
+
+// Smooth-variant pair gradient for square p against q (pair_cached_smooth):
+// returns gap^2 and adds d/dp into g.
+__device__ __forceinline__ double pair_smooth(double px, double py, double c, double s, double qx, double qy,
+                                              double d, double t, double& gx, double& gy, double& ga) {
+    const double dx = qx - px, dy = qy - py;
+    if (dx * dx + dy * dy >= 2.000001) return 0.0;
+    const double cd = c * d + s * t, sd = s * d - c * t;
+    const double rad = 0.5 + 0.5 * (fabs(cd) + fabs(sd));
+    const double deriv = 0.5 * (-sgn_s(cd) * sd + sgn_s(sd) * cd);
+    const double ux[4] = {c, -s, d, -t}, uy[4] = {s, c, t, d};
+    double gap = -1e100, ggx = 0, ggy = 0, gga = 0;
+    for (int k = 0; k < 4; ++k) {
+        const double v = dx * ux[k] + dy * uy[k], z = fabs(v) - rad;
+        if (z > gap) {
+            gap = z;
+            const double sv = v >= 0.0 ? 1.0 : -1.0;
+            ggx = -sv * ux[k];
+            ggy = -sv * uy[k];
+            gga = -deriv + (k < 2 ? sv * (-dx * uy[k] + dy * ux[k]) : 0.0);
+        }
+    }
+    if (gap >= 0.0) return 0.0;
+    gx += 2.0 * gap * ggx;
+    gy += 2.0 * gap * ggy;
+    ga += 2.0 * gap * gga;
+    return gap * gap;
+}
+
+__device__ __forceinline__ double wall_smooth(double x, double y, double c, double s, double L, double& gx,
+                                              double& gy, double& ga) {
+    const double r = 0.5 * (fabs(c) + fabs(s));
+    const double dr = 0.5 * (-sgn_s(c) * s + sgn_s(s) * c);
+    const double v[4] = {r - x, x + r - L, r - y, y + r - L};
+    double e = 0.0;
+    for (int k = 0; k < 4; ++k) {
+        if (v[k] > 0.0) {
+            e += v[k] * v[k];
+            const double f = 2.0 * v[k];
+            gx += f * (k == 0 ? -1.0 : k == 1 ? 1.0 : 0.0);
+            gy += f * (k == 2 ? -1.0 : k == 3 ? 1.0 : 0.0);
+            ga += f * dr;
+        }
+    }
+    return e;
+}
+
+__device__ double block_sum(double v, double* red) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+    for (int w = 0; w < kPT / 32; ++w) t += red[w];
+    return t;
+}
+
+__device__ double block_max(double v, double* red) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = red[0];
+    for (int w = 1; w < kPT / 32; ++w) t = fmax(t, red[w]);
+    return t;
+}
+
+// Energy (and gradient into g when g != nullptr) of the state q at side L.
+__device__ double energy(int n, const double3* q, const double2* cs, double L, double3* g, double* red) {
+    double e = 0.0;
+    for (int i = threadIdx.x; i < n; i += kPT) {
+        const double3 p = q[i];
+        const double2 pc = cs[i];
+        double gx = 0, gy = 0, ga = 0;
+        e += wall_smooth(p.x, p.y, pc.x, pc.y, L, gx, gy, ga);
+        for (int j = 0; j < n; ++j) {
+            if (j == i) continue;
+            const double3 o = q[j];
+            const double2 oc = cs[j];
+            double hx = 0, hy = 0, ha = 0;
+            const double pe = pair_smooth(p.x, p.y, pc.x, pc.y, o.x, o.y, oc.x, oc.y, hx, hy, ha);
+            if (j > i) e += pe;
+            gx += hx;
+            gy += hy;
+            ga += ha;
+        }
+        if (g) g[i] = make_double3(gx, gy, ga);
+    }
+    return block_sum(e, red);
+}
+
+// Certified side of q (dilation lambda, bounding box of the dilated state).
+__device__ double cert_side_all(int n, const double3* q, const double2* cs, double* red, double& lam_out,
+                                double& x0, double& y0) {
+    double lam = 1.0;
+    for (int i = threadIdx.x; i < n; i += kPT) {
+        const double3 p = q[i];
+        const double ci = cs[i].x, si = cs[i].y;
+        for (int j = i + 1; j < n; ++j) {
+            const double dx = p.x - q[j].x, dy = p.y - q[j].y;
+            if (dx * dx + dy * dy >= 2.05) continue;
+            const double cj = cs[j].x, sj = cs[j].y;
+            const double c12 = fabs(ci * cj + si * sj), s12 = fabs(-si * cj + ci * sj);
+            const double r = 0.5 + 0.5 * (c12 + s12);
+            const double v = fmax(fmax(fabs(dx * ci + dy * si), fabs(-dx * si + dy * ci)),
+                                  fmax(fabs(dx * cj + dy * sj), fabs(-dx * sj + dy * cj)));
+            lam = fmax(lam, v > 1e-12 ? (r + 2.6e-8) / v : 1e9);
+        }
+    }
+    lam = block_max(lam, red);
+    lam_out = lam;
+    if (lam > 1.008) return 1e30;
+    double a0 = 1e300, a1 = -1e300, b0 = 1e300, b1 = -1e300;
+    for (int i = threadIdx.x; i < n; i += kPT) {
+        const double r = 0.5 * (fabs(cs[i].x) + fabs(cs[i].y));
+        const double x = q[i].x * lam, y = q[i].y * lam;
+        a0 = fmin(a0, x - r);
+        a1 = fmax(a1, x + r);
+        b0 = fmin(b0, y - r);
+        b1 = fmax(b1, y + r);
+    }
+    x0 = -block_max(-a0, red);
+    const double xm = block_max(a1, red);
+    y0 = -block_max(-b0, red);
+    const double ym = block_max(b1, red);
+    return fmax(xm - x0, ym - y0);
+}
+
+__device__ __forceinline__ double wrap_q(double a) {
+    a = fmod(a, 1.57079632679489661923);
+    return a < 0.0 ? a + 1.57079632679489661923 : a;
+}
+
+__device__ void trig_of(int n, const double3* q, double2* cs) {
+    for (int i = threadIdx.x; i < n; i += kPT) {
+        double s, c;
+        sincos(q[i].z, &s, &c);
+        cs[i] = make_double2(c, s);
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kPT) polish_kernel(const int32_t* __restrict__ job_list,
+                                                     const JobDev* __restrict__ jdev, JobMut* __restrict__ jmut,
+                                                     double* __restrict__ best) {
+    extern __shared__ __align__(16) unsigned char dyn[];
+    __shared__ double red[kPT / 32];
+    const int job = job_list[blockIdx.x];
+    const JobDev jd = jdev[job];
+    const int n = jd.n;
+    double Lb = jmut[job].best_L;
+    if (jd.polish_iters <= 0 || Lb >= 1e29 || jmut[job].status < 0) return;
+    double3* q0 = reinterpret_cast<double3*>(dyn);  // accepted state of the descent
+    double3* q = q0 + n;                            // trial state
+    double3* g = q + n;                             // gradient at q0
+    double3* sv = g + n;                            // best so far (translated, dilated)
+    double2* cs = reinterpret_cast<double2*>(sv + n);  // cos/sin of the state being evaluated
+    double* b = best + jd.best_off;
+    for (int i = threadIdx.x; i < n; i += kPT) sv[i] = make_double3(b[3 * i], b[3 * i + 1], b[3 * i + 2]);
+    __syncthreads();
+    double delta = 1e-4;
+    int budget = jd.polish_iters;
+    for (int attempt = 0; attempt < 12 && budget > 0 && delta > 1e-9; ++attempt) {
+        const double f = 1.0 - delta, Lt = Lb * f;
+        for (int i = threadIdx.x; i < n; i += kPT) q0[i] = make_double3(sv[i].x * f, sv[i].y * f, sv[i].z);
+        __syncthreads();
+        trig_of(n, q0, cs);
+        double E = energy(n, q0, cs, Lt, g, red);
+        double alpha = 0.05;
+        while (budget > 0 && E > 1e-26) {
+            --budget;
+            bool moved = false;
+            for (int ls = 0; ls < 8 && !moved; ++ls) {
+                for (int i = threadIdx.x; i < n; i += kPT) {
+                    const double3 p = q0[i], d = g[i];
+                    q[i] = make_double3(p.x - alpha * d.x, p.y - alpha * d.y, wrap_q(p.z - alpha * d.z));
+                }
+                __syncthreads();
+                trig_of(n, q, cs);
+                const double En = energy(n, q, cs, Lt, nullptr, red);
+                if (En < E) {
+                    E = En;
+                    moved = true;
+                    alpha = fmin(alpha * 1.5, 0.5);
+                    for (int i = threadIdx.x; i < n; i += kPT) q0[i] = q[i];
+                    __syncthreads();
+                } else {
+                    alpha *= 0.3;
+                }
+            }
+            if (!moved) break;
+            E = energy(n, q0, cs, Lt, g, red);  // cs holds the trig of q == q0
+        }
+        trig_of(n, q0, cs);
+        double lam = 0, x0 = 0, y0 = 0;
+        const double Lc = cert_side_all(n, q0, cs, red, lam, x0, y0);
+        if (Lc < Lb) {
+            Lb = Lc;
+            for (int i = threadIdx.x; i < n; i += kPT)
+                sv[i] = make_double3(q0[i].x * lam - x0, q0[i].y * lam - y0, q0[i].z);
+            __syncthreads();
+        } else {
+            delta *= 0.3;
+        }
+    }
+    for (int i = threadIdx.x; i < n; i += kPT) {
+        b[3 * i] = sv[i].x;
+        b[3 * i + 1] = sv[i].y;
+        b[3 * i + 2] = sv[i].z;
+    }
+    if (threadIdx.x == 0) jmut[job].best_L = Lb;
+}
+
+int launch_polish(cudaStream_t stream, int njobs, const int32_t* job_list, const JobDev* jdev, JobMut* jmut,
+                  double* best, size_t smem) {
+    static bool attr_done[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!attr_done[dev & 63]) {
+        SQS_CUDA(cudaFuncSetAttribute(polish_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        attr_done[dev & 63] = true;
+    }
+    if (njobs <= 0) return SQS_OK;
+    polish_kernel<<<njobs, kPT, smem, stream>>>(job_list, jdev, jmut, best);
+    SQS_CUDA(cudaGetLastError());
+    return SQS_OK;
+}
+
+}  // namespace ann
+}  // namespace sqs

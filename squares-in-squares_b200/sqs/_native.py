@@ -36,6 +36,24 @@ class Verdict(C.Structure):
                 ("L", C.c_char * 80), ("reason", C.c_char * 112)]
 
 
+class Job(C.Structure):
+    """sqs_job (include/sqs.h)."""
+    _fields_ = [("n", C.c_int32), ("replicas", C.c_int32), ("sweeps", C.c_int32), ("exchange_every", C.c_int32),
+                ("polish_iters", C.c_int32), ("flags", C.c_int32), ("L0", C.c_double), ("tmin", C.c_double),
+                ("tmax", C.c_double), ("sigma_xy", C.c_double), ("sigma_a", C.c_double), ("shrink", C.c_double),
+                ("seed", C.c_uint64), ("xya", C.POINTER(C.c_double))]
+
+
+class JobResult(C.Structure):
+    """sqs_job_result (include/sqs.h)."""
+    _fields_ = [("status", C.c_int32), ("certified", C.c_int32), ("shrinks", C.c_int32),
+                ("improvements", C.c_int32), ("sweeps_done", C.c_int32), ("replicas", C.c_int32),
+                ("L_cert", C.c_double), ("L_polished", C.c_double), ("dilation", C.c_double),
+                ("score", C.c_double), ("proposals", C.c_int64), ("accepted", C.c_int64),
+                ("exchange_attempts", C.c_int64), ("exchange_accepts", C.c_int64), ("device_ms", C.c_double),
+                ("L", C.c_char * 80), ("reason", C.c_char * 112)]
+
+
 # name -> (restype, argtypes)
 SIGNATURES: dict[str, tuple] = {
     "sqs_version": (C.c_char_p, []),
@@ -59,6 +77,8 @@ SIGNATURES: dict[str, tuple] = {
     "sqs_sat_energy": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_int]),
     "sqs_sat_energy_host": (C.c_int, [_vp, C.c_int, C.c_int, _fp, _fp, _fp, _fp, _u32p]),
     "sqs_certify_batch": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, C.c_char_p, _vp, C.c_int, C.POINTER(Verdict)]),
+    "sqs_anneal_batch": (C.c_int, [_vp, C.POINTER(Job), C.c_int, C.c_int, C.POINTER(C.POINTER(C.c_double)),
+                                   C.POINTER(JobResult)]),
 }
 
 _LIB = None

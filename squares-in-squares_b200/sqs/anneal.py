@@ -1,0 +1,88 @@
+"""Anneal-and-certify jobs on the GPU: parallel-tempering annealing of n unit
+squares in a shrinking container, FP64 best-state recompute, FP64 gradient
+polish and interval certification of the best packing, batched.
+
+A job's result depends only on its inputs and seed (counter-based RNG), so it
+is the same whether the job runs alone, in a batch of other jobs, or sliced.
+The result dictionaries carry the fields the reference's search programs
+write into their raw JSON (seeded.cu:949-974, packing.cu:859-865) plus the
+certified side.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as N
+
+MAX_N = 1000
+
+
+@dataclass
+class AnnealJob:
+    xya: np.ndarray                 # (n, 3) initial state: centre x, centre y, angle (radians)
+    L0: float                       # initial container side
+    replicas: int = 8
+    sweeps: int = 1000              # one sweep = n proposals per replica
+    exchange_every: int = 10
+    tmin: float = 1e-3
+    tmax: float = 1e-1
+    sigma_xy: float = 0.02
+    sigma_a: float = 0.05
+    shrink: float = 0.001
+    seed: int = 42
+    polish_iters: int = 200
+    n: int = field(init=False)
+
+    def __post_init__(self):
+        self.xya = np.ascontiguousarray(self.xya, dtype=np.float64).reshape(-1, 3)
+        self.n = self.xya.shape[0]
+
+
+def _cjob(j: AnnealJob) -> N.Job:
+    return N.Job(n=j.n, replicas=j.replicas, sweeps=j.sweeps, exchange_every=j.exchange_every,
+                 polish_iters=j.polish_iters, flags=0, L0=j.L0, tmin=j.tmin, tmax=j.tmax, sigma_xy=j.sigma_xy,
+                 sigma_a=j.sigma_a, shrink=j.shrink, seed=j.seed & 0xFFFFFFFFFFFFFFFF,
+                 xya=j.xya.ctypes.data_as(C.POINTER(C.c_double)))
+
+
+def anneal_batch(jobs: list[AnnealJob], *, ctx: N.Context | None = None, slice_sweeps: int = 0) -> list[dict]:
+    """Run jobs in batched launches; returns one result dict per job."""
+    own = ctx is None
+    ctx = ctx or N.Context(0)
+    try:
+        arr = (N.Job * max(1, len(jobs)))(*[_cjob(j) for j in jobs])
+        res = (N.JobResult * max(1, len(jobs)))()
+        outs = [np.zeros((j.n, 3)) for j in jobs]
+        ptrs = (C.POINTER(C.c_double) * max(1, len(jobs)))(*[o.ctypes.data_as(C.POINTER(C.c_double)) for o in outs])
+        N.check(N.lib().sqs_anneal_batch(ctx.handle, arr, len(jobs), slice_sweeps, ptrs, res))
+    finally:
+        if own:
+            ctx.close()
+    out = []
+    for j, r, q in zip(jobs, res, outs):
+        ok = bool(r.certified)
+        rows = [dict(square_id=str(i), x=format(float(x), ".17g"), y=format(float(y), ".17g"),
+                     angle=format(float(a), ".17g")) for i, (x, y, a) in enumerate(q)] if ok else None
+        out.append(dict(
+            n=j.n, status=int(r.status), certified=ok, L=r.L.decode() if ok else None,
+            reason=r.reason.decode(), target_L=float(r.L_cert), L_cert=float(r.L_cert),
+            L_polished=float(r.L_polished), dilation=float(r.dilation), score=float(r.score),
+            shrinks=int(r.shrinks), improvements=int(r.improvements), sweeps=int(r.sweeps_done),
+            chains=int(r.replicas), proposals=int(r.proposals), accepted=int(r.accepted),
+            exchange_attempts=int(r.exchange_attempts), exchange_accepts=int(r.exchange_accepts),
+            device_ms=float(r.device_ms), q=q.tolist() if ok else None, rows=rows))
+    return out
+
+
+def jittered_grid(n: int, jitter: float = 0.05, angle_hi: float = 0.1, seed: int = 42):
+    """Grid centres at half-integers (ceil(sqrt n) columns) plus uniform jitter
+    and small angles: the plain single-instance configuration's start."""
+    rng = np.random.default_rng(seed)
+    w = math.isqrt(n - 1) + 1
+    i = np.arange(n)
+    xy = np.stack([i % w + 0.5, i // w + 0.5], axis=1) + rng.uniform(-jitter, jitter, (n, 2))
+    return np.concatenate([xy, rng.uniform(0.0, angle_hi, (n, 1))], axis=1), float(w)
