@@ -111,6 +111,25 @@ int sqs_certify_batch(sqs_ctx* ctx, int count, const int32_t* n_of, const int64_
                       const int32_t* square_id, const char* text, const int64_t* lit_off, int flags,
                       sqs_verdict* out);
 
+/* Allocation-free form of sqs_certify_batch, for callers that cannot
+ * allocate GPU memory while they run: a host that owns all device memory
+ * through its own pool, or a latency-critical loop that forbids allocation
+ * after start-up.  No counterpart in the reference, which always certifies
+ * on the CPU.  Same arguments, results and errors as sqs_certify_batch, but
+ * it calls no cudaMalloc, cudaFree or other allocating routine: all device
+ * scratch is one static array of about 7.6 MiB that every device holds from
+ * library load until process exit, and host staging is static too.  Limits
+ * per call: 4,096 packings, 16,384 squares, 2 MiB of literal text (and, with
+ * SQS_CERT_ROUNDTRIP, literals under 4,096 bytes); larger calls fail with
+ * SQS_EINVAL.  The first call on a device looks up the array's device
+ * address and uploads constants, so make that first call before any stream
+ * capture.  The scratch keeps the last call's contents (what must start at
+ * zero is cleared on entry); calls that overlap -- from several threads, or
+ * on several contexts of one device -- race on it and must not be issued. */
+int sqs_certify_batch_static(sqs_ctx* ctx, int count, const int32_t* n_of, const int64_t* row_start,
+                             const int32_t* square_id, const char* text, const int64_t* lit_off, int flags,
+                             sqs_verdict* out);
+
 /* ------------------------------------------------ annealing + polish */
 /* One anneal-and-certify job: parallel tempering of n unit squares in a
  * container that shrinks after every new best state.  The job's whole

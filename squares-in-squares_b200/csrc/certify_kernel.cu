@@ -891,3 +891,254 @@ extern "C" int sqs_certify_batch(sqs_ctx* ctx, int count, const int32_t* n_of, c
     }
     return SQS_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free certification: the same kernels, with every device buffer
+// carved from one file-scope array and every host buffer static.  For callers
+// that must not allocate device memory at run time -- a host that owns all
+// GPU memory through its own pool, a real-time loop that forbids allocation
+// after start-up -- at the price of fixed limits and of a process-wide
+// buffer that concurrent calls share.
+namespace sqs {
+namespace cert {
+
+constexpr int kStaticMaxSquares = 16384;
+constexpr int kStaticMaxPackings = 4096;
+constexpr size_t kStaticMaxText = 2u << 20;               // literal bytes per call
+constexpr uint32_t kStaticPairCap = 16u * kStaticMaxSquares + 4096u;
+
+constexpr size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
+constexpr size_t kSoText = 0;
+constexpr size_t kSoOff = kSoText + al256(kStaticMaxText);
+constexpr size_t kSoLen = kSoOff + al256(sizeof(int64_t) * 3 * kStaticMaxSquares);
+constexpr size_t kSoN = kSoLen + al256(sizeof(int32_t) * 3 * kStaticMaxSquares);
+constexpr size_t kSoS0 = kSoN + al256(sizeof(int32_t) * kStaticMaxPackings);
+constexpr size_t kSoBk = kSoS0 + al256(sizeof(int64_t) * kStaticMaxPackings);
+constexpr size_t kSoLits = kSoBk + al256(sizeof(int32_t) * kStaticMaxPackings);
+constexpr size_t kSoOut = kSoLits + al256(sizeof(Lit) * 3 * kStaticMaxSquares);
+constexpr size_t kSoPa = kSoOut + al256(sizeof(PkOut) * kStaticMaxPackings);
+constexpr size_t kSoPb = kSoPa + al256(sizeof(Pair) * kStaticPairCap);
+constexpr size_t kSoCnt = kSoPb + al256(sizeof(Pair) * kStaticPairCap);
+constexpr size_t kStaticScratchBytes = kSoCnt + 256;  // about 7.6 MiB
+
+// The scratch every call of sqs_certify_batch_static shares.  In host code
+// this name is only a stand-in: the device address comes from
+// cudaGetSymbolAddress, taken once per device.
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+static void* s_scratch_addr[64] = {nullptr};
+
+// Host staging (static, not heap): literal slices in square-id order, packing
+// tables, round-tripped literals, the per-packing records read back.
+static int64_t s_raw_off[3 * kStaticMaxSquares];
+static int32_t s_raw_len[3 * kStaticMaxSquares];
+static int32_t s_pk_n[kStaticMaxPackings];
+static int64_t s_pk_sq0[kStaticMaxPackings];
+static int32_t s_bucket[kStaticMaxPackings];
+static unsigned char s_live[kStaticMaxPackings];
+static int64_t s_row_of[kMaxN];
+static char s_rt_text[kStaticMaxText];
+static char s_lit_tmp[4096];
+static PkOut s_out[kStaticMaxPackings];
+
+static void fifty_into(const Fix<9>& v, char* dst, size_t cap) {
+    const uint64_t B = 1000000000ULL;
+    uint64_t low = v.d[6] % 10000ULL, top = v.d[6] / 10000ULL;
+    const bool tail = v.d[7] || v.d[8] || v.d[9];
+    const bool up = low > 5000ULL || (low == 5000ULL && (tail || (top & 1ULL)));
+    uint64_t o[7] = {v.d[0], v.d[1], v.d[2], v.d[3], v.d[4], v.d[5], top};
+    if (up && ++o[6] >= 100000ULL) {
+        o[6] -= 100000ULL;
+        int i = 5;
+        for (; i >= 1; --i) {
+            if (++o[i] < B) break;
+            o[i] -= B;
+        }
+        if (i < 1) o[0] += 1;
+    }
+    bool allz = true;
+    for (uint64_t w : o) allz &= w == 0;
+    std::snprintf(dst, cap, "%s%llu.%09llu%09llu%09llu%09llu%09llu%05llu", (v.neg && !allz) ? "-" : "",
+                  (unsigned long long)o[0], (unsigned long long)o[1], (unsigned long long)o[2],
+                  (unsigned long long)o[3], (unsigned long long)o[4], (unsigned long long)o[5],
+                  (unsigned long long)o[6]);
+}
+
+}  // namespace cert
+}  // namespace sqs
+
+extern "C" int sqs_certify_batch_static(sqs_ctx* ctx, int count, const int32_t* n_of, const int64_t* row_start,
+                                        const int32_t* square_id, const char* text, const int64_t* lit_off,
+                                        int flags, sqs_verdict* out) {
+    if (int r = enter(ctx)) return r;
+    SQS_REQUIRE(count >= 0 && count <= kStaticMaxPackings, "count %d out of 0..%d (static certifier limit)", count,
+                kStaticMaxPackings);
+    if (count == 0) return SQS_OK;
+    SQS_REQUIRE(n_of && row_start && text && lit_off && out, "null host pointer");
+    const int dev = ctx->device & 63;
+    if (!s_scratch_addr[dev]) {  // once per device, with that device current (sqs::enter)
+        void* p = nullptr;
+        SQS_CUDA(cudaGetSymbolAddress(&p, g_static_scratch));
+        s_scratch_addr[dev] = p;
+    }
+    if (int r = upload_consts(ctx->device)) return r;
+    const bool do_rt = (flags & SQS_CERT_ROUNDTRIP) != 0;
+    // envelope checks and literal slices, as sqs_certify_batch does them
+    int64_t S = 0;
+    size_t rt_used = 0;
+    for (int p = 0; p < count; ++p) {
+        const int n = n_of[p];
+        sqs_verdict& v = out[p];
+        std::memset(&v, 0, sizeof v);
+        v.n = n;
+        s_live[p] = 0;
+        SQS_REQUIRE(n >= 1 && n <= kMaxN, "packing %d: n=%d out of 1..%d", p, n, kMaxN);
+        v.score = grid_score(n);
+        const int64_t r0 = row_start[p], r1 = row_start[p + 1];
+        SQS_REQUIRE(r1 >= r0, "packing %d: row_start not monotone", p);
+        if (r1 - r0 != n) {
+            std::snprintf(v.reason, sizeof v.reason, "n=%d: expected %d rows, got %lld", n, n, (long long)(r1 - r0));
+            continue;
+        }
+        for (int i = 0; i < n; ++i) s_row_of[i] = -1;
+        bool bad = false;
+        for (int64_t r = r0; r < r1 && !bad; ++r) {
+            const int sid = square_id ? square_id[r] : (int)(r - r0);
+            if (sid < 0 || sid >= n || s_row_of[sid] >= 0) bad = true;
+            else s_row_of[sid] = r;
+        }
+        if (bad) {
+            std::snprintf(v.reason, sizeof v.reason, "n=%d: square_ids should be 0..%d", n, n - 1);
+            continue;
+        }
+        SQS_REQUIRE(S + n <= kStaticMaxSquares, "more than %d squares in one static-certifier call",
+                    kStaticMaxSquares);
+        s_live[p] = 1;
+        s_pk_n[p] = n;
+        s_pk_sq0[p] = S;
+        for (int i = 0; i < n; ++i) {
+            const int64_t r = s_row_of[i];
+            for (int k = 0; k < 3; ++k) {
+                const int64_t a = lit_off[3 * r + k], b = lit_off[3 * r + k + 1];
+                SQS_REQUIRE(b >= a, "literal offsets not monotone at row %lld", (long long)r);
+                const int64_t q = 3 * (S + i) + k;
+                if (do_rt) {
+                    SQS_REQUIRE((size_t)(b - a) < sizeof(s_lit_tmp), "literal longer than %zu bytes",
+                                sizeof(s_lit_tmp) - 1);
+                    std::memcpy(s_lit_tmp, text + a, (size_t)(b - a));
+                    s_lit_tmp[b - a] = 0;
+                    const double val = std::strtod(s_lit_tmp, nullptr);
+                    char buf[40];
+                    for (int prec = 15; prec <= 17; ++prec) {
+                        std::snprintf(buf, sizeof buf, "%.*g", prec, val);
+                        if (std::strtod(buf, nullptr) == val) break;
+                    }
+                    size_t len = std::strlen(buf);
+                    const bool plain = std::strpbrk(buf, ".eE") == nullptr;
+                    SQS_REQUIRE(rt_used + len + 2 <= kStaticMaxText, "literals exceed %zu bytes", kStaticMaxText);
+                    std::memcpy(s_rt_text + rt_used, buf, len);
+                    if (plain) {
+                        std::memcpy(s_rt_text + rt_used + len, ".0", 2);
+                        len += 2;
+                    }
+                    s_raw_off[q] = (int64_t)rt_used;
+                    s_raw_len[q] = (int32_t)len;
+                    rt_used += len;
+                } else {
+                    s_raw_off[q] = a;
+                    s_raw_len[q] = (int32_t)std::min<int64_t>(b - a, 1 << 20);
+                }
+            }
+        }
+        S += n;
+    }
+    const size_t text_bytes = do_rt ? rt_used : (size_t)lit_off[3 * row_start[count]];
+    SQS_REQUIRE(text_bytes <= kStaticMaxText, "literals exceed %zu bytes (static certifier limit)", kStaticMaxText);
+    int nb[3] = {0, 0, 0};
+    for (int p = 0; p < count; ++p)
+        if (s_live[p]) ++nb[s_pk_n[p] <= 64 ? 0 : (s_pk_n[p] <= 256 ? 1 : 2)];
+    int fill[3] = {0, nb[0], nb[0] + nb[1]};
+    for (int p = 0; p < count; ++p) {
+        if (!s_live[p]) continue;
+        const int b = s_pk_n[p] <= 64 ? 0 : (s_pk_n[p] <= 256 ? 1 : 2);
+        s_bucket[fill[b]++] = p;
+    }
+    char* D = (char*)s_scratch_addr[dev];
+    cudaStream_t st = ctx->stream;
+    if (text_bytes)
+        SQS_CUDA(cudaMemcpyAsync(D + kSoText, do_rt ? s_rt_text : text, text_bytes, cudaMemcpyHostToDevice, st));
+    SQS_CUDA(cudaMemcpyAsync(D + kSoOff, s_raw_off, sizeof(int64_t) * 3 * (size_t)S, cudaMemcpyHostToDevice, st));
+    SQS_CUDA(cudaMemcpyAsync(D + kSoLen, s_raw_len, sizeof(int32_t) * 3 * (size_t)S, cudaMemcpyHostToDevice, st));
+    SQS_CUDA(cudaMemcpyAsync(D + kSoN, s_pk_n, sizeof(int32_t) * (size_t)count, cudaMemcpyHostToDevice, st));
+    SQS_CUDA(cudaMemcpyAsync(D + kSoS0, s_pk_sq0, sizeof(int64_t) * (size_t)count, cudaMemcpyHostToDevice, st));
+    SQS_CUDA(cudaMemcpyAsync(D + kSoBk, s_bucket, sizeof(int32_t) * (size_t)(nb[0] + nb[1] + nb[2]),
+                             cudaMemcpyHostToDevice, st));
+    // the shared scratch keeps the previous call's contents: clear what starts at zero
+    SQS_CUDA(cudaMemsetAsync(D + kSoOut, 0, sizeof(PkOut) * (size_t)count, st));
+    SQS_CUDA(cudaMemsetAsync(D + kSoCnt, 0, 64, st));
+    const char* d_text = D + kSoText;
+    const int64_t* d_off = (const int64_t*)(D + kSoOff);
+    const int32_t* d_len = (const int32_t*)(D + kSoLen);
+    const int32_t* d_n = (const int32_t*)(D + kSoN);
+    const int64_t* d_s0 = (const int64_t*)(D + kSoS0);
+    const int32_t* d_bk = (const int32_t*)(D + kSoBk);
+    Lit* d_lits = (Lit*)(D + kSoLits);
+    PkOut* d_out = (PkOut*)(D + kSoOut);
+    Pair* pa = (Pair*)(D + kSoPa);
+    Pair* pb = (Pair*)(D + kSoPb);
+    uint32_t* cnt = (uint32_t*)(D + kSoCnt);
+    const uint32_t cap = kStaticPairCap;
+    if (int r = launch_packing<64, 64>(ctx, nb[0], d_bk, d_n, d_s0, d_text, d_off, d_len, d_lits, d_out, pa, cnt, cap))
+        return r;
+    if (int r = launch_packing<128, 256>(ctx, nb[1], d_bk + nb[0], d_n, d_s0, d_text, d_off, d_len, d_lits, d_out,
+                                         pa, cnt, cap))
+        return r;
+    if (int r = launch_packing<256, 1024>(ctx, nb[2], d_bk + nb[0] + nb[1], d_n, d_s0, d_text, d_off, d_len, d_lits,
+                                          d_out, pa, cnt, cap))
+        return r;
+    const int blocks = ctx->sm_count * 8;
+    if (int r = launch_stage<7>(ctx, pa, cnt, cap, pb, cnt + 1, cap, d_s0, d_lits, d_text, d_out, blocks)) return r;
+    if (int r = launch_stage<15>(ctx, pb, cnt + 1, cap, pa, cnt + 2, cap, d_s0, d_lits, d_text, d_out, blocks))
+        return r;
+    if (int r = launch_stage<58>(ctx, pa, cnt + 2, cap, nullptr, nullptr, 0, d_s0, d_lits, d_text, d_out, blocks))
+        return r;
+    SQS_CUDA(cudaMemcpyAsync(s_out, d_out, sizeof(PkOut) * (size_t)count, cudaMemcpyDeviceToHost, st));
+    SQS_CUDA(cudaStreamSynchronize(st));
+    static const char* what[4] = {"cannot parse coordinates", "value out of range for a double",
+                                  "coordinate out of bounds", "angle out of bounds"};
+    for (int p = 0; p < count; ++p) {
+        if (!s_live[p]) continue;
+        sqs_verdict& v = out[p];
+        const PkOut& o = s_out[p];
+        const int n = s_pk_n[p];
+        if (o.flags & kPairOverflow) {
+            set_error("packing %d: undecided-pair list overflowed", p);
+            return SQS_ENOMEM;
+        }
+        if (o.err_key != kNoKey) {
+            std::snprintf(v.reason, sizeof v.reason, "n=%d, square %u: %s", n, o.err_key / 4, what[o.err_key % 4]);
+            continue;
+        }
+        if (o.fkey != kNoPair) {
+            std::snprintf(v.reason, sizeof v.reason, "infeasible: Squares %d and %d overlap (float check)", o.fu, o.fv);
+            continue;
+        }
+        if (o.flags & kCertOverlap) {
+            std::snprintf(v.reason, sizeof v.reason, "infeasible: Squares overlap (certified)");
+            continue;
+        }
+        if (o.flags & kUndecidable) {
+            std::snprintf(v.reason, sizeof v.reason, "infeasible: Overlap undecidable at max precision");
+            continue;
+        }
+        const double sf = fx::approx(o.side), lb = std::sqrt((double)n);
+        if (sf < lb - 1e-7) {
+            std::snprintf(v.reason, sizeof v.reason, "infeasible: L is below area lower bound");
+            continue;
+        }
+        v.ok = 1;
+        std::snprintf(v.reason, sizeof v.reason, "ok");
+        fifty_into(o.side, v.L, sizeof v.L);
+        v.score = std::max(0.0, sf / lb - 1.0);
+    }
+    return SQS_OK;
+}

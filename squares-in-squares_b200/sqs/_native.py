@@ -77,6 +77,8 @@ SIGNATURES: dict[str, tuple] = {
     "sqs_sat_energy": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_int]),
     "sqs_sat_energy_host": (C.c_int, [_vp, C.c_int, C.c_int, _fp, _fp, _fp, _fp, _u32p]),
     "sqs_certify_batch": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, C.c_char_p, _vp, C.c_int, C.POINTER(Verdict)]),
+    "sqs_certify_batch_static": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, C.c_char_p, _vp, C.c_int,
+                                           C.POINTER(Verdict)]),
     "sqs_anneal_batch": (C.c_int, [_vp, C.POINTER(Job), C.c_int, C.c_int, C.POINTER(C.POINTER(C.c_double)),
                                    C.POINTER(JobResult)]),
 }
