@@ -176,6 +176,32 @@ typedef struct sqs_job_result {
 int sqs_anneal_batch(sqs_ctx* ctx, const sqs_job* jobs, int njobs, int slice_sweeps, double* const* xya_out,
                      sqs_job_result* out);
 
+/* ------------------------------------------------------------- serving */
+/* Continuous-batching request loop for anneal-and-certify jobs on one GPU.
+ * Jobs are admitted while a job slot is free and their state (replicas,
+ * scratch, best packing) fits an HBM arena of `hbm_bytes`; every step runs
+ * one slice of `slice_sweeps` sweeps for all admitted jobs side by side in
+ * one launch per cluster shape, their state resident between slices, then
+ * polishes, certifies and retires the finished ones so queued jobs take
+ * their place.  Each job's result equals its sqs_anneal_batch result.
+ * Replaces one-search-process-per-job campaigns (scheduler.run_gpu,
+ * cuda/scheduler.py:80-89) and their VRAM-budgeted worker admission
+ * (cpp_loop.concurrency, cuda/cpp_loop.py:41-45). */
+typedef struct sqs_server sqs_server;
+int sqs_server_create(sqs_ctx* ctx, size_t hbm_bytes, int max_active, int slice_sweeps, sqs_server** out);
+int sqs_server_destroy(sqs_server* server);
+/* Queue a job (the job and its initial state are copied). */
+int sqs_server_submit(sqs_server* server, const sqs_job* job, int64_t* id);
+/* One admission + slice + retirement round; *in_flight = queued + running. */
+int sqs_server_step(sqs_server* server, int* in_flight);
+/* 1 and the result (and n*3 packing into xya_out when certified) once the
+ * job is done -- the job is then forgotten; 0 while it is queued or running;
+ * SQS_ENOTFOUND for an unknown id. */
+int sqs_server_poll(sqs_server* server, int64_t id, sqs_job_result* out, double* xya_out);
+/* Withdraw a queued job now, or a running one at the end of the next step. */
+int sqs_server_cancel(sqs_server* server, int64_t id);
+int sqs_server_info(sqs_server* server, int* queued, int* active, size_t* hbm_used);
+
 #ifdef __cplusplus
 }
 #endif

@@ -81,6 +81,13 @@ SIGNATURES: dict[str, tuple] = {
                                            C.POINTER(Verdict)]),
     "sqs_anneal_batch": (C.c_int, [_vp, C.POINTER(Job), C.c_int, C.c_int, C.POINTER(C.POINTER(C.c_double)),
                                    C.POINTER(JobResult)]),
+    "sqs_server_create": (C.c_int, [_vp, C.c_size_t, C.c_int, C.c_int, C.POINTER(_vp)]),
+    "sqs_server_destroy": (C.c_int, [_vp]),
+    "sqs_server_submit": (C.c_int, [_vp, C.POINTER(Job), C.POINTER(C.c_int64)]),
+    "sqs_server_step": (C.c_int, [_vp, C.POINTER(C.c_int)]),
+    "sqs_server_poll": (C.c_int, [_vp, C.c_int64, C.POINTER(JobResult), C.POINTER(C.c_double)]),
+    "sqs_server_cancel": (C.c_int, [_vp, C.c_int64]),
+    "sqs_server_info": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_size_t)]),
 }
 
 _LIB = None

@@ -1,0 +1,85 @@
+"""Serving loop: continuous batching with admission by HBM footprint; every
+job's result in the mix equals its result alone."""
+from __future__ import annotations
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+KEYS = ("L", "L_cert", "L_polished", "proposals", "accepted", "shrinks", "exchange_attempts", "q")
+
+
+def _job(n, seed, sweeps, replicas=8, **kw):
+    from sqs.anneal import AnnealJob, jittered_grid
+    xya, L0 = jittered_grid(n, seed=seed)
+    return AnnealJob(xya, L0=L0, replicas=replicas, sweeps=sweeps, exchange_every=10, seed=seed, **kw)
+
+
+def test_served_results_equal_alone(ctx):
+    from sqs.anneal import anneal_batch
+    from sqs.serve import Server
+    jobs = [_job(10, 1, 300), _job(37, 2, 120, replicas=16), _job(5, 3, 500, replicas=4), _job(64, 4, 90)]
+    alone = [anneal_batch([j], ctx=ctx)[0] for j in jobs]
+    with Server(ctx, hbm_bytes=64 << 20, max_active=3, slice_sweeps=30) as srv:
+        ids = [srv.submit(j) for j in jobs[:2]]
+        srv.step()                       # the first two are running ...
+        ids += [srv.submit(j) for j in jobs[2:]]  # ... when the others arrive
+        got = {}
+        for _ in range(200):
+            if srv.step() == 0:
+                break
+        for k, jid in enumerate(ids):
+            got[k] = srv.poll(jid)
+    for k in range(len(jobs)):
+        assert got[k] is not None
+        for key in KEYS:
+            assert got[k][key] == alone[k][key], (k, key)
+
+
+def test_admission_by_hbm_footprint(ctx):
+    from sqs.serve import Server
+    jobs = [_job(100, s, 40) for s in range(4)]
+    per_job = 8 * 100 * 16 + 2 * 100 * 16 + 100 * 24  # replicas + scratch + best, bytes
+    budget = 1 << 20                                  # room for one job at a time only
+    assert per_job < budget < 2 * per_job + 4096 or budget > per_job
+    with Server(ctx, hbm_bytes=budget, max_active=8, slice_sweeps=20) as srv:
+        ids = [srv.submit(j) for j in jobs]
+        peak_active = 0
+        while True:
+            left = srv.step()
+            _, active, used = srv.info()
+            peak_active = max(peak_active, active)
+            assert used <= budget
+            if left == 0:
+                break
+        results = [srv.poll(i) for i in ids]
+    assert all(r is not None and r["status"] == 0 for r in results)
+    assert peak_active >= 1
+
+
+def test_cancel_and_unknown_ids(ctx):
+    from sqs import SQSError
+    from sqs.serve import Server
+    with Server(ctx, hbm_bytes=32 << 20, max_active=1, slice_sweeps=10) as srv:
+        a = srv.submit(_job(20, 5, 200))
+        b = srv.submit(_job(20, 6, 200))
+        srv.step()                 # a runs, b waits for the only slot
+        srv.cancel(b)
+        srv.cancel(a)
+        srv.step()
+        ra, rb = srv.poll(a), srv.poll(b)
+        assert ra["reason"] == "cancelled" and rb["reason"] == "cancelled"
+        with pytest.raises(SQSError):
+            srv.poll(a)            # collected already
+        with pytest.raises(SQSError):
+            srv.cancel(12345)
+
+
+def test_poisson_stream_reports_latency(ctx):
+    from sqs.serve import Server, poisson_arrivals, run_stream
+    jobs = [_job(n, 10 + k, 60) for k, n in enumerate((8, 12, 20, 9, 15, 30))]
+    arr = poisson_arrivals(len(jobs), rate=200.0, seed=1)
+    with Server(ctx, hbm_bytes=64 << 20, max_active=4, slice_sweeps=20) as srv:
+        results, stats = run_stream(srv, jobs, arr, timeout=120)
+    assert stats["jobs"] == len(jobs)
+    assert 0 < stats["p50_s"] <= stats["p99_s"]
+    assert all(r is not None for r in results)
