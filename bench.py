@@ -298,6 +298,7 @@ def run_sqs(args, D: Dist):
     d2h = configs * 4 + x32.nbytes
 
     peak, peak_kind = peaks()
+    kernel_name = "sat_energy_warp_kernel" if (threads <= 0 and n <= 256) else "sat_energy_kernel"
     algo = algorithmic_bytes(configs, n)
     achieved = algo / (mean_ms / 1e3) / 1e9
     line = dict(
@@ -310,8 +311,8 @@ def run_sqs(args, D: Dist):
         e2e=dict(value=e2e_val, unit=UNIT, h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h,
                  steps=e2e_steps, call="sqs_sat_energy_host (pinned host buffers)"),
         roofline=dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
-                      traffic=ncu_traffic("sat_energy_kernel"), peak_kind=peak_kind,
-                      algorithmic_bytes_per_launch=algo, kernel="sat_energy_kernel"),
+                      traffic=ncu_traffic(kernel_name), peak_kind=peak_kind,
+                      algorithmic_bytes_per_launch=algo, kernel=kernel_name),
         gpu_launches=launches,
         pairs_per_step=pairs_per_step,
         clocks=clk,
@@ -319,6 +320,11 @@ def run_sqs(args, D: Dist):
     if D.rank == 0 and D.world == 1 and not args.no_cpu_baseline:
         val, kind, cores, sample, _, _ = cpu_pairs_per_s(x32, s32, args.cpu_seconds)
         line["cpu_baseline"] = dict(value=val, unit=UNIT, cores=cores, kind=kind, sample=sample)
+    if D.rank == 0 and D.world == 1 and not args.no_extras:
+        line["certify"] = bench_certify(ctx, args.cpu_seconds)
+        line["served"] = bench_served_sweep(ctx, args.served_rates)
+        line["plain_pt"] = bench_plain_pt(ctx)
+        line["batched"] = bench_batched(ctx)
     for d in (d_x, d_s, d_e, d_g, d_c):
         d.free()
     for h in (hin, hs, he, hg):
@@ -326,6 +332,131 @@ def run_sqs(args, D: Dist):
     ctx.close()
     if D.rank == 0:
         print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ extras
+def bench_certify(ctx, cpu_seconds: float, count: int = 10000):
+    """The interval-certifier batch: 10,000 packings, n log-uniform in
+    [5, 1000], half exact grids, half tilted near-contact lattices, 5% with
+    injected 1e-10 overlaps; GPU end to end from host strings vs the
+    reference certifier (certifier.cpp) on all host cores."""
+    import numpy as np
+
+    from sqs import core
+    from sqs.workloads import certify_corpus
+
+    items = certify_corpus(count, seed=42)
+    arrs = core.pack_batch(items)
+    squares = int(sum(n for n, _ in items))
+    core.certify_arrays(*arrs, ctx=ctx)  # warm-up (first-use set-up)
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        out = core.certify_arrays(*arrs, ctx=ctx)
+        times.append(time.perf_counter() - t0)
+    gpu_s = min(times)
+    gpu_ok = np.array([out[k].ok for k in range(count)], np.int32)
+    res = dict(workload=f"{count} packings, {squares} squares, n log-uniform [5, 1000]",
+               packings_per_s=count / gpu_s, squares_per_s=squares / gpu_s, seconds=gpu_s,
+               accepted=int(gpu_ok.sum()), call="sqs_certify_batch (host strings in, verdicts out)")
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    which = "ref" if O.ref_available() else "oracle"
+    # bounded CPU sample: packings in corpus order until ~cpu_seconds of work
+    k, t0, done, agree = 0, time.perf_counter(), 0, True
+    while k < count and time.perf_counter() - t0 < cpu_seconds:
+        sub = items[k:k + 64]
+        ok, _, used = O.certify_batch(*core.pack_batch(sub), which=which)
+        agree &= bool(np.array_equal(ok, gpu_ok[k:k + len(sub)]))
+        done += len(sub)
+        k += len(sub)
+    cpu_s = time.perf_counter() - t0
+    res["cpu_baseline"] = dict(packings_per_s=done / cpu_s, cores=used,
+                               kind="reference" if which == "ref" else "port",
+                               sample=f"first {done} packings of the batch")
+    res["verdicts_equal_on_sample"] = agree
+    res["speedup_vs_cpu"] = res["packings_per_s"] / res["cpu_baseline"]["packings_per_s"]
+    return res
+
+
+def bench_served(ctx, count: int = 48, rate: float = 200.0):
+    """Served vs plain: a Poisson stream of anneal-and-certify jobs (n
+    log-uniform in [5, 64], 16 replicas, 300 sweeps each -- a bounded budget so
+    the run ends in seconds) through the continuous-batching server, and the
+    same jobs one launch per job; same final L by construction, checked."""
+    import math
+
+    import numpy as np
+
+    from sqs.anneal import AnnealJob, jittered_grid
+    from sqs.serve import Server, poisson_arrivals, run_plain, run_stream
+
+    rng = np.random.default_rng(7)
+    jobs = []
+    for k in range(count):
+        n = int(round(math.exp(rng.uniform(math.log(5), math.log(64)))))
+        xya, L0 = jittered_grid(n, seed=100 + k)
+        jobs.append(AnnealJob(xya, L0=L0, replicas=16, sweeps=300, exchange_every=10, tmin=1e-3, tmax=1e-1,
+                              seed=1000 + k, polish_iters=100))
+    arr = poisson_arrivals(count, rate, seed=3)
+    with Server(ctx, hbm_bytes=1 << 30, max_active=count, slice_sweeps=50) as srv:
+        served, s_stats = run_stream(srv, jobs, arr, timeout=300)
+    plain, p_stats = run_plain(ctx, jobs, arr)
+    same_L = all((a or {}).get("L") == (b or {}).get("L") for a, b in zip(served, plain))
+    return dict(workload=f"{count} jobs, Poisson {rate:g}/s, n log-uniform [5, 64], 16 replicas, 300 sweeps",
+                served=s_stats, plain=p_stats, equal_final_L=same_L,
+                served_over_plain=s_stats["certified_jobs_per_s"] / max(p_stats["certified_jobs_per_s"], 1e-12))
+
+
+def bench_plain_pt(ctx):
+    """The plain single-instance PT-SA job: n=10, L0=4, grid + U(+-0.05)
+    jitter and U[0, 0.1) angles from seed 42, 8 replicas on 1e-3..1e-1,
+    20,000 sweeps, shrink 0.1% per improvement, FP64 polish, certification."""
+    from sqs.anneal import AnnealJob, anneal_batch, jittered_grid
+
+    xya, _ = jittered_grid(10, seed=42)
+    job = AnnealJob(xya, L0=4.0, replicas=8, sweeps=20000, exchange_every=10, tmin=1e-3, tmax=1e-1, seed=42)
+    t0 = time.perf_counter()
+    r = anneal_batch([job], ctx=ctx)[0]
+    dt = time.perf_counter() - t0
+    return dict(workload="n=10, 8 replicas, 20,000 sweeps", seconds=dt, certified=r["certified"], L=r["L"],
+                proposals=r["proposals"], proposals_per_s=r["proposals"] / dt, shrinks=r["shrinks"])
+
+
+def bench_served_sweep(ctx, rates: str):
+    out = {}
+    for r in [float(x) for x in rates.split(",") if x]:
+        out[f"{r:g}/s"] = bench_served(ctx, rate=r)
+    return out
+
+
+def bench_batched(ctx, sweeps: int = 50, instances: int = 512):
+    """Batched PT-SA, one launch: 512 instances, n uniform in [20, 400]
+    (seeded), 32 replicas on 1e-4..5e-2, sigma 0.02 / 0.05 rad, exchange every
+    10 sweeps, FP64 recompute of each best; a bounded sweep budget."""
+    import math
+
+    import numpy as np
+
+    from sqs.anneal import AnnealJob, anneal_batch, jittered_grid
+
+    rng = np.random.default_rng(42)
+    jobs = []
+    for k in range(instances):
+        n = int(rng.integers(20, 401))
+        xya, L0 = jittered_grid(n, seed=k)
+        jobs.append(AnnealJob(xya, L0=L0, replicas=32, sweeps=sweeps, exchange_every=10, tmin=1e-4, tmax=5e-2,
+                              sigma_xy=0.02, sigma_a=0.05, seed=k, polish_iters=0))
+    anneal_batch(jobs[:4], ctx=ctx)  # warm-up
+    t0 = time.perf_counter()
+    res = anneal_batch(jobs, ctx=ctx)
+    dt = time.perf_counter() - t0
+    props = sum(r["proposals"] for r in res)
+    dev_s = res[0]["device_ms"] / 1e3
+    return dict(workload=f"{instances} instances, n U[20,400], 32 replicas, {sweeps} sweeps",
+                proposals=props, seconds=dt, device_seconds=dev_s, proposals_per_s=props / dev_s,
+                squares=int(sum(j.n for j in jobs)) * 32, certified=sum(r["certified"] for r in res))
 
 
 def main():
@@ -337,7 +468,24 @@ def main():
     ap.add_argument("--threads", type=int, default=0, help="CTA width (0 = library default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the certifier / served / plain-PT / batched sections")
+    ap.add_argument("--section", choices=("certify", "served", "plain_pt", "batched"),
+                    help="run only this extra section (for profiling) and print its dict")
+    ap.add_argument("--batched-instances", type=int, default=512)
+    ap.add_argument("--batched-sweeps", type=int, default=50)
+    ap.add_argument("--served-rates", default="50,200,1000")
     args = ap.parse_args()
+    if args.section:
+        from sqs import Context
+
+        with Context(int(os.environ.get("LOCAL_RANK", 0))) as ctx:
+            fn = dict(certify=lambda: bench_certify(ctx, args.cpu_seconds),
+                      served=lambda: bench_served_sweep(ctx, args.served_rates),
+                      plain_pt=lambda: bench_plain_pt(ctx),
+                      batched=lambda: bench_batched(ctx, args.batched_sweeps, args.batched_instances))[args.section]
+            print(json.dumps({args.section: fn()}), flush=True)
+        return
     if args.warmup < 3:
         args.warmup = 3
     D = Dist()

@@ -78,8 +78,10 @@ int64_t sqs_launch_count(sqs_ctx* ctx);
  * The energy model is the reference's total_cached (seeded.cu:148-162) with
  * pair_cached (seeded.cu:41-65) and boundary (seeded.cu:96-113); the gradient
  * is the sum over pairs of d pair / d square plus the boundary gradient, as
- * the reference's polish assembles it (seeded.cu:637-650).  `threads` is the
- * CTA width (32, 64, 128 or 256; 0 = chosen by n). */
+ * the reference's polish assembles it (seeded.cu:637-650).  `threads`
+ * selects the kernel: 0 = chosen by n; 32, 64, 128 or 256 = one CTA of that
+ * width per configuration; -2, -4 or -8 = one warp per configuration with
+ * that many warps per CTA (n <= 256). */
 int sqs_sat_energy(sqs_ctx* ctx, int configs, int n, const float* xya, const float* side,
                    float* energy, float* grad, uint32_t* cand, int threads);
 /* The same with host buffers: copies in, launches, copies out, synchronises. */

@@ -756,3 +756,41 @@ void sqo_roundtrip(const char* s, char* out, int cap) {
 }
 
 }  // extern "C"
+
+#include <atomic>
+#include <thread>
+
+// Batch form of sqo_certify, threaded over packings (the layout of
+// ref_evaluate_batch in ref_certifier.cpp).
+extern "C" int sqo_certify_batch(int count, const int* n_of, const long long* row_start, const int* sid,
+                                 const char* text, const long long* lit_off, int threads, int* ok_out,
+                                 double* score_out) {
+    std::atomic<int> next{0};
+    auto work = [&]() {
+        for (int p = next.fetch_add(1); p < count; p = next.fetch_add(1)) {
+            const long long r0 = row_start[p], rows = row_start[p + 1] - r0;
+            std::vector<std::string> xs, ys, as;
+            std::vector<int> ids;
+            for (long long r = r0; r < r0 + rows; ++r) {
+                ids.push_back(sid ? sid[r] : (int)(r - r0));
+                xs.emplace_back(text + lit_off[3 * r], (size_t)(lit_off[3 * r + 1] - lit_off[3 * r]));
+                ys.emplace_back(text + lit_off[3 * r + 1], (size_t)(lit_off[3 * r + 2] - lit_off[3 * r + 1]));
+                as.emplace_back(text + lit_off[3 * r + 2], (size_t)(lit_off[3 * r + 3] - lit_off[3 * r + 2]));
+            }
+            std::vector<const char*> px, py, pa;
+            for (long long k = 0; k < rows; ++k) {
+                px.push_back(xs[(size_t)k].c_str());
+                py.push_back(ys[(size_t)k].c_str());
+                pa.push_back(as[(size_t)k].c_str());
+            }
+            orc::Verdict v = orc::evaluate(n_of[p], (int)rows, ids.data(), px.data(), py.data(), pa.data());
+            ok_out[p] = v.ok ? 1 : 0;
+            if (score_out) score_out[p] = v.score;
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < threads; ++t) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
+    return threads;
+}

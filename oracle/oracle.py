@@ -54,6 +54,9 @@ def lib():
                                   C.c_char_p, C.c_int, _dp]
         L.sqo_roundtrip.restype = None
         L.sqo_roundtrip.argtypes = [C.c_char_p, C.c_char_p, C.c_int]
+        L.sqo_certify_batch.restype = C.c_int
+        L.sqo_certify_batch.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_void_p,
+                                        C.c_int, C.c_void_p, C.c_void_p]
         _LIB = L
     return _LIB
 
@@ -87,6 +90,9 @@ def ref_certifier():
                                    C.c_char_p, C.c_int, _dp]
         L.ref_roundtrip.restype = None
         L.ref_roundtrip.argtypes = [C.c_char_p, C.c_char_p, C.c_int]
+        L.ref_evaluate_batch.restype = C.c_int
+        L.ref_evaluate_batch.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_void_p,
+                                         C.c_int, C.c_void_p, C.c_void_p]
         _REF_CERT = L
     return _REF_CERT
 
@@ -163,3 +169,20 @@ def roundtrip(s, which="oracle"):
     fn = lib().sqo_roundtrip if which == "oracle" else ref_certifier().ref_roundtrip
     fn(str(s).encode(), out, 64)
     return out.value.decode()
+
+
+def certify_batch(n_of, row_start, sid, text, lit_off, which="oracle", threads=None):
+    """Threaded batch certification of packed arrays (sqs.core.pack_batch
+    layout): returns (ok int32[count], score float64[count], threads used)."""
+    n_of = np.ascontiguousarray(n_of, np.int32)
+    row_start = np.ascontiguousarray(row_start, np.int64)
+    sid = np.ascontiguousarray(sid, np.int32)
+    lit_off = np.ascontiguousarray(lit_off, np.int64)
+    count = len(n_of)
+    ok = np.zeros(count, np.int32)
+    score = np.zeros(count)
+    threads = threads or os.cpu_count() or 1
+    fn = lib().sqo_certify_batch if which == "oracle" else ref_certifier().ref_evaluate_batch
+    used = fn(count, n_of.ctypes.data, row_start.ctypes.data, sid.ctypes.data, text, lit_off.ctypes.data,
+              threads, ok.ctypes.data, score.ctypes.data)
+    return ok, score, used

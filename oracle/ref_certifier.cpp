@@ -35,3 +35,37 @@ extern "C" int ref_evaluate(int n, int rows, const int* sid, const char* const* 
 extern "C" void ref_roundtrip(const char* s, char* out, int cap) {
     put(out, cap, cert::roundtrip_float_str(s));
 }
+
+#include <atomic>
+#include <thread>
+
+// Certify `count` packings with `threads` worker threads pulling packings from
+// an atomic counter, as certifier.cpp's main does (:1011-1032).  Packing p
+// has rows row_start[p] .. row_start[p+1]-1; row r's literals are
+// text[lit_off[3r+k] .. lit_off[3r+k+1]).  ok_out[p] = 1 when accepted.
+extern "C" int ref_evaluate_batch(int count, const int* n_of, const long long* row_start, const int* sid,
+                                  const char* text, const long long* lit_off, int threads, int* ok_out,
+                                  double* score_out) {
+    std::atomic<int> next{0};
+    auto work = [&]() {
+        for (int p = next.fetch_add(1); p < count; p = next.fetch_add(1)) {
+            std::vector<cert::RowData> rd;
+            for (long long r = row_start[p]; r < row_start[p + 1]; ++r) {
+                cert::RowData d;
+                d.square_id = sid ? sid[r] : (int)(r - row_start[p]);
+                d.x.assign(text + lit_off[3 * r], (size_t)(lit_off[3 * r + 1] - lit_off[3 * r]));
+                d.y.assign(text + lit_off[3 * r + 1], (size_t)(lit_off[3 * r + 2] - lit_off[3 * r + 1]));
+                d.angle.assign(text + lit_off[3 * r + 2], (size_t)(lit_off[3 * r + 3] - lit_off[3 * r + 2]));
+                rd.push_back(std::move(d));
+            }
+            cert::PuzzleResult res = cert::evaluate_single_puzzle(n_of[p], rd);
+            ok_out[p] = res.ok ? 1 : 0;
+            if (score_out) score_out[p] = res.score;
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < threads; ++t) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
+    return threads;
+}

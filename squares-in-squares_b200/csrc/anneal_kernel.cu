@@ -239,15 +239,75 @@ __device__ double cert_side(const Rep& R, int n, const Grid& g, int lane, double
     return fmax(__dsub_rn(bx1, bx0), __dsub_rn(by1, by0));
 }
 
-// Quench of one replica: Jacobi gradient descent on its overlap + wall
-// energy with a backtracking step (every square moves at once; gradients are
-// summed in fixed point, so the result does not depend on neighbour order).
-// The reference's analogue is the per-epoch polish (seeded.cu:621-713).
-__device__ long long quench(const Rep& R, int n, Grid& g, float L, int lane, int iters, float4* grad,
-                            float4* saved, long long E) {
+// ---- CTA-cooperative forms (every thread of the CTA works on one replica)
+__device__ bool build_cells_cta(const Rep& R, int n, const Grid& g) {
+    const int ncell = g.G * g.G, tid = threadIdx.x, nt = blockDim.x;
+    for (int c = tid; c < ncell; c += nt) R.cnt[c] = 0;
+    for (int k = tid; k < ncell * kCellK; k += nt) R.slot[k] = 0;
+    __syncthreads();
+    bool ok = true;
+    for (int i = tid; i < n; i += nt) {
+        const float4 p = R.sq[i];
+        const int c = g.cx(p.y) * g.G + g.cx(p.x);
+        const unsigned k = atomicAdd(reinterpret_cast<unsigned*>(R.cnt + (c & ~3)), 1u << (8 * (c & 3)));
+        const unsigned slot_k = (k >> (8 * (c & 3))) & 0xffu;
+        if (slot_k < (unsigned)kCellK) R.slot[c * kCellK + slot_k] = (uint16_t)i;
+        else ok = false;
+    }
+    const bool bad = __syncthreads_or(!ok);
+    if (bad) {
+        for (int c = tid; c < ncell; c += nt)
+            if (R.cnt[c] > kCellK) R.cnt[c] = (uint8_t)kCellK;
+        __syncthreads();
+    }
+    return !bad;
+}
+
+__device__ long long block_sum_ll(long long v, long long* red) {
+    v = warp_sum_ll(v);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    __syncthreads();
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    long long t = 0;
+    for (int k = 0; k < nw; ++k) t += red[k];
+    return t;
+}
+
+// Full fixed-point energy with one thread per square.
+__device__ long long full_energy_cta(const Rep& R, int n, const Grid& g, float L, long long* red) {
+    long long e = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const float4 P = R.sq[i];
+        e += qe(wall_e(P.x, P.y, P.z, P.w, L));
+        const int cx = g.cx(P.x), cy = g.cx(P.y);
+        for (int dy = -1; dy <= 1; ++dy) {
+            for (int dxc = -1; dxc <= 1; ++dxc) {
+                const int x = cx + dxc, y = cy + dy;
+                if (x < 0 || x >= g.G || y < 0 || y >= g.G) continue;
+                const int cell = y * g.G + x;
+                const int m = R.cnt[cell];
+                for (int k = 0; k < m; ++k) {
+                    const int j = R.slot[cell * kCellK + k];
+                    if (j <= i) continue;
+                    const float4 Q = R.sq[j];
+                    const float dx = Q.x - P.x, dy2 = Q.y - P.y;
+                    if (dx * dx + dy2 * dy2 < kPairCut2) e += qe(sat_pair_energy(dx, dy2, P.z, P.w, Q.z, Q.w));
+                }
+            }
+        }
+    }
+    return block_sum_ll(e, red);
+}
+
+// The quench of the coldest replica by the whole CTA: the same Jacobi
+// descent with backtracking as `quench`, one thread per square.  Integer
+// sums make the result identical to a single warp's.
+__device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters, float4* grad, float4* saved,
+                                long long E, long long* red) {
     float alpha = 0.05f;
     for (int it = 0; it < iters && E > 0; ++it) {
-        for (int i = lane; i < n; i += 32) {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
             const float4 P = R.sq[i];
             float wx = 0.f, wy = 0.f, wa = 0.f;
             wall_energy_grad(P.x, P.y, P.z, P.w, L, wx, wy, wa);
@@ -278,9 +338,9 @@ __device__ long long quench(const Rep& R, int n, Grid& g, float L, int lane, int
                                   (float)qa * (1.0f / kEScale), 0.f);
             saved[i] = make_float4(P.x, P.y, R.ang[i], 0.f);
         }
-        __syncwarp();
+        __syncthreads();
         for (int tries = 0; tries < 6; ++tries) {
-            for (int i = lane; i < n; i += 32) {
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
                 const float4 d = grad[i], o = saved[i];
                 const float sx = fminf(0.1f, fmaxf(-0.1f, alpha * d.x));
                 const float sy = fminf(0.1f, fmaxf(-0.1f, alpha * d.y));
@@ -292,9 +352,9 @@ __device__ long long quench(const Rep& R, int n, Grid& g, float L, int lane, int
                 R.sq[i] = make_float4(o.x - sx, o.y - sy, cs, sn);
                 R.ang[i] = a;
             }
-            __syncwarp();
-            const bool fits = build_cells(R, n, g, lane);
-            const long long En = fits ? full_energy(R, n, g, L, lane) : E;
+            __syncthreads();
+            const bool fits = build_cells_cta(R, n, g);
+            const long long En = fits ? full_energy_cta(R, n, g, L, red) : E;
             if (fits && En < E) {
                 E = En;
                 alpha = fminf(alpha * 1.3f, 0.2f);
@@ -302,15 +362,15 @@ __device__ long long quench(const Rep& R, int n, Grid& g, float L, int lane, int
             }
             alpha *= 0.3f;
             if (tries == 5) {  // no improvement: restore the saved state
-                for (int i = lane; i < n; i += 32) {
+                for (int i = threadIdx.x; i < n; i += blockDim.x) {
                     const float4 o = saved[i];
                     float sn, cs;
                     sincosf(o.z, &sn, &cs);
                     R.sq[i] = make_float4(o.x, o.y, cs, sn);
                     R.ang[i] = o.z;
                 }
-                __syncwarp();
-                build_cells(R, n, g, lane);
+                __syncthreads();
+                build_cells_cta(R, n, g);
                 it = iters;
             }
         }
@@ -330,6 +390,8 @@ struct CtaShared {
     int bad;                   // any overflow in the cluster
     float newL;
     unsigned long long props[kMaxRl], accs[kMaxRl];
+    long long red[kMaxRl];
+    long long qE;              // energy of the replica quenched by this CTA
 };
 
 __global__ void __launch_bounds__(1024) anneal_kernel(const int32_t* __restrict__ job_list,
@@ -474,11 +536,24 @@ __global__ void __launch_bounds__(1024) anneal_kernel(const int32_t* __restrict_
         // job's trajectory does not depend on how it is sliced.
         const bool xpoint = (sweep + 1) % jd.exchange_every == 0;
         if (!xpoint && sweep + 1 != jd.sweeps_total) continue;
+        // the replica on the coldest rung is quenched toward zero overlap by
+        // every thread of the CTA that holds it
+        {
+            int cold = 0;
+            for (int q = 0; q < R; ++q)
+                if (S.jm.perm[q] == 0) cold = q;
+            if (jd.quench_iters > 0 && cold / Rl == rank) {
+                if (w == cold % Rl && lane == 0) S.qE = E;
+                __syncthreads();
+                const Rep cr = rep_view(dyn + (cold % Rl) * rb, n, jd.Gmax);
+                const long long qe_out = quench_cta(cr, n, g, L, jd.quench_iters, pos + jd.scr_off,
+                                                    pos + jd.scr_off + n, S.qE, S.red);
+                if (w == cold % Rl) E = qe_out;
+                __syncthreads();
+            }
+        }
         if (active) {
             double Lc = 1e30, lam = 0, x0 = 0, y0 = 0;
-            // the replica on the coldest rung is quenched toward zero overlap
-            if (S.jm.perm[r] == 0 && jd.quench_iters > 0)
-                E = quench(rep, n, g, L, lane, jd.quench_iters, pos + jd.scr_off, pos + jd.scr_off + n, E);
             // any state whose overlaps a dilation of at most 0.8% removes is a
             // certified candidate (penetrations of depth d cost about d^2 each)
             if (E < qe(1e-4f)) Lc = cert_side(rep, n, g, lane, lam, x0, y0);
@@ -620,8 +695,10 @@ int launch_anneal(cudaStream_t stream, int njobs, int cs, int Rl, size_t smem, c
     int dev = 0;
     cudaGetDevice(&dev);
     if (!attr_done[dev & 63]) {
+        cudaFuncAttributes fa;
+        SQS_CUDA(cudaFuncGetAttributes(&fa, anneal_kernel));
         SQS_CUDA(cudaFuncSetAttribute(anneal_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      232448 - (int)sizeof(CtaShared)));
+                                      232448 - (int)fa.sharedSizeBytes));
         SQS_CUDA(cudaFuncSetAttribute(anneal_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
         attr_done[dev & 63] = true;
     }

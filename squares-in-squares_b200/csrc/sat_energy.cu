@@ -33,6 +33,25 @@ constexpr int kSatMaxN = 1024;
 constexpr float kCellMin = 1.41422f;  // > sqrt(2.000001) = 1.4142139
 constexpr int kQueue = 64;            // per-warp pair queue entries
 
+// Gradient accumulation with native 32-bit integer shared-memory atomics
+// (shared-memory float atomics are several times slower): a contribution v
+// is split into floor(v * 2^12) and the remaining fraction in units of 2^-32,
+// two integer sums that cannot overflow for n <= 1024 (|v| < 6 per pair) and
+// that do not depend on the order of the additions.
+struct GradFix {
+    int* hi;        // [3n]
+    unsigned* lo;   // [3n]
+    __device__ __forceinline__ void add(int k, float v) const {
+        const float s = v * 4096.0f;
+        const float f = floorf(s);
+        atomicAdd(hi + k, (int)f);
+        atomicAdd(lo + k, __float2uint_rn((s - f) * 1048576.0f));
+    }
+    __device__ __forceinline__ float value(int k) const {
+        return (float)(((double)hi[k] + (double)lo[k] * (1.0 / 1048576.0)) * (1.0 / 4096.0));
+    }
+};
+
 __host__ __device__ inline int sat_grid_cap(int n) {
     // Cell grid side cap: about sqrt(2n) cells per side, at most 45 (L = 64).
     int g = (int)sqrtf(2.0f * (float)n);
@@ -43,8 +62,9 @@ __host__ __device__ inline size_t sat_smem_bytes(int n, int threads) {
     const int G = sat_grid_cap(n);
     size_t b = 0;
     b += (size_t)n * 16;                      // stash (x, y, c, s) by original index
-    b += (size_t)n * 16;                      // cell-sorted (x, y, c, s)
-    b += (size_t)n * 12;                      // gradient accumulators by original index
+    b += (size_t)n * 16;                      // cell-sorted (x, y) and (c, s)
+    b += (size_t)n * 12;                      // wall gradient by original index
+    b += (size_t)n * 24;                      // pair gradient accumulators (GradFix)
     b += (size_t)n * 4;                       // sorted -> (original index, cell)
     b += (size_t)n * 4;                       // original -> (cell, rank)
     b += (size_t)(G * G + 1) * 4;             // cell counts / starts
@@ -65,9 +85,11 @@ __global__ void __launch_bounds__(T) sat_energy_kernel(int n, const float* __res
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int Gcap = sat_grid_cap(n);
     float4* stash = reinterpret_cast<float4*>(smem);
-    float4* sorted = stash + n;
-    float* gacc = reinterpret_cast<float*>(sorted + n);
-    short2* sorted_meta = reinterpret_cast<short2*>(gacc + 3 * n);  // (orig, cell)
+    float2* sxy = reinterpret_cast<float2*>(stash + n);             // cell-sorted centres
+    float2* scs = sxy + n;                                          // cell-sorted cos/sin
+    float* gacc = reinterpret_cast<float*>(scs + n);                // wall gradient
+    GradFix gf{reinterpret_cast<int*>(gacc + 3 * n), reinterpret_cast<unsigned*>(gacc + 6 * n)};
+    short2* sorted_meta = reinterpret_cast<short2*>(gacc + 9 * n);  // (orig, cell)
     short2* orig_meta = sorted_meta + n;                            // (cell, rank)
     int* cells = reinterpret_cast<int*>(orig_meta + n);             // G*G + 1
     uint32_t* queues = reinterpret_cast<uint32_t*>(cells + Gcap * Gcap + 1);
@@ -127,7 +149,9 @@ __global__ void __launch_bounds__(T) sat_energy_kernel(int n, const float* __res
     for (int i = tid; i < n; i += T) {
         const short2 m = orig_meta[i];
         const int pos = cells[m.x] + m.y;
-        sorted[pos] = stash[i];
+        const float4 v = stash[i];
+        sxy[pos] = make_float2(v.x, v.y);
+        scs[pos] = make_float2(v.z, v.w);
         sorted_meta[pos] = make_short2((short)i, m.x);
     }
     __syncthreads();
@@ -135,17 +159,23 @@ __global__ void __launch_bounds__(T) sat_energy_kernel(int n, const float* __res
     for (int c = tid; c < ncell; c += T) {
         const int a = cells[c], b = cells[c + 1];
         for (int u = a + 1; u < b; ++u) {
-            const float4 kv = sorted[u];
+            const float2 kxy = sxy[u], kcs = scs[u];
             const short2 km = sorted_meta[u];
             int w = u - 1;
             while (w >= a && sorted_meta[w].x > km.x) {
-                sorted[w + 1] = sorted[w];
+                sxy[w + 1] = sxy[w];
+                scs[w + 1] = scs[w];
                 sorted_meta[w + 1] = sorted_meta[w];
                 --w;
             }
-            sorted[w + 1] = kv;
+            sxy[w + 1] = kxy;
+            scs[w + 1] = kcs;
             sorted_meta[w + 1] = km;
         }
+    }
+    for (int k = tid; k < 3 * n; k += T) {
+        gf.hi[k] = 0;
+        gf.lo[k] = 0u;
     }
     __syncthreads();
 
@@ -155,17 +185,17 @@ __global__ void __launch_bounds__(T) sat_energy_kernel(int n, const float* __res
     int qn = 0;  // warp-uniform queue length
     auto narrow = [&](uint32_t entry) {
         const int p = (int)(entry & 0xffffu), q = (int)(entry >> 16);
-        const float4 P = sorted[p], Q = sorted[q];
+        const float2 P = sxy[p], Q = sxy[q], Pc = scs[p], Qc = scs[q];
         PairGrad g;
-        if (sat_pair_grad(Q.x - P.x, Q.y - P.y, P.z, P.w, Q.z, Q.w, g)) {
+        if (sat_pair_grad(Q.x - P.x, Q.y - P.y, Pc.x, Pc.y, Qc.x, Qc.y, g)) {
             e_loc += g.e;
             const int i = sorted_meta[p].x, j = sorted_meta[q].x;
-            atomicAdd(&gacc[3 * i], g.px);
-            atomicAdd(&gacc[3 * i + 1], g.py);
-            atomicAdd(&gacc[3 * i + 2], g.pa);
-            atomicAdd(&gacc[3 * j], g.qx);
-            atomicAdd(&gacc[3 * j + 1], g.qy);
-            atomicAdd(&gacc[3 * j + 2], g.qa);
+            gf.add(3 * i, g.px);
+            gf.add(3 * i + 1, g.py);
+            gf.add(3 * i + 2, g.pa);
+            gf.add(3 * j, g.qx);
+            gf.add(3 * j + 1, g.qy);
+            gf.add(3 * j + 2, g.qa);
         }
     };
     for (int base = warp * 32; base < n; base += T) {
@@ -173,7 +203,7 @@ __global__ void __launch_bounds__(T) sat_energy_kernel(int n, const float* __res
         int a1 = 0, len1 = 0, a2 = 0, len = 0;
         float px = 0.f, py = 0.f;
         if (p < n) {
-            const float4 P = sorted[p];
+            const float2 P = sxy[p];
             px = P.x;
             py = P.y;
             const int cell = sorted_meta[p].y, cy = cell / G, cx = cell - cy * G;
@@ -194,7 +224,7 @@ __global__ void __launch_bounds__(T) sat_energy_kernel(int n, const float* __res
             int q = 0;
             if (t < len) {
                 q = t < len1 ? a1 + t : a2 + (t - len1);
-                const float4 Q = sorted[q];
+                const float2 Q = sxy[q];
                 const float dx = Q.x - px, dy = Q.y - py;
                 const float d2 = dx * dx + dy * dy;
                 pass = d2 < kPairCut2;
@@ -239,8 +269,264 @@ __global__ void __launch_bounds__(T) sat_energy_kernel(int n, const float* __res
     }
     if (grad) {
         float* dst = grad + (size_t)cfg * 3 * n;
-        for (int k = tid; k < 3 * n; k += T) dst[k] = gacc[k];
+        for (int k = tid; k < 3 * n; k += T) dst[k] = gacc[k] + gf.value(k);
     }
+}
+
+// ---------------------------------------------------------------------------
+// Warp-per-configuration form for n <= 256: the same phases as above run by
+// one warp without block barriers, several configurations per CTA.  A lane
+// keeps its (up to 8) squares in registers from the load to the scatter, all
+// loads are issued before any is used, and the cell grid is sized from n, so
+// ~7.7 KB of shared memory per configuration lets a whole 4,096-configuration
+// batch be resident in one wave.
+constexpr int kWarpMaxN = 256;
+constexpr int kWarpNpl = kWarpMaxN / 32;
+
+__host__ __device__ inline int warp_grid_cap(int n) {
+    int g = (int)sqrtf((float)n) + 2;
+    return g > 45 ? 45 : g;
+}
+
+__host__ __device__ inline size_t warp_smem_bytes(int n) {
+    const int G = warp_grid_cap(n);
+    // sorted (x, y) + (c, s), pair-gradient accumulators, original index (byte),
+    // cell starts (uint16), pair queue
+    size_t b = (size_t)n * 16 + (size_t)n * 12 + (((size_t)n + 3) & ~(size_t)3) +
+               (((size_t)(G * G + 1) * 2 + 3) & ~(size_t)3) + kQueue * 4;
+    return (b + 15) & ~(size_t)15;
+}
+
+// Pair-gradient sums of the warp kernel: one 32-bit integer per component in
+// units of 2^-20.  With n <= 256 a square has at most 255 partners and each
+// pair term is below 6 in magnitude, so a sum stays below 2^31 units; every
+// term is rounded once (error < 5e-7) and the sum is exact and order-free.
+constexpr float kGScale = 1048576.0f;
+
+template <int W, bool COUNT>
+__global__ void __launch_bounds__(W * 32) sat_energy_warp_kernel(int configs, int n, const float* __restrict__ xya,
+                                                                 const float* __restrict__ side,
+                                                                 float* __restrict__ energy, float* __restrict__ grad,
+                                                                 uint32_t* __restrict__ cand) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int cfg = blockIdx.x * W + warp;
+    if (cfg >= configs) return;
+    const size_t wb = warp_smem_bytes(n);
+    unsigned char* base = smem + (size_t)warp * wb;
+    const int Gcap = warp_grid_cap(n);
+    float2* sxy = reinterpret_cast<float2*>(base);            // cell-sorted centres
+    float2* scs = sxy + n;                                     // cell-sorted cos/sin
+    int* gq = reinterpret_cast<int*>(scs + n);                 // pair-gradient sums (kGScale units)
+    uint8_t* orig = reinterpret_cast<uint8_t*>(gq + 3 * n);    // sorted -> original index
+    uint16_t* cells = reinterpret_cast<uint16_t*>(orig + ((n + 3) & ~3));  // G*G + 1 starts
+    uint32_t* queue = reinterpret_cast<uint32_t*>(cells + (((Gcap * Gcap + 1) + 1) & ~1));
+
+    const float L = side[cfg];
+    int G = (int)(L / kCellMin);
+    G = G < 1 ? 1 : (G > Gcap ? Gcap : G);
+    const float inv_cell = (float)G / L;
+    const int ncell = G * G;
+    for (int c = lane; c <= ncell; c += 32) cells[c] = 0;
+    float* gdst = grad ? grad + (size_t)cfg * 3 * n : nullptr;
+
+    // 1. all loads first, then trig, walls and cell ranks
+    const float* src = xya + (size_t)cfg * 3 * n;
+    float px[kWarpNpl], py[kWarpNpl], pa[kWarpNpl];
+#pragma unroll
+    for (int k = 0; k < kWarpNpl; ++k) {
+        const int i = lane + 32 * k;
+        if (i < n) {
+            px[k] = src[3 * i];
+            py[k] = src[3 * i + 1];
+            pa[k] = src[3 * i + 2];
+        }
+    }
+    __syncwarp();
+    float e_loc = 0.f;
+    float pc[kWarpNpl], ps[kWarpNpl];
+    int cr[kWarpNpl];  // cell << 16 | rank
+#pragma unroll
+    for (int k = 0; k < kWarpNpl; ++k) {
+        const int i = lane + 32 * k;
+        if (i < n) {
+            sincosf(pa[k], &ps[k], &pc[k]);
+            float gx = 0.f, gy = 0.f, ga = 0.f;
+            e_loc += wall_energy_grad(px[k], py[k], pc[k], ps[k], L, gx, gy, ga);
+            if (gdst) {  // the wall term goes straight out; pair terms are added at the end
+                gdst[3 * i] = gx;
+                gdst[3 * i + 1] = gy;
+                gdst[3 * i + 2] = ga;
+            }
+            gq[3 * i] = gq[3 * i + 1] = gq[3 * i + 2] = 0;
+            int cx = (int)floorf(px[k] * inv_cell), cy = (int)floorf(py[k] * inv_cell);
+            cx = cx < 0 ? 0 : (cx >= G ? G - 1 : cx);
+            cy = cy < 0 ? 0 : (cy >= G ? G - 1 : cy);
+            const int cell = cy * G + cx;
+            // per-cell counts in 16-bit halves of 32-bit words (native integer atomics)
+            const unsigned old = atomicAdd(reinterpret_cast<unsigned*>(cells) + (cell >> 1), 1u << (16 * (cell & 1)));
+            cr[k] = (cell << 16) | (int)((old >> (16 * (cell & 1))) & 0xffffu);
+        }
+    }
+    __syncwarp();
+    // 2. exclusive scan of the cell counts, scatter from registers
+    {
+        const int per = (ncell + 31) / 32;
+        const int lo = lane * per, hi = min(lo + per, ncell);
+        int sum = 0;
+        for (int c = lo; c < hi; ++c) sum += cells[c];
+        int incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        int run = incl - sum;
+        for (int c = lo; c < hi; ++c) {
+            const int k = cells[c];
+            cells[c] = run;
+            run += k;
+        }
+        if (lane == 31) cells[ncell] = incl;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < kWarpNpl; ++k) {
+        const int i = lane + 32 * k;
+        if (i < n) {
+            const int cell = cr[k] >> 16;
+            const int pos = cells[cell] + (cr[k] & 0xffff);
+            sxy[pos] = make_float2(px[k], py[k]);
+            scs[pos] = make_float2(pc[k], ps[k]);
+            orig[pos] = (uint8_t)i;
+        }
+    }
+    __syncwarp();
+    for (int c = lane; c < ncell; c += 32) {  // each cell's entries by original index
+        const int a = cells[c], b = cells[c + 1];
+        for (int u = a + 1; u < b; ++u) {
+            const float2 kxy = sxy[u], kcs = scs[u];
+            const uint8_t km = orig[u];
+            int w = u - 1;
+            while (w >= a && orig[w] > km) {
+                sxy[w + 1] = sxy[w];
+                scs[w + 1] = scs[w];
+                orig[w + 1] = orig[w];
+                --w;
+            }
+            sxy[w + 1] = kxy;
+            scs[w + 1] = kcs;
+            orig[w + 1] = km;
+        }
+    }
+    __syncwarp();
+
+    // 3. broad phase into the warp queue, narrow phase 32 pairs at a time
+    uint32_t cand_loc = 0;
+    int qn = 0;
+    auto narrow = [&](uint32_t entry) {
+        const int p = (int)(entry & 0xffffu), q = (int)(entry >> 16);
+        const float2 P = sxy[p], Q = sxy[q], Pc = scs[p], Qc = scs[q];
+        PairGrad g;
+        if (sat_pair_grad(Q.x - P.x, Q.y - P.y, Pc.x, Pc.y, Qc.x, Qc.y, g)) {
+            e_loc += g.e;
+            const int i = orig[p], j = orig[q];
+            atomicAdd(gq + 3 * i, __float2int_rn(g.px * kGScale));
+            atomicAdd(gq + 3 * i + 1, __float2int_rn(g.py * kGScale));
+            atomicAdd(gq + 3 * i + 2, __float2int_rn(g.pa * kGScale));
+            atomicAdd(gq + 3 * j, __float2int_rn(g.qx * kGScale));
+            atomicAdd(gq + 3 * j + 1, __float2int_rn(g.qy * kGScale));
+            atomicAdd(gq + 3 * j + 2, __float2int_rn(g.qa * kGScale));
+        }
+    };
+    for (int base0 = 0; base0 < n; base0 += 32) {
+        const int p = base0 + lane;
+        int a1 = 0, len1 = 0, a2 = 0, len = 0;
+        float qx0 = 0.f, qy0 = 0.f;
+        if (p < n) {
+            const float2 P = sxy[p];
+            qx0 = P.x;
+            qy0 = P.y;
+            int cx = (int)floorf(P.x * inv_cell), cy = (int)floorf(P.y * inv_cell);
+            cx = cx < 0 ? 0 : (cx >= G ? G - 1 : cx);
+            cy = cy < 0 ? 0 : (cy >= G ? G - 1 : cy);
+            a1 = p + 1;
+            len1 = cells[cy * G + min(cx + 2, G)] - a1;
+            int len2 = 0;
+            if (cy + 1 < G) {
+                a2 = cells[(cy + 1) * G + max(cx - 1, 0)];
+                len2 = cells[(cy + 1) * G + min(cx + 2, G)] - a2;
+            }
+            len = len1 + len2;
+            a2 -= len1;  // q = a2 + t for t >= len1
+        }
+        const int maxlen = __reduce_max_sync(0xffffffffu, len);
+        for (int t = 0; t < maxlen; ++t) {
+            bool pass = false;
+            int q = 0;
+            if (t < len) {
+                q = (t < len1 ? a1 : a2) + t;
+                const float2 Q = sxy[q];
+                const float dx = Q.x - qx0, dy = Q.y - qy0;
+                const float d2 = dx * dx + dy * dy;
+                pass = d2 < kPairCut2;
+                if (COUNT) cand_loc += d2 < 2.0f;
+            }
+            const uint32_t m = __ballot_sync(0xffffffffu, pass);
+            if (pass) queue[qn + __popc(m & ((1u << lane) - 1u))] = (uint32_t)p | ((uint32_t)q << 16);
+            qn += __popc(m);
+            if (qn >= 32) {
+                __syncwarp();
+                narrow(queue[lane]);
+                __syncwarp();
+                if (lane < qn - 32) queue[lane] = queue[32 + lane];
+                __syncwarp();
+                qn -= 32;
+            }
+        }
+    }
+    __syncwarp();
+    if (lane < qn) narrow(queue[lane]);
+    __syncwarp();
+
+    // 4. reductions and the coalesced gradient store
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        e_loc += __shfl_xor_sync(0xffffffffu, e_loc, o);
+        cand_loc += __shfl_xor_sync(0xffffffffu, cand_loc, o);
+    }
+    if (lane == 0) {
+        energy[cfg] = e_loc;
+        if (COUNT) cand[cfg] = cand_loc;
+    }
+    if (gdst) {
+        for (int k = lane; k < 3 * n; k += 32) gdst[k] += (float)gq[k] * (1.0f / kGScale);
+    }
+}
+
+template <int W>
+static int launch_warp(sqs_ctx* ctx, int configs, int n, const float* xya, const float* side, float* energy,
+                       float* grad, uint32_t* cand) {
+    const size_t smem = warp_smem_bytes(n) * W;
+    static bool attr_set[64] = {false};
+    const int dev = ctx->device & 63;
+    if (!attr_set[dev]) {
+        SQS_CUDA(cudaFuncSetAttribute(sat_energy_warp_kernel<W, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      200 * 1024));
+        SQS_CUDA(cudaFuncSetAttribute(sat_energy_warp_kernel<W, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      200 * 1024));
+        attr_set[dev] = true;
+    }
+    const unsigned blocks = (unsigned)((configs + W - 1) / W);
+    if (cand)
+        sat_energy_warp_kernel<W, true><<<blocks, W * 32, smem, ctx->stream>>>(configs, n, xya, side, energy, grad,
+                                                                               cand);
+    else
+        sat_energy_warp_kernel<W, false><<<blocks, W * 32, smem, ctx->stream>>>(configs, n, xya, side, energy, grad,
+                                                                                nullptr);
+    SQS_CUDA(cudaGetLastError());
+    ctx->launches += 1;
+    return SQS_OK;
 }
 
 template <int T>
@@ -266,7 +552,17 @@ int sat_energy_launch(sqs_ctx* ctx, int configs, int n, const float* xya, const 
     SQS_REQUIRE(n >= 1 && n <= kSatMaxN, "n %d out of 1..%d", n, kSatMaxN);
     SQS_REQUIRE(xya && side && energy, "null device pointer");
     if (configs == 0) return SQS_OK;
-    if (threads == 0) threads = n <= 256 ? 64 : 128;
+    if (threads == 0) threads = n <= kWarpMaxN ? -4 : 128;
+    if (threads < 0) {  // warp-per-configuration kernel, -threads warps per CTA
+        SQS_REQUIRE(n <= kWarpMaxN, "the warp-per-configuration kernel takes n <= %d", kWarpMaxN);
+        switch (-threads) {
+            case 2: return launch_warp<2>(ctx, configs, n, xya, side, energy, grad, cand);
+            case 4: return launch_warp<4>(ctx, configs, n, xya, side, energy, grad, cand);
+            case 8: return launch_warp<8>(ctx, configs, n, xya, side, energy, grad, cand);
+            default: break;
+        }
+        SQS_REQUIRE(false, "threads %d: warps per CTA must be 2, 4 or 8", threads);
+    }
     switch (threads) {
         case 32: return launch<32>(ctx, configs, n, xya, side, energy, grad, cand);
         case 64: return launch<64>(ctx, configs, n, xya, side, energy, grad, cand);

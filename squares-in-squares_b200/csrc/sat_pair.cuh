@@ -50,13 +50,31 @@ __device__ __forceinline__ bool sat_pair_grad(float dx, float dy, float cp, floa
     const float deriv = 0.5f * (sgnf(sd) * cd - sgnf(cd) * sd);
     const float two_gap = 2.f * gap;
     g.e = gap * gap;
-    // first maximum in order 0,1,2,3 (gradient of p)
+    // Without a tie both squares use the same axis: one selection serves both.
+    const int ties = (z0 == gap) + (z1 == gap) + (z2 == gap) + (z3 == gap);
+    if (ties == 1) {
+        const bool k0 = z0 == gap, k1 = z1 == gap, k2 = z2 == gap;
+        const float ux = k0 ? cp : (k1 ? -sp : (k2 ? cq : -sq));
+        const float uy = k0 ? sp : (k1 ? cp : (k2 ? sq : cq));
+        const float v = k0 ? v0 : (k1 ? v1 : (k2 ? v2 : v3));
+        const float tv = k0 ? v1 : (k1 ? -v0 : (k2 ? v3 : -v2));  // d v / d(own angle)
+        const float s = sgnf(v);
+        const float tp = (k0 || k1) ? s * tv : 0.f, tq = (k0 || k1) ? 0.f : s * tv;
+        g.px = -two_gap * s * ux;
+        g.py = -two_gap * s * uy;
+        g.pa = two_gap * (tp - deriv);
+        g.qx = -g.px;
+        g.qy = -g.py;
+        g.qa = two_gap * (tq + deriv);
+        return true;
+    }
+    // first maximum in order 0,1,2,3 (gradient of p), as selects
     {
-        float ux, uy, v, torque = 0.f;
-        if (z0 == gap) { ux = cp; uy = sp; v = v0; torque = sgnf(v0) * v1; }
-        else if (z1 == gap) { ux = -sp; uy = cp; v = v1; torque = -sgnf(v1) * v0; }
-        else if (z2 == gap) { ux = cq; uy = sq; v = v2; }
-        else { ux = -sq; uy = cq; v = v3; }
+        const bool k0 = z0 == gap, k1 = !k0 && z1 == gap, k2 = !k0 && !k1 && z2 == gap;
+        const float ux = k0 ? cp : (k1 ? -sp : (k2 ? cq : -sq));
+        const float uy = k0 ? sp : (k1 ? cp : (k2 ? sq : cq));
+        const float v = k0 ? v0 : (k1 ? v1 : (k2 ? v2 : v3));
+        const float torque = k0 ? sgnf(v0) * v1 : (k1 ? -sgnf(v1) * v0 : 0.f);
         const float s = sgnf(v);
         g.px = -two_gap * s * ux;
         g.py = -two_gap * s * uy;
@@ -64,11 +82,11 @@ __device__ __forceinline__ bool sat_pair_grad(float dx, float dy, float cp, floa
     }
     // first maximum in order 2,3,0,1 (gradient of q)
     {
-        float ux, uy, v, torque = 0.f;
-        if (z2 == gap) { ux = cq; uy = sq; v = v2; torque = sgnf(v2) * v3; }
-        else if (z3 == gap) { ux = -sq; uy = cq; v = v3; torque = -sgnf(v3) * v2; }
-        else if (z0 == gap) { ux = cp; uy = sp; v = v0; }
-        else { ux = -sp; uy = cp; v = v1; }
+        const bool k2 = z2 == gap, k3 = !k2 && z3 == gap, k0 = !k2 && !k3 && z0 == gap;
+        const float ux = k2 ? cq : (k3 ? -sq : (k0 ? cp : -sp));
+        const float uy = k2 ? sq : (k3 ? cq : (k0 ? sp : cp));
+        const float v = k2 ? v2 : (k3 ? v3 : (k0 ? v0 : v1));
+        const float torque = k2 ? sgnf(v2) * v3 : (k3 ? -sgnf(v3) * v2 : 0.f);
         const float s = sgnf(v);
         g.qx = two_gap * s * ux;
         g.qy = two_gap * s * uy;
