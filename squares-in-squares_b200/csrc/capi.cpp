@@ -113,6 +113,7 @@ int sqs_ctx_destroy(sqs_ctx* ctx) {
     ctx->d_cand.release();
     ctx->d_misc.release();
     ctx->d_anneal.release();
+    ctx->d_cert.release();
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SQS_OK;

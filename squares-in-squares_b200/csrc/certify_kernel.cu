@@ -607,6 +607,102 @@ __global__ void __launch_bounds__(128) cert_stage_kernel(
     }
 }
 
+// ------------------------------------------------------------ cached stages
+// The same interval test with every square's interval corners computed once
+// per stage, as the reference caches them per square (ensure_sq_iv,
+// certifier.cpp:600-635): a square sits in about four undecided pairs of a
+// contact-heavy packing, and its parse + Taylor sin/cos is the expensive part.
+//   mark   claims a cache slot for each square of a live pair (one claim per
+//          square: slot_of[] holds -1, then -2 while claimed, then the slot);
+//   build  one thread per claimed square writes its IvSq<F> to the cache in
+//          HBM;
+//   pair   one thread per pair runs iv_sat on references into the cache.
+// Flags only ever get set, so a pair the mark kernel skipped (its packing
+// already decided) is skipped by the pair kernel too.
+struct SqRef {
+    int32_t sq;  // global square index (packing's first square + id)
+    int32_t pk;
+};
+
+__device__ __forceinline__ bool pair_live(const PkOut& po) {
+    return po.fkey == kNoPair && !(po.flags & kCertOverlap);
+}
+
+__global__ void __launch_bounds__(256) cert_mark_kernel(const Pair* __restrict__ in, const uint32_t* __restrict__ in_count,
+                                                       uint32_t in_cap, const int64_t* __restrict__ pk_sq0,
+                                                       int32_t* __restrict__ slot_of, SqRef* __restrict__ list,
+                                                       uint32_t* __restrict__ list_count, uint32_t list_cap,
+                                                       PkOut* __restrict__ out) {
+    const uint32_t total = min(*in_count, in_cap);
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const Pair pr = in[t];
+        if (!pair_live(out[pr.pk])) continue;
+        const int64_t s0 = pk_sq0[pr.pk];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int32_t g = (int32_t)(s0 + (k ? pr.v : pr.u));
+            if (atomicCAS(&slot_of[g], -1, -2) == -1) {
+                const uint32_t slot = atomicAdd(list_count, 1u);
+                if (slot < list_cap) {
+                    list[slot] = SqRef{g, pr.pk};
+                    slot_of[g] = (int32_t)slot;
+                } else {
+                    atomicOr(&out[pr.pk].flags, kPairOverflow);
+                }
+            }
+        }
+    }
+}
+
+template <int F>
+__global__ void __launch_bounds__(128) cert_build_kernel(const SqRef* __restrict__ list,
+                                                        const uint32_t* __restrict__ list_count, uint32_t list_cap,
+                                                        const int64_t* __restrict__ pk_sq0,
+                                                        const Lit* __restrict__ lits, const char* __restrict__ text,
+                                                        IvSq<F>* __restrict__ cache) {
+    const uint32_t total = min(*list_count, list_cap);
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const SqRef r = list[t];
+        const int64_t s0 = pk_sq0[r.pk];
+        const Iv<F> ox = fx::parse_iv<F>(text, lits[3 * s0]);
+        const Iv<F> oy = fx::parse_iv<F>(text, lits[3 * s0 + 1]);
+        make_ivsq<F>(text, lits + 3 * (int64_t)r.sq, ox, oy, cache[t]);
+    }
+}
+
+template <int F>
+__global__ void __launch_bounds__(128) cert_pair_kernel(const Pair* __restrict__ in,
+                                                       const uint32_t* __restrict__ in_count, uint32_t in_cap,
+                                                       Pair* __restrict__ next, uint32_t* __restrict__ next_count,
+                                                       uint32_t next_cap, const int64_t* __restrict__ pk_sq0,
+                                                       const int32_t* __restrict__ slot_of,
+                                                       const IvSq<F>* __restrict__ cache, PkOut* __restrict__ out) {
+    const uint32_t total = min(*in_count, in_cap);
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const Pair pr = in[t];
+        PkOut& po = out[pr.pk];
+        if (!pair_live(po)) continue;
+        const int64_t s0 = pk_sq0[pr.pk];
+        const int32_t a = slot_of[s0 + pr.u], b = slot_of[s0 + pr.v];
+        if (a < 0 || b < 0) {  // no cache entry (the slot list overflowed): report, never guess
+            atomicOr(&po.flags, kPairOverflow);
+            continue;
+        }
+        const int r = iv_sat<F>(cache[a], cache[b]);
+        if (r < 0) {
+            atomicOr(&po.flags, kCertOverlap);
+        } else if (r == 0) {
+            if (next == nullptr) {
+                atomicOr(&po.flags, kUndecidable);
+            } else {
+                const uint32_t slot = atomicAdd(next_count, 1u);
+                if (slot < next_cap) next[slot] = pr;
+                else atomicOr(&po.flags, kPairOverflow);
+            }
+        }
+    }
+}
+
 // ------------------------------------------------------------ host side
 // Constants (600-digit pi/2, 2 pi) are analysed without the 100-character
 // literal limit that applies to submitted coordinates.
@@ -718,6 +814,51 @@ static int launch_stage(sqs_ctx* ctx, const Pair* in, const uint32_t* in_count, 
     return SQS_OK;
 }
 
+static unsigned grid_for(sqs_ctx* ctx, uint32_t items, unsigned threads) {
+    const uint64_t want = ((uint64_t)items + threads - 1) / threads;
+    const uint64_t cap = (uint64_t)ctx->sm_count * 8;
+    return (unsigned)std::max<uint64_t>(1, std::min(want, cap));
+}
+
+// One escalation stage with the per-square cache.  Reads back the stage's
+// pair count (a stage without pairs launches nothing) and the number of
+// claimed squares (the cache is sized to exactly those).
+template <int F>
+static int cached_stage(sqs_ctx* ctx, const Pair* in, const uint32_t* in_count, uint32_t cap, Pair* next,
+                        uint32_t* next_count, const int64_t* d_s0, const Lit* d_lits, const char* d_text,
+                        PkOut* d_out, int32_t* slot_of, SqRef* list, uint32_t* list_count, int64_t S) {
+    uint32_t h_in = 0;
+    SQS_CUDA(cudaMemcpyAsync(&h_in, in_count, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    SQS_CUDA(cudaStreamSynchronize(ctx->stream));
+    h_in = std::min(h_in, cap);
+    if (h_in == 0) return SQS_OK;
+    const uint32_t list_cap = (uint32_t)std::min<int64_t>(S, 2ll * h_in);
+    SQS_CUDA(cudaMemsetAsync(slot_of, 0xff, (size_t)S * sizeof(int32_t), ctx->stream));
+    SQS_CUDA(cudaMemsetAsync(list_count, 0, sizeof(uint32_t), ctx->stream));
+    cert_mark_kernel<<<grid_for(ctx, h_in, 256), 256, 0, ctx->stream>>>(in, in_count, cap, d_s0, slot_of, list,
+                                                                         list_count, list_cap, d_out);
+    SQS_CUDA(cudaGetLastError());
+    ctx->launches += 1;
+    uint32_t h_sq = 0;
+    SQS_CUDA(cudaMemcpyAsync(&h_sq, list_count, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    SQS_CUDA(cudaStreamSynchronize(ctx->stream));
+    h_sq = std::min(h_sq, list_cap);
+    IvSq<F>* cache = nullptr;
+    if (h_sq > 0) {
+        if (int r = ctx->d_cert.reserve((size_t)h_sq * sizeof(IvSq<F>))) return r;
+        cache = (IvSq<F>*)ctx->d_cert.p;
+        cert_build_kernel<F><<<grid_for(ctx, h_sq, 128), 128, 0, ctx->stream>>>(list, list_count, list_cap, d_s0,
+                                                                                 d_lits, d_text, cache);
+        SQS_CUDA(cudaGetLastError());
+        ctx->launches += 1;
+    }
+    cert_pair_kernel<F><<<grid_for(ctx, h_in, 128), 128, 0, ctx->stream>>>(
+        in, in_count, cap, next, next_count, next ? cap : 0, d_s0, slot_of, cache, d_out);
+    SQS_CUDA(cudaGetLastError());
+    ctx->launches += 1;
+    return SQS_OK;
+}
+
 }  // namespace cert
 }  // namespace sqs
 
@@ -787,6 +928,7 @@ extern "C" int sqs_certify_batch(sqs_ctx* ctx, int count, const int32_t* n_of, c
         }
         S += n;
     }
+    SQS_REQUIRE(S < (1ll << 30), "%lld squares in one call (limit 2^30)", (long long)S);
     const char* blob = do_rt ? rt_text.data() : text;
     size_t blob_bytes = do_rt ? rt_text.size() : (size_t)lit_off[3 * row_start[count]];
     if (blob_bytes == 0) blob_bytes = 1;
@@ -807,6 +949,7 @@ extern "C" int sqs_certify_batch(sqs_ctx* ctx, int count, const int32_t* n_of, c
     const Seg g_b0 = seg(bk[0].size() * 4 + 4), g_b1 = seg(bk[1].size() * 4 + 4), g_b2 = seg(bk[2].size() * 4 + 4);
     const Seg g_lits = seg((size_t)(3 * S + 3) * sizeof(Lit)), g_out = seg((size_t)count * sizeof(PkOut));
     const Seg g_pa = seg((size_t)cap * sizeof(Pair)), g_pb = seg((size_t)cap * sizeof(Pair)), g_cnt = seg(64);
+    const Seg g_slot = seg((size_t)S * sizeof(int32_t) + 4), g_list = seg((size_t)S * sizeof(SqRef) + 8);
     if (int r = ctx->d_misc.reserve(tot)) return r;
     char* D = (char*)ctx->d_misc.p;
     auto up = [&](const Seg& s, const void* h, size_t bytes) -> int {
@@ -839,11 +982,15 @@ extern "C" int sqs_certify_batch(sqs_ctx* ctx, int count, const int32_t* n_of, c
                                          d_off, d_len, d_lits, d_out, pa, cnt, cap)) return r;
     if (int r = launch_packing<256, 1024>(ctx, (int)bk[2].size(), (const int32_t*)(D + g_b2.off), d_n, d_s0,
                                           d_text, d_off, d_len, d_lits, d_out, pa, cnt, cap)) return r;
-    const int blocks = ctx->sm_count * 8;
-    if (int r = launch_stage<7>(ctx, pa, cnt, cap, pb, cnt + 1, cap, d_s0, d_lits, d_text, d_out, blocks)) return r;
-    if (int r = launch_stage<15>(ctx, pb, cnt + 1, cap, pa, cnt + 2, cap, d_s0, d_lits, d_text, d_out, blocks))
+    int32_t* slot_of = (int32_t*)(D + g_slot.off);
+    SqRef* list = (SqRef*)(D + g_list.off);
+    if (int r = cached_stage<7>(ctx, pa, cnt, cap, pb, cnt + 1, d_s0, d_lits, d_text, d_out, slot_of, list, cnt + 3, S))
         return r;
-    if (int r = launch_stage<58>(ctx, pa, cnt + 2, cap, nullptr, nullptr, 0, d_s0, d_lits, d_text, d_out, blocks))
+    if (int r = cached_stage<15>(ctx, pb, cnt + 1, cap, pa, cnt + 2, d_s0, d_lits, d_text, d_out, slot_of, list,
+                                 cnt + 3, S))
+        return r;
+    if (int r = cached_stage<58>(ctx, pa, cnt + 2, cap, nullptr, nullptr, d_s0, d_lits, d_text, d_out, slot_of, list,
+                                 cnt + 3, S))
         return r;
     std::vector<PkOut> h((size_t)count);
     SQS_CUDA(cudaMemcpyAsync(h.data(), d_out, (size_t)count * sizeof(PkOut), cudaMemcpyDeviceToHost, ctx->stream));

@@ -64,6 +64,7 @@ struct sqs_ctx {
     int64_t launches = 0;
     // staging for the host-pointer entry points
     sqs::DevBuf d_in, d_side, d_out, d_grad, d_cand, d_misc, d_anneal;
+    sqs::DevBuf d_cert;  // the certifier's per-square interval cache
 };
 
 namespace sqs {

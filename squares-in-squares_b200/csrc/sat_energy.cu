@@ -298,10 +298,19 @@ __host__ __device__ inline size_t warp_smem_bytes(int n) {
 }
 
 // Pair-gradient sums of the warp kernel: one 32-bit integer per component in
-// units of 2^-20.  With n <= 256 a square has at most 255 partners and each
-// pair term is below 6 in magnitude, so a sum stays below 2^31 units; every
-// term is rounded once (error < 5e-7) and the sum is exact and order-free.
-constexpr float kGScale = 1048576.0f;
+// units of 2^-19.  A pair term is bounded by 2 r_max (|d| + 1/sqrt 2) =
+// 2 * 1.2071 * 2.1213 < 5.13, so with n <= 256 (at most 255 partners) a sum
+// stays below 2^31 units; every term is rounded once (error < 1e-6) and the
+// sum is exact and order-free.
+constexpr float kGScale = 524288.0f;
+
+// round(v * kGScale) to the nearest integer (ties to even) on the FMA pipe:
+// for |v * kGScale| < 2^22 the fused v * 2^19 + 1.5 * 2^23 lands in
+// [2^23, 2^24), where one float ulp is 1, so its bit pattern minus that of
+// 1.5 * 2^23 is the rounded integer.  |v| < 5.13 keeps it within range.
+__device__ __forceinline__ int gq_units(float v) {
+    return __float_as_int(fmaf(v, kGScale, 12582912.0f)) - 0x4B400000;
+}
 
 template <int W, bool COUNT>
 __global__ void __launch_bounds__(W * 32) sat_energy_warp_kernel(int configs, int n, const float* __restrict__ xya,
@@ -431,12 +440,12 @@ __global__ void __launch_bounds__(W * 32) sat_energy_warp_kernel(int configs, in
         if (sat_pair_grad(Q.x - P.x, Q.y - P.y, Pc.x, Pc.y, Qc.x, Qc.y, g)) {
             e_loc += g.e;
             const int i = orig[p], j = orig[q];
-            atomicAdd(gq + 3 * i, __float2int_rn(g.px * kGScale));
-            atomicAdd(gq + 3 * i + 1, __float2int_rn(g.py * kGScale));
-            atomicAdd(gq + 3 * i + 2, __float2int_rn(g.pa * kGScale));
-            atomicAdd(gq + 3 * j, __float2int_rn(g.qx * kGScale));
-            atomicAdd(gq + 3 * j + 1, __float2int_rn(g.qy * kGScale));
-            atomicAdd(gq + 3 * j + 2, __float2int_rn(g.qa * kGScale));
+            atomicAdd(gq + 3 * i, gq_units(g.px));
+            atomicAdd(gq + 3 * i + 1, gq_units(g.py));
+            atomicAdd(gq + 3 * i + 2, gq_units(g.pa));
+            atomicAdd(gq + 3 * j, gq_units(g.qx));
+            atomicAdd(gq + 3 * j + 1, gq_units(g.qy));
+            atomicAdd(gq + 3 * j + 2, gq_units(g.qa));
         }
     };
     for (int base0 = 0; base0 < n; base0 += 32) {

@@ -23,7 +23,8 @@ namespace sqs {
 
 constexpr float kPairCut2 = 2.000001f;  // seeded.cu:43
 
-__device__ __forceinline__ float sgnf(float v) { return (float)((v > 0.f) - (v < 0.f)); }
+// sign(v) in {-1, 0, 1} with selects only (no integer -> float conversion).
+__device__ __forceinline__ float sgnf(float v) { return v > 0.f ? 1.f : (v < 0.f ? -1.f : 0.f); }
 
 struct PairGrad {
     float e;            // gap^2
