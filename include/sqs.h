@@ -66,6 +66,8 @@ int sqs_flush_l2(sqs_ctx* ctx);
 /* Kernel launches this context issued since creation (all of libsqs's own
  * kernels; library copies/memsets are not counted). */
 int64_t sqs_launch_count(sqs_ctx* ctx);
+/* Replays of captured CUDA graphs (the annealer's slice loop) on ctx. */
+int64_t sqs_graph_replay_count(sqs_ctx* ctx);
 
 /* --------------------------------------------------------- SAT energy */
 /* FP32 cell-list SAT overlap + wall energy and gradient of `configs`
@@ -141,9 +143,10 @@ typedef struct sqs_job {
     int32_t n;               /* squares, 1..1000                                  */
     int32_t replicas;        /* temperature rungs, 1..64                          */
     int32_t sweeps;          /* sweep budget; one sweep = n proposals per replica */
-    int32_t exchange_every;  /* sweeps between replica-exchange rounds           */
+    int32_t exchange_every;  /* sweeps between replica-exchange rounds; 0 = chosen
+                                by the autotuner (needs SQS_JOB_AUTOTUNE)         */
     int32_t polish_iters;    /* FP64 gradient-polish iterations on the best state */
-    int32_t flags;           /* reserved, 0                                       */
+    int32_t flags;           /* SQS_JOB_* bits, 0 = fixed default launch shape    */
     double L0;               /* initial container side                            */
     double tmin, tmax;       /* geometric temperature ladder                      */
     double sigma_xy;         /* proposal std-dev of a centre coordinate           */
@@ -153,10 +156,29 @@ typedef struct sqs_job {
     const double* xya;       /* initial state, n rows of (x, y, angle), host      */
 } sqs_job;
 
+/* Launch shape, cell side and (when the job leaves it at 0) exchange
+ * interval from the autotuner (sqs_autotune) instead of the fixed default:
+ * the smallest cluster that fits, cells of side 1.59.  Shape and cell side
+ * do not change a job's trajectory (energies are exact fixed-point sums, the
+ * quench sums each square's gradient in one thread); only a move rejected
+ * because its target cell was full can, and sqs_job_result.overflows counts
+ * those. */
+#define SQS_JOB_AUTOTUNE 1
+/* Pin the launch shape instead: a cluster of `cs` CTAs (1..16; it must
+ * divide the replica count and fit) and cell side index k (0: 1.59, 1: 1.75,
+ * 2: 1.95, 3: 2.2).  Same trajectory as any other shape (see above). */
+#define SQS_JOB_CLUSTER(cs) ((int32_t)(cs) << 8)
+#define SQS_JOB_CELL(k) ((int32_t)(k) << 16)
+
 typedef struct sqs_job_result {
     int32_t status;          /* 0 ok; < 0 job error (see reason)                  */
     int32_t certified;       /* the interval certifier accepted the packing      */
     int32_t shrinks, improvements, sweeps_done, replicas;
+    int32_t cluster_ctas;    /* CTAs per job the job ran on                       */
+    int32_t replicas_per_cta;/* replicas (warps) per CTA                          */
+    int32_t exchange_every;  /* sweeps between exchange rounds it ran with        */
+    int32_t overflows;       /* moves rejected because the target cell was full  */
+    double cell_side;        /* minimum cell side of its cell lists               */
     double L_cert;           /* FP64 dilation-certified side of the best state    */
     double L_polished;       /* the same after the gradient polish                */
     double dilation;         /* centre dilation under which the packing certified*/
@@ -174,9 +196,32 @@ typedef struct sqs_job_result {
  * reference's `packing` / `seeded` search programs (packing.cu:768-868,
  * seeded.cu:831-983) and its certified_candidate dilation ladder
  * (demo.py:25-40).  slice_sweeps > 0 runs the jobs in slices of that many
- * sweeps (state kept resident in HBM between slices); 0 = one slice. */
+ * sweeps (state kept resident in HBM between slices); 0 = one slice.  With
+ * three or more slices the slice loop is captured once as a CUDA graph (one
+ * launch per cluster shape) and replayed.  Jobs flagged SQS_JOB_AUTOTUNE are
+ * tuned for latency when njobs == 1, for throughput otherwise. */
 int sqs_anneal_batch(sqs_ctx* ctx, const sqs_job* jobs, int njobs, int slice_sweeps, double* const* xya_out,
                      sqs_job_result* out);
+
+/* Autotuner of the batched annealer's launch: times the job's own state on
+ * every launch shape that fits (cluster size x replicas per CTA) and cell
+ * sides 1.59 .. 2.2, with the job copied to fill one wave of the GPU
+ * (throughput) or alone (latency), then, when job->exchange_every is 0, the
+ * exchange interval: the smallest of 1, 2, 5, 10, 20, 50, 100 sweeps whose
+ * checkpoint costs at most 5% of the sweeps between.  Choices are cached per
+ * process by (n rounded to a quarter octave, replicas, mode); a cached class
+ * returns at once (trials = 0).  The reference tunes its search launches
+ * offline by sweeping configurations in separate runs (cuda/autotune.py). */
+typedef struct sqs_tuning {
+    int32_t cluster_ctas;      /* CTAs per job                                  */
+    int32_t replicas_per_cta;  /* warps per CTA, one replica each               */
+    int32_t exchange_every;    /* the job's, or the tuned one when it was 0     */
+    int32_t trials;            /* timed launches (0: answered from the cache)  */
+    double cell_side;          /* minimum cell side                             */
+    double us_per_sweep;       /* device time per sweep of the chosen shape     */
+} sqs_tuning;
+#define SQS_TUNE_LATENCY 1     /* time the job alone instead of a full wave     */
+int sqs_autotune(sqs_ctx* ctx, const sqs_job* job, int mode, sqs_tuning* out);
 
 /* ------------------------------------------------------------- serving */
 /* Continuous-batching request loop for anneal-and-certify jobs on one GPU.

@@ -10,6 +10,7 @@ constexpr int kMaxR = 64;            // replicas (temperature rungs) per job
 constexpr int kMaxRl = 32;           // replicas (warps) per CTA
 constexpr int kCellK = 12;           // slot capacity of one cell
 constexpr float kCellSide = 1.59f;   // >= sqrt(2.000001) + largest centre move (0.12 * sqrt 2)
+constexpr float kCellSideMax = 2.2f; // largest cell side the autotuner tries
 constexpr float kMaxStep = 0.12f;    // clamp of each proposal coordinate
 constexpr int kMaxN = 1000;
 
@@ -19,7 +20,7 @@ struct JobDev {
     int32_t sweeps_total, exchange_every;
     int32_t Gmax, polish_iters;       // cell grid side for the initial container; polish iterations
     float sigma_xy, sigma_a, tmin, tmax;
-    float shrink, L0, pad0, pad1;
+    float shrink, L0, cell, pad1;     // cell: minimum cell side of the cell lists (>= kCellSide)
     uint64_t seed;
     int64_t pos_off;                  // float4 index of replica 0, square 0
     int64_t best_off;                 // double index of the best state (n x 3)
@@ -33,7 +34,8 @@ struct JobMut {
     int32_t sweep;                    // sweeps completed
     int32_t xround;                   // exchange rounds completed
     int32_t status;                   // 0 running, 1 finished, < 0 error
-    int32_t shrinks, improvements, pad0, pad1;
+    int32_t shrinks, improvements;
+    int32_t overflows, pad1;          // overflows: moves rejected because the target cell was full
     double best_L;                    // best FP64 dilation-certified side (1e30: none yet)
     uint64_t proposals, accepted, xatt, xacc;
     int32_t perm[kMaxR];              // rung (temperature index) of each replica

@@ -15,7 +15,9 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "anneal_host.h"
@@ -25,11 +27,13 @@ namespace ann {
 
 constexpr size_t kSmemLimit = 232448 - 4096;  // dynamic shared memory per CTA (static part reserved)
 
-// Smallest cluster (CTAs per job) whose per-CTA replica share fits.
-static bool plan_job(int n, int R, double L0, Plan& p) {
-    p.Gmax = std::max(1, (int)(L0 / (double)kCellSide));
+// Smallest cluster (CTAs per job), from cs_min up, whose per-CTA replica
+// share fits, with cells of side at least `cell`.
+static bool plan_job(int n, int R, double L0, float cell, int cs_min, Plan& p) {
+    p.cell = cell;
+    p.Gmax = std::max(1, (int)(L0 / (double)cell));
     p.rb = replica_smem_bytes(n, p.Gmax);
-    for (int cs = 1; cs <= 16; ++cs) {
+    for (int cs = std::max(1, cs_min); cs <= 16; ++cs) {
         if (R % cs) continue;
         const int Rl = R / cs;
         if (Rl > kMaxRl) continue;
@@ -66,7 +70,7 @@ void put(char* dst, size_t cap, const std::string& s) {
     dst[k] = 0;
 }
 
-int prepare_job(const sqs_job& J, int j, JobDev& d, JobMut& m, Plan& p) {
+int prepare_job(const sqs_job& J, int j, JobDev& d, JobMut& m, Plan& p, const Shape* shape) {
     SQS_REQUIRE(J.n >= 1 && J.n <= kMaxN, "job %d: n=%d out of 1..%d", j, J.n, kMaxN);
     SQS_REQUIRE(J.replicas >= 1 && J.replicas <= kMaxR, "job %d: replicas=%d out of 1..%d", j, J.replicas, kMaxR);
     SQS_REQUIRE(J.sweeps >= 0 && J.sweeps <= 100000000, "job %d: sweeps=%d out of range", j, J.sweeps);
@@ -79,8 +83,9 @@ int prepare_job(const sqs_job& J, int j, JobDev& d, JobMut& m, Plan& p) {
     SQS_REQUIRE(J.polish_iters >= 0 && J.polish_iters <= 100000, "job %d: polish_iters out of range", j);
     SQS_REQUIRE(J.xya != nullptr, "job %d: null initial state", j);
     for (int i = 0; i < 3 * J.n; ++i) SQS_REQUIRE(std::isfinite(J.xya[i]), "job %d: non-finite initial coordinate", j);
-    SQS_REQUIRE(plan_job(J.n, J.replicas, J.L0, p), "job %d: n=%d with %d replicas does not fit a cluster of <= 16 CTAs",
-                j, J.n, J.replicas);
+    const bool tuned = shape && shape->cs > 0;
+    SQS_REQUIRE(plan_job(J.n, J.replicas, J.L0, tuned ? shape->cell : kCellSide, tuned ? shape->cs : 1, p),
+                "job %d: n=%d with %d replicas does not fit a cluster of <= 16 CTAs", j, J.n, J.replicas);
     std::memset(&d, 0, sizeof d);
     d.n = J.n;
     d.R = J.replicas;
@@ -96,6 +101,7 @@ int prepare_job(const sqs_job& J, int j, JobDev& d, JobMut& m, Plan& p) {
     d.tmax = (float)J.tmax;
     d.shrink = (float)J.shrink;
     d.L0 = (float)J.L0;
+    d.cell = p.cell;
     d.seed = J.seed;
     d.quench_iters = 64;
     std::memset(&m, 0, sizeof m);
@@ -115,8 +121,13 @@ void init_replicas(const sqs_job& J, float4* dst) {
                 make_float4((float)J.xya[3 * i], (float)J.xya[3 * i + 1], (float)wrap_quarter(J.xya[3 * i + 2]), 0.f);
 }
 
-void fill_result(const sqs_job& J, const JobMut& m, float dev_ms, sqs_job_result& o) {
+void fill_result(const sqs_job& J, const JobDev& d, const JobMut& m, float dev_ms, sqs_job_result& o) {
     o.status = m.status == kFinished ? 0 : (m.status < 0 ? m.status : SQS_ETIMEOUT);
+    o.cluster_ctas = d.cs;
+    o.replicas_per_cta = d.Rl;
+    o.exchange_every = d.exchange_every;
+    o.overflows = m.overflows;
+    o.cell_side = d.cell;
     o.shrinks = m.shrinks;
     o.improvements = m.improvements;
     o.sweeps_done = m.sweep;
@@ -137,6 +148,214 @@ void fill_result(const sqs_job& J, const JobMut& m, float dev_ms, sqs_job_result
 // (cuda/polish.py:52-65): the first centre dilation in 1+1e-10 .. 1+1e-6
 // under which the GPU certifier accepts the packing.  `best[k]` is job k's
 // n x 3 FP64 state; results go to out[k] and, when certified, xya_out[k].
+// ------------------------------------------------------------ autotuner
+// Candidate launch shapes of a job: every cluster size that divides the
+// replica count and fits, for each cell side; each is timed on the job's own
+// initial state (copies of the job fill one wave of the GPU in throughput
+// mode; the job runs alone in latency mode) and the fastest wins.  Shape and
+// cell side leave the trajectory unchanged (see SQS_JOB_AUTOTUNE), so the
+// choice only moves time.  The reference's counterpart is an offline launch
+// matrix run as separate processes and summarised afterwards
+// (cuda/autotune.py:8-41).
+namespace {
+struct TuneVal {
+    int cs;
+    float cell;
+    int xe;       // tuned exchange interval (0: not tuned)
+    double us;    // device microseconds per sweep
+};
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int, int>, TuneVal> g_tune;  // (device, n class, R, mode, exchange tuned)
+constexpr float kTuneCells[] = {kCellSide, 1.75f, 1.95f, kCellSideMax};
+constexpr int kTuneXe[] = {1, 2, 5, 10, 20, 50, 100};
+constexpr size_t kTuneBytes = (size_t)1 << 30;  // trial state cap
+
+int n_class(int n) { return (int)std::floor(4.0 * std::log2((double)n)); }
+}  // namespace
+
+// Device milliseconds of `copies` copies of J (sweeps, exchange interval and
+// plan fixed), the best of `reps` runs, each from the initial state.
+static int trial_ms(sqs_ctx* ctx, const sqs_job& J0, const Plan& p, int copies, int sweeps, int xe, int reps,
+                    float* ms) {
+    sqs_job J = J0;
+    J.sweeps = sweeps;
+    J.exchange_every = xe;
+    J.polish_iters = 0;
+    JobDev d;
+    JobMut m;
+    Plan q;
+    Shape sh;
+    sh.cs = p.cs;
+    sh.cell = p.cell;
+    if (int r = prepare_job(J, 0, d, m, q, &sh)) return r;
+    const int64_t pe = job_pos_elems(J);
+    size_t tot = 0;
+    auto seg = [&](size_t b) { size_t o = tot; tot += (b + 255) & ~(size_t)255; return o; };
+    const size_t o_jd = seg(sizeof(JobDev) * copies), o_jm = seg(sizeof(JobMut) * copies);
+    const size_t o_pos = seg(sizeof(float4) * (size_t)pe * copies);
+    const size_t o_best = seg(sizeof(double) * 3 * (size_t)J.n * copies), o_list = seg(sizeof(int32_t) * copies);
+    if (int r = ctx->d_tune.reserve(tot)) return r;
+    char* D = (char*)ctx->d_tune.p;
+    std::vector<JobDev> jd((size_t)copies, d);
+    std::vector<JobMut> jm((size_t)copies, m);
+    std::vector<int32_t> list((size_t)copies);
+    for (int c = 0; c < copies; ++c) {
+        jd[(size_t)c].pos_off = (int64_t)c * pe;
+        jd[(size_t)c].scr_off = (int64_t)c * pe + (int64_t)J.replicas * J.n;
+        jd[(size_t)c].best_off = (int64_t)c * 3 * J.n;
+        list[(size_t)c] = c;
+    }
+    std::vector<float4> pos((size_t)pe);
+    init_replicas(J, pos.data());
+    SQS_CUDA(cudaMemcpyAsync(D + o_jd, jd.data(), sizeof(JobDev) * copies, cudaMemcpyHostToDevice, ctx->stream));
+    SQS_CUDA(cudaMemcpyAsync(D + o_list, list.data(), sizeof(int32_t) * copies, cudaMemcpyHostToDevice, ctx->stream));
+    float best = 1e30f;
+    for (int rep = 0; rep < reps; ++rep) {
+        SQS_CUDA(cudaMemcpyAsync(D + o_jm, jm.data(), sizeof(JobMut) * copies, cudaMemcpyHostToDevice, ctx->stream));
+        for (int c = 0; c < copies; ++c)
+            SQS_CUDA(cudaMemcpyAsync(D + o_pos + sizeof(float4) * (size_t)pe * c, pos.data(), sizeof(float4) * pos.size(),
+                                     cudaMemcpyHostToDevice, ctx->stream));
+        SQS_CUDA(cudaEventRecord(ctx->ev[60], ctx->stream));
+        if (int r = launch_anneal(ctx->stream, copies, p.cs, p.Rl, (size_t)(p.rb * p.Rl), (const int32_t*)(D + o_list),
+                                  (const JobDev*)(D + o_jd), (JobMut*)(D + o_jm), (float4*)(D + o_pos),
+                                  (double*)(D + o_best), sweeps))
+            return r;
+        ctx->launches += 1;
+        SQS_CUDA(cudaEventRecord(ctx->ev[61], ctx->stream));
+        SQS_CUDA(cudaStreamSynchronize(ctx->stream));
+        float t = 0.f;
+        SQS_CUDA(cudaEventElapsedTime(&t, ctx->ev[60], ctx->ev[61]));
+        best = std::min(best, t);
+    }
+    *ms = best;
+    return SQS_OK;
+}
+
+static int copies_for(const sqs_job& J, const Plan& p, int mode, int* copies) {
+    *copies = 1;
+    if (mode & SQS_TUNE_LATENCY) return SQS_OK;
+    int waves = 1;
+    if (int r = anneal_max_clusters(p.cs, p.Rl, (size_t)(p.rb * p.Rl), &waves)) return r;
+    const size_t per = sizeof(float4) * (size_t)job_pos_elems(J) + sizeof(double) * 3 * (size_t)J.n + 1024;
+    *copies = (int)std::max<int64_t>(1, std::min<int64_t>(waves, (int64_t)(kTuneBytes / per)));
+    return SQS_OK;
+}
+
+static int autotune(sqs_ctx* ctx, const sqs_job& job, int mode, sqs_tuning& out) {
+    std::memset(&out, 0, sizeof out);
+    sqs_job J = job;
+    const bool tune_xe = J.exchange_every <= 0;
+    if (tune_xe) J.exchange_every = 10;  // interval used while shapes are compared
+    {
+        JobDev d;
+        JobMut m;
+        Plan p;
+        if (int r = prepare_job(J, 0, d, m, p)) return r;  // validates the job
+    }
+    const auto key = std::make_tuple(ctx->device, n_class(J.n), J.replicas, mode & SQS_TUNE_LATENCY, (int)tune_xe);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) {
+            Plan p;
+            // a class member with a larger n may need a larger cluster for the same cell side
+            if (plan_job(J.n, J.replicas, J.L0, it->second.cell, it->second.cs, p) ||
+                plan_job(J.n, J.replicas, J.L0, it->second.cell, 1, p)) {
+                out.cluster_ctas = p.cs;
+                out.replicas_per_cta = p.Rl;
+                out.cell_side = p.cell;
+                out.exchange_every = tune_xe ? it->second.xe : job.exchange_every;
+                out.us_per_sweep = it->second.us;
+                out.trials = 0;
+                return SQS_OK;
+            }
+        }
+    }
+    const int sweeps = std::max(2, std::min(100, (2000 + J.n - 1) / J.n));
+    const int xe = std::min(J.exchange_every, sweeps);
+    Plan best{};
+    float best_ms = 1e30f;
+    int trials = 0;
+    for (float cell : kTuneCells) {
+        for (int cs = 1; cs <= 16; ++cs) {
+            Plan p;
+            if (!plan_job(J.n, J.replicas, J.L0, cell, cs, p) || p.cs != cs) continue;
+            int copies = 1;
+            if (int r = copies_for(J, p, mode, &copies)) return r;
+            float ms = 0.f;
+            if (int r = trial_ms(ctx, J, p, copies, sweeps, xe, 2, &ms)) return r;
+            trials += 2;
+            const float per_copy = ms / (float)copies;  // throughput: time per job
+            if (per_copy < best_ms) {
+                best_ms = per_copy;
+                best = p;
+            }
+        }
+    }
+    SQS_REQUIRE(best_ms < 1e29f, "autotune: no launch shape fits n=%d with %d replicas", J.n, J.replicas);
+    int xe_best = job.exchange_every;
+    if (tune_xe) {
+        // checkpoint cost c and sweep cost s from T sweeps with 1 and with T checkpoints
+        const int T = std::max(8, sweeps);
+        int copies = 1;
+        if (int r = copies_for(J, best, mode, &copies)) return r;
+        float a = 0.f, b = 0.f;
+        if (int r = trial_ms(ctx, J, best, copies, T, T, 2, &a)) return r;
+        if (int r = trial_ms(ctx, J, best, copies, T, 1, 2, &b)) return r;
+        trials += 4;
+        const double c = std::max(0.0, (double)(b - a) / (double)(T - 1));
+        const double sw = std::max(1e-9, ((double)a - c) / (double)T);
+        xe_best = kTuneXe[sizeof(kTuneXe) / sizeof(kTuneXe[0]) - 1];
+        for (int x : kTuneXe) {
+            if (c <= 0.05 * (double)x * sw) {
+                xe_best = x;
+                break;
+            }
+        }
+    }
+    const double us = 1e3 * (double)best_ms / (double)sweeps;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune[key] = TuneVal{best.cs, best.cell, tune_xe ? xe_best : 0, us};
+    }
+    out.cluster_ctas = best.cs;
+    out.replicas_per_cta = best.Rl;
+    out.cell_side = best.cell;
+    out.exchange_every = xe_best;
+    out.us_per_sweep = us;
+    out.trials = trials;
+    return SQS_OK;
+}
+
+int resolve_job(sqs_ctx* ctx, const sqs_job& job, int mode, sqs_job& eff, Shape& shape) {
+    eff = job;
+    shape = Shape{};
+    SQS_REQUIRE((job.flags & ~0xfff01) == 0, "unknown job flags 0x%x", (unsigned)job.flags);
+    const int pin_cs = (job.flags >> 8) & 0xff, pin_cell = (job.flags >> 16) & 0xf;
+    if (pin_cs || pin_cell) {
+        SQS_REQUIRE(!(job.flags & SQS_JOB_AUTOTUNE), "SQS_JOB_AUTOTUNE and a pinned shape exclude each other");
+        SQS_REQUIRE(pin_cs <= 16 && pin_cell < (int)(sizeof(kTuneCells) / sizeof(kTuneCells[0])),
+                    "pinned shape out of range (cluster %d, cell index %d)", pin_cs, pin_cell);
+        shape.cell = kTuneCells[pin_cell];
+        Plan p;
+        SQS_REQUIRE(job.n >= 1 && job.n <= kMaxN && job.replicas >= 1 && job.replicas <= kMaxR &&
+                        std::isfinite(job.L0) && job.L0 > 0 && job.L0 <= 64,
+                    "job out of range");
+        SQS_REQUIRE(plan_job(job.n, job.replicas, job.L0, shape.cell, std::max(1, pin_cs), p) &&
+                        (pin_cs == 0 || p.cs == pin_cs),
+                    "pinned cluster of %d CTAs does not fit n=%d with %d replicas", pin_cs, job.n, job.replicas);
+        shape.cs = p.cs;
+        return SQS_OK;
+    }
+    if (!(job.flags & SQS_JOB_AUTOTUNE)) return SQS_OK;
+    sqs_tuning t;
+    if (int r = autotune(ctx, job, mode, t)) return r;
+    shape.cs = t.cluster_ctas;
+    shape.cell = (float)t.cell_side;
+    if (job.exchange_every <= 0) eff.exchange_every = t.exchange_every;
+    return SQS_OK;
+}
+
 int certify_states(sqs_ctx* ctx, const std::vector<int>& ns, const std::vector<const double*>& best,
                    const std::vector<sqs_job_result*>& out, const std::vector<double*>& xya_out) {
     static const double ladder[5] = {1 + 1e-10, 1 + 1e-9, 1 + 1e-8, 1 + 1e-7, 1 + 1e-6};
@@ -204,10 +423,14 @@ extern "C" int sqs_anneal_batch(sqs_ctx* ctx, const sqs_job* jobs, int njobs, in
     std::vector<JobDev> jd((size_t)njobs);
     std::vector<JobMut> jm((size_t)njobs);
     std::vector<Plan> plan((size_t)njobs);
+    std::vector<sqs_job> eff((size_t)njobs);
     int64_t pos_total = 0, best_total = 0;
+    const int mode = njobs == 1 ? SQS_TUNE_LATENCY : 0;
     for (int j = 0; j < njobs; ++j) {
         std::memset(&out[j], 0, sizeof(sqs_job_result));
-        if (int r = prepare_job(jobs[j], j, jd[(size_t)j], jm[(size_t)j], plan[(size_t)j])) return r;
+        Shape shape;
+        if (int r = resolve_job(ctx, jobs[j], mode, eff[(size_t)j], shape)) return r;
+        if (int r = prepare_job(eff[(size_t)j], j, jd[(size_t)j], jm[(size_t)j], plan[(size_t)j], &shape)) return r;
         jd[(size_t)j].pos_off = pos_total;
         jd[(size_t)j].best_off = best_total;
         jd[(size_t)j].scr_off = pos_total + (int64_t)jobs[j].replicas * jobs[j].n;
@@ -262,17 +485,48 @@ extern "C" int sqs_anneal_batch(sqs_ctx* ctx, const sqs_job* jobs, int njobs, in
     }
     // a slice is a whole number of exchange blocks of every job
     int slice = slice_sweeps > 0 ? slice_sweeps : std::max(1, max_sweeps);
+    if (int r = prime_anneal()) return r;
     cudaEvent_t e0 = ctx->ev[62], e1 = ctx->ev[63];
     SQS_CUDA(cudaEventRecord(e0, ctx->stream));
-    const int rounds = (max_sweeps + slice - 1) / slice;
-    for (int k = 0; k < std::max(1, rounds); ++k) {
+    const int rounds = std::max(1, (max_sweeps + slice - 1) / slice);
+    auto one_round = [&]() -> int {
         for (size_t g = 0; g < keys.size(); ++g) {
             if (int r = launch_anneal(ctx->stream, (int)spans[g].second, keys[g].first, keys[g].second, smems[g],
                                       d_list + spans[g].first, d_jd, d_jm, d_pos, d_best, slice))
                 return r;
-            ctx->launches += 1;
         }
+        return SQS_OK;
+    };
+    if (rounds < 3) {
+        for (int k = 0; k < rounds; ++k)
+            if (int r = one_round()) return r;
+    } else {
+        // the slice loop as a CUDA graph: one round (a launch per cluster
+        // shape) captured once and replayed; every launch reads its jobs'
+        // progress from device memory, so the replays need no host updates
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        SQS_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = one_round();
+        const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+        if (rc != SQS_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        SQS_CUDA(ce);
+        cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+        if (ie != cudaSuccess) {
+            cudaGraphDestroy(graph);
+            SQS_CUDA(ie);
+        }
+        cudaError_t le = cudaSuccess;
+        for (int k = 0; k < rounds && le == cudaSuccess; ++k) le = cudaGraphLaunch(exec, ctx->stream);
+        cudaGraphExecDestroy(exec);
+        cudaGraphDestroy(graph);
+        SQS_CUDA(le);
+        ctx->graph_replays += rounds;
     }
+    ctx->launches += (int64_t)rounds * (int64_t)keys.size();
     // FP64 gradient polish of every job's best state (jobs with polish_iters > 0)
     size_t psmem = 0;
     for (int j = 0; j < njobs; ++j) psmem = std::max(psmem, polish_smem_bytes(jobs[j].n));
@@ -293,7 +547,7 @@ extern "C" int sqs_anneal_batch(sqs_ctx* ctx, const sqs_job* jobs, int njobs, in
     std::vector<sqs_job_result*> optr;
     std::vector<double*> xptr;
     for (int j = 0; j < njobs; ++j) {
-        fill_result(jobs[j], jm[(size_t)j], dev_ms, out[j]);
+        fill_result(eff[(size_t)j], jd[(size_t)j], jm[(size_t)j], dev_ms, out[j]);
         const JobMut& m = jm[(size_t)j];
         if (m.status == kErrCells || m.best_L >= 1e29) continue;
         ns.push_back(jobs[j].n);
@@ -303,4 +557,11 @@ extern "C" int sqs_anneal_batch(sqs_ctx* ctx, const sqs_job* jobs, int njobs, in
     }
     if (int r = certify_states(ctx, ns, bptr, optr, xptr)) return r;
     return SQS_OK;
+}
+
+extern "C" int sqs_autotune(sqs_ctx* ctx, const sqs_job* job, int mode, sqs_tuning* out) {
+    if (int r = enter(ctx)) return r;
+    SQS_REQUIRE(job && out, "null argument");
+    SQS_REQUIRE((mode & ~SQS_TUNE_LATENCY) == 0, "unknown tuning mode %d", mode);
+    return autotune(ctx, *job, mode, *out);
 }

@@ -12,9 +12,18 @@ namespace ann {
 
 struct Plan {
     int cs, Rl, Gmax;
-    int64_t rb;  // shared-memory bytes of one replica
+    int64_t rb;   // shared-memory bytes of one replica
+    float cell;   // minimum cell side
 };
 
+// A launch shape chosen by the autotuner (cs = 0: none, use the default plan).
+struct Shape {
+    int cs = 0;
+    float cell = kCellSide;
+};
+
+int prime_anneal();
+int anneal_max_clusters(int cs, int Rl, size_t smem, int* out);
 int launch_anneal(cudaStream_t stream, int njobs, int cs, int Rl, size_t smem, const int32_t* job_list,
                   const JobDev* jdev, JobMut* jmut, float4* pos, double* best, int slice);
 int launch_polish(cudaStream_t stream, int njobs, const int32_t* job_list, const JobDev* jdev, JobMut* jmut,
@@ -23,12 +32,18 @@ size_t polish_smem_bytes(int n);
 
 void put(char* dst, size_t cap, const std::string& s);
 // Validate one job and fill its device records (offsets left to the caller).
-int prepare_job(const sqs_job& J, int j, JobDev& d, JobMut& m, Plan& p);
+// `shape` (optional) fixes the cluster size and cell side instead of the
+// default (smallest cluster that fits, cells of side kCellSide).
+int prepare_job(const sqs_job& J, int j, JobDev& d, JobMut& m, Plan& p, const Shape* shape = nullptr);
+// Resolve SQS_JOB_AUTOTUNE: the tuned shape of the job's class (tuning it on
+// first sight) and, when the job leaves exchange_every at 0, the tuned
+// interval written into `eff` (a copy of the job).  No flag: eff = job.
+int resolve_job(sqs_ctx* ctx, const sqs_job& job, int mode, sqs_job& eff, Shape& shape);
 // float4 elements of a job's state region: R*n replica squares + 2n quench scratch.
 int64_t job_pos_elems(const sqs_job& J);
 // Every replica starts from the job's initial state (angles wrapped to [0, pi/2)).
 void init_replicas(const sqs_job& J, float4* dst);
-void fill_result(const sqs_job& J, const JobMut& m, float dev_ms, sqs_job_result& o);
+void fill_result(const sqs_job& J, const JobDev& d, const JobMut& m, float dev_ms, sqs_job_result& o);
 int certify_states(sqs_ctx* ctx, const std::vector<int>& ns, const std::vector<const double*>& best,
                    const std::vector<sqs_job_result*>& out, const std::vector<double*>& xya_out);
 

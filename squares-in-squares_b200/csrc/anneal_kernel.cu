@@ -62,9 +62,9 @@ struct Grid {
     }
 };
 
-__device__ __forceinline__ Grid make_grid(float L, int Gmax) {
+__device__ __forceinline__ Grid make_grid(float L, int Gmax, float cell) {
     Grid g;
-    int G = (int)(L / kCellSide);
+    int G = (int)(L / cell);
     g.G = G < 1 ? 1 : (G > Gmax ? Gmax : G);
     g.inv = (float)g.G / L;
     return g;
@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(1024) anneal_kernel(const int32_t* __restrict_
     const int64_t rb = replica_smem_bytes(n, jd.Gmax);
     Rep rep = rep_view(dyn + (active ? w : 0) * rb, n, jd.Gmax);
     float L = S.jm.L;
-    Grid g = make_grid(L, jd.Gmax);
+    Grid g = make_grid(L, jd.Gmax, jd.cell);
     const uint32_t k0 = (uint32_t)jd.seed, k1 = (uint32_t)(jd.seed >> 32);
 
     // load the replica
@@ -458,6 +458,7 @@ __global__ void __launch_bounds__(1024) anneal_kernel(const int32_t* __restrict_
         E = S.jm.sweep == 0 ? full_energy(rep, n, g, L, lane) : S.jm.E[r];
     }
     unsigned long long props = 0, accs = 0;
+    int ovf = 0;
     float invT = active ? 1.0f / S.temps[S.jm.perm[r]] : 0.f;
 
     const int sweep0 = S.jm.sweep;
@@ -506,7 +507,10 @@ __global__ void __launch_bounds__(1024) anneal_kernel(const int32_t* __restrict_
                 bool acc = dq <= 0 || u01(b1) < __expf(-de * invT);
                 const int ncx = g.cx(nx), ncy = g.cx(ny);
                 const int oc = ocy * g.G + ocx, ncell = ncy * g.G + ncx;
-                if (acc && oc != ncell && rep.cnt[ncell] >= kCellK) acc = false;
+                if (acc && oc != ncell && rep.cnt[ncell] >= kCellK) {
+                    acc = false;
+                    ++ovf;
+                }
                 ++props;
                 if (acc) {
                     ++accs;
@@ -635,7 +639,7 @@ __global__ void __launch_bounds__(1024) anneal_kernel(const int32_t* __restrict_
         if (S.newL < L) {
             const float f = S.newL / L;
             L = S.newL;
-            g = make_grid(L, jd.Gmax);
+            g = make_grid(L, jd.Gmax, jd.cell);
             if (active) {
                 for (int i = lane; i < n; i += 32) {
                     rep.sq[i].x *= f;
@@ -672,6 +676,7 @@ __global__ void __launch_bounds__(1024) anneal_kernel(const int32_t* __restrict_
             jmut[job].E[r] = E;
             atomicAdd(reinterpret_cast<unsigned long long*>(&jmut[job].proposals), props);
             atomicAdd(reinterpret_cast<unsigned long long*>(&jmut[job].accepted), accs);
+            if (ovf) atomicAdd(&jmut[job].overflows, ovf);
         }
     }
     if (rank == 0 && tid == 0) {
@@ -689,11 +694,12 @@ __global__ void __launch_bounds__(1024) anneal_kernel(const int32_t* __restrict_
     }
 }
 
-int launch_anneal(cudaStream_t stream, int njobs, int cs, int Rl, size_t smem, const int32_t* job_list,
-                  const JobDev* jdev, JobMut* jmut, float4* pos, double* best, int slice) {
+// Kernel attributes (dynamic shared memory up to the opt-in limit,
+// non-portable cluster sizes), once per device; call before any capture.
+int prime_anneal() {
     static bool attr_done[64] = {false};
     int dev = 0;
-    cudaGetDevice(&dev);
+    SQS_CUDA(cudaGetDevice(&dev));
     if (!attr_done[dev & 63]) {
         cudaFuncAttributes fa;
         SQS_CUDA(cudaFuncGetAttributes(&fa, anneal_kernel));
@@ -702,6 +708,32 @@ int launch_anneal(cudaStream_t stream, int njobs, int cs, int Rl, size_t smem, c
         SQS_CUDA(cudaFuncSetAttribute(anneal_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
         attr_done[dev & 63] = true;
     }
+    return SQS_OK;
+}
+
+// Clusters of this shape that can be resident at once (one wave).
+int anneal_max_clusters(int cs, int Rl, size_t smem, int* out) {
+    if (int r = prime_anneal()) return r;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)cs, 1, 1);
+    cfg.blockDim = dim3((unsigned)(Rl * 32), 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int num = 0;
+    SQS_CUDA(cudaOccupancyMaxActiveClusters(&num, anneal_kernel, &cfg));
+    *out = num;
+    return SQS_OK;
+}
+
+int launch_anneal(cudaStream_t stream, int njobs, int cs, int Rl, size_t smem, const int32_t* job_list,
+                  const JobDev* jdev, JobMut* jmut, float4* pos, double* best, int slice) {
+    if (int r = prime_anneal()) return r;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(njobs * cs), 1, 1);
     cfg.blockDim = dim3((unsigned)(Rl * 32), 1, 1);

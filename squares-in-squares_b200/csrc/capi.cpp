@@ -114,6 +114,7 @@ int sqs_ctx_destroy(sqs_ctx* ctx) {
     ctx->d_misc.release();
     ctx->d_anneal.release();
     ctx->d_cert.release();
+    ctx->d_tune.release();
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SQS_OK;
@@ -205,5 +206,6 @@ int sqs_flush_l2(sqs_ctx* ctx) {
 }
 
 int64_t sqs_launch_count(sqs_ctx* ctx) { return ctx ? ctx->launches : -1; }
+int64_t sqs_graph_replay_count(sqs_ctx* ctx) { return ctx ? ctx->graph_replays : -1; }
 
 }  // extern "C"

@@ -62,9 +62,11 @@ struct sqs_ctx {
     void* flush = nullptr;
     size_t flush_bytes = 0;
     int64_t launches = 0;
+    int64_t graph_replays = 0;  // CUDA-graph launches of captured slice loops
     // staging for the host-pointer entry points
     sqs::DevBuf d_in, d_side, d_out, d_grad, d_cand, d_misc, d_anneal;
     sqs::DevBuf d_cert;  // the certifier's per-square interval cache
+    sqs::DevBuf d_tune;  // the annealer autotuner's trial state
 };
 
 namespace sqs {

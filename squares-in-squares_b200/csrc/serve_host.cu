@@ -189,12 +189,15 @@ extern "C" int sqs_server_destroy(sqs_server* s) {
 
 extern "C" int sqs_server_submit(sqs_server* s, const sqs_job* job, int64_t* id) {
     SQS_REQUIRE(s && job && id, "null argument");
+    SQS_REQUIRE(job->xya != nullptr || job->n <= 0, "null initial state");
+    if (int r = enter(s->ctx)) return r;
     SJob j;
     j.id = s->next_id;
-    j.job = *job;
+    Shape shape;
+    if (int r = resolve_job(s->ctx, *job, 0, j.job, shape)) return r;
     j.xya.assign(job->xya, job->xya + 3 * (size_t)std::max(0, job->n));
     j.job.xya = j.xya.data();
-    if (int r = prepare_job(j.job, 0, j.jd, j.jm, j.plan)) return r;
+    if (int r = prepare_job(j.job, 0, j.jd, j.jm, j.plan, &shape)) return r;
     SQS_REQUIRE(job_bytes(j.job) <= s->arena_bytes, "job state (%zu bytes) exceeds the server's HBM budget",
                 job_bytes(j.job));
     *id = j.id;
@@ -205,7 +208,7 @@ extern "C" int sqs_server_submit(sqs_server* s, const sqs_job* job, int64_t* id)
     stored.job.xya = stored.xya.data();  // the vector moved with the record
     if (stored.jm.status != kRunning) {   // zero-sweep job: nothing to anneal
         stored.state = kDone;
-        fill_result(stored.job, stored.jm, 0.f, stored.res);
+        fill_result(stored.job, stored.jd, stored.jm, 0.f, stored.res);
     } else {
         s->queue.push_back(key);
     }
@@ -281,7 +284,7 @@ extern "C" int sqs_server_step(sqs_server* s, int* in_flight) {
         for (size_t q = 0; q < fin.size(); ++q) {
             SJob& j = s->jobs[s->slot_job[(size_t)fin[q]]];
             j.res = sqs_job_result{};
-            fill_result(j.job, s->h_jm[(size_t)fin[q]], 0.f, j.res);
+            fill_result(j.job, j.jd, s->h_jm[(size_t)fin[q]], 0.f, j.res);
             if (j.cancel) {
                 j.res.status = SQS_ENOTFOUND;
                 put(j.res.reason, sizeof j.res.reason, "cancelled");

@@ -48,10 +48,22 @@ class JobResult(C.Structure):
     """sqs_job_result (include/sqs.h)."""
     _fields_ = [("status", C.c_int32), ("certified", C.c_int32), ("shrinks", C.c_int32),
                 ("improvements", C.c_int32), ("sweeps_done", C.c_int32), ("replicas", C.c_int32),
+                ("cluster_ctas", C.c_int32), ("replicas_per_cta", C.c_int32), ("exchange_every", C.c_int32),
+                ("overflows", C.c_int32), ("cell_side", C.c_double),
                 ("L_cert", C.c_double), ("L_polished", C.c_double), ("dilation", C.c_double),
                 ("score", C.c_double), ("proposals", C.c_int64), ("accepted", C.c_int64),
                 ("exchange_attempts", C.c_int64), ("exchange_accepts", C.c_int64), ("device_ms", C.c_double),
                 ("L", C.c_char * 80), ("reason", C.c_char * 112)]
+
+
+class Tuning(C.Structure):
+    """sqs_tuning (include/sqs.h)."""
+    _fields_ = [("cluster_ctas", C.c_int32), ("replicas_per_cta", C.c_int32), ("exchange_every", C.c_int32),
+                ("trials", C.c_int32), ("cell_side", C.c_double), ("us_per_sweep", C.c_double)]
+
+
+JOB_AUTOTUNE = 1
+TUNE_LATENCY = 1
 
 
 # name -> (restype, argtypes)
@@ -74,6 +86,7 @@ SIGNATURES: dict[str, tuple] = {
     "sqs_event_elapsed": (C.c_int, [_vp, C.c_int, C.c_int, _fp]),
     "sqs_flush_l2": (C.c_int, [_vp]),
     "sqs_launch_count": (C.c_int64, [_vp]),
+    "sqs_graph_replay_count": (C.c_int64, [_vp]),
     "sqs_sat_energy": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_int]),
     "sqs_sat_energy_host": (C.c_int, [_vp, C.c_int, C.c_int, _fp, _fp, _fp, _fp, _u32p]),
     "sqs_certify_batch": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, C.c_char_p, _vp, C.c_int, C.POINTER(Verdict)]),
@@ -87,6 +100,7 @@ SIGNATURES: dict[str, tuple] = {
     "sqs_server_step": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "sqs_server_poll": (C.c_int, [_vp, C.c_int64, C.POINTER(JobResult), C.POINTER(C.c_double)]),
     "sqs_server_cancel": (C.c_int, [_vp, C.c_int64]),
+    "sqs_autotune": (C.c_int, [_vp, C.POINTER(Job), C.c_int, C.POINTER(Tuning)]),
     "sqs_server_info": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_size_t)]),
 }
 
@@ -214,6 +228,9 @@ class Context:
 
     def launches(self) -> int:
         return int(lib().sqs_launch_count(self.handle))
+
+    def graph_replays(self) -> int:
+        return int(lib().sqs_graph_replay_count(self.handle))
 
     def alloc(self, shape, dtype) -> DeviceArray:
         return DeviceArray(self, shape, dtype)

@@ -35,6 +35,9 @@ class AnnealJob:
     shrink: float = 0.001
     seed: int = 42
     polish_iters: int = 200
+    autotune: bool = False          # launch shape / cell side (and exchange_every=0) from the autotuner
+    cluster: int = 0                # pinned cluster size (0: default / tuned)
+    cell_index: int = 0             # pinned cell side index (0: 1.59, 1: 1.75, 2: 1.95, 3: 2.2)
     n: int = field(init=False)
 
     def __post_init__(self):
@@ -44,7 +47,7 @@ class AnnealJob:
 
 def _cjob(j: AnnealJob) -> N.Job:
     return N.Job(n=j.n, replicas=j.replicas, sweeps=j.sweeps, exchange_every=j.exchange_every,
-                 polish_iters=j.polish_iters, flags=0, L0=j.L0, tmin=j.tmin, tmax=j.tmax, sigma_xy=j.sigma_xy,
+                 polish_iters=j.polish_iters, flags=(N.JOB_AUTOTUNE if j.autotune else 0) | (j.cluster << 8) | (j.cell_index << 16), L0=j.L0, tmin=j.tmin, tmax=j.tmax, sigma_xy=j.sigma_xy,
                  sigma_a=j.sigma_a, shrink=j.shrink, seed=j.seed & 0xFFFFFFFFFFFFFFFF,
                  xya=j.xya.ctypes.data_as(C.POINTER(C.c_double)))
 
@@ -74,8 +77,26 @@ def anneal_batch(jobs: list[AnnealJob], *, ctx: N.Context | None = None, slice_s
             shrinks=int(r.shrinks), improvements=int(r.improvements), sweeps=int(r.sweeps_done),
             chains=int(r.replicas), proposals=int(r.proposals), accepted=int(r.accepted),
             exchange_attempts=int(r.exchange_attempts), exchange_accepts=int(r.exchange_accepts),
-            device_ms=float(r.device_ms), q=q.tolist() if ok else None, rows=rows))
+            device_ms=float(r.device_ms), q=q.tolist() if ok else None, rows=rows,
+            launch=dict(cluster_ctas=int(r.cluster_ctas), replicas_per_cta=int(r.replicas_per_cta),
+                        exchange_every=int(r.exchange_every), cell_side=float(r.cell_side),
+                        overflows=int(r.overflows))))
     return out
+
+
+def autotune(job: AnnealJob, *, ctx: N.Context | None = None, latency: bool = False) -> dict:
+    """The autotuner's launch shape for a job's class (sqs_autotune)."""
+    own = ctx is None
+    ctx = ctx or N.Context(0)
+    try:
+        t = N.Tuning()
+        cj = _cjob(job)
+        N.check(N.lib().sqs_autotune(ctx.handle, C.byref(cj), N.TUNE_LATENCY if latency else 0, C.byref(t)))
+    finally:
+        if own:
+            ctx.close()
+    return dict(cluster_ctas=t.cluster_ctas, replicas_per_cta=t.replicas_per_cta, exchange_every=t.exchange_every,
+                trials=t.trials, cell_side=t.cell_side, us_per_sweep=t.us_per_sweep)
 
 
 def jittered_grid(n: int, jitter: float = 0.05, angle_hi: float = 0.1, seed: int = 42):
