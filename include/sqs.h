@@ -203,6 +203,32 @@ typedef struct sqs_job_result {
 int sqs_anneal_batch(sqs_ctx* ctx, const sqs_job* jobs, int njobs, int slice_sweeps, double* const* xya_out,
                      sqs_job_result* out);
 
+/* FP64 gradient polish of `count` packings, one CTA each, all pairs.
+ * Packing k has n_of[k] rows (1..1000) of (x, y, angle) in xya, packings
+ * back to back; the polished packings go to xya_out (same layout; may equal
+ * xya), translated so the bounding box of the certifying dilation starts at
+ * the origin.  The incumbent is the input's FP64 dilation-certified side
+ * (seeded.cu:175-226: every close pair separated once the centres are
+ * scaled by lambda <= 1.008); an input too overlapped for that first has
+ * its centres spread by lambda (at most 1.5x) and descends its overlap
+ * energy at its bounding-box side scaled alike.  Each attempt
+ * compresses the incumbent by 1 - delta, descends the squared-penetration
+ * energy (pair_cached_smooth, seeded.cu:67-90) with a backtracking line
+ * search, and keeps the result when its certified side is smaller; delta
+ * shrinks after a failed attempt; `iters` bounds the gradient steps.
+ * Replaces the reference's polish (cuda/polish.py:67-107, SLSQP on the
+ * CPU for n <= 50) and its device polish of every chain (seeded.cu:621-713).
+ * The side is the FP64 dilation bound; the interval certifier's verdict is
+ * sqs_certify_batch's (polish.certify_q applies the dilation ladder). */
+typedef struct sqs_polish_result {
+    double L_in;             /* certified side of the input (1e30: none)       */
+    double L_out;            /* the same after the polish (1e30: none)         */
+    int32_t iterations;      /* gradient steps used                            */
+    int32_t improved;        /* L_out < L_in                                   */
+} sqs_polish_result;
+int sqs_polish_batch(sqs_ctx* ctx, int count, const int32_t* n_of, const double* xya, int iters, double* xya_out,
+                     sqs_polish_result* out);
+
 /* Autotuner of the batched annealer's launch: times the job's own state on
  * every launch shape that fits (cluster size x replicas per CTA) and cell
  * sides 1.59 .. 2.2, with the job copied to fill one wave of the GPU

@@ -565,3 +565,45 @@ extern "C" int sqs_autotune(sqs_ctx* ctx, const sqs_job* job, int mode, sqs_tuni
     SQS_REQUIRE((mode & ~SQS_TUNE_LATENCY) == 0, "unknown tuning mode %d", mode);
     return autotune(ctx, *job, mode, *out);
 }
+
+extern "C" int sqs_polish_batch(sqs_ctx* ctx, int count, const int32_t* n_of, const double* xya, int iters,
+                                double* xya_out, sqs_polish_result* out) {
+    if (int r = enter(ctx)) return r;
+    SQS_REQUIRE(count >= 0, "count %d < 0", count);
+    if (count == 0) return SQS_OK;
+    SQS_REQUIRE(n_of && xya && xya_out && out, "null host pointer");
+    SQS_REQUIRE(iters >= 0 && iters <= 1000000, "iters %d out of 0..1000000", iters);
+    std::vector<int64_t> row0((size_t)count + 1, 0);
+    int nmax = 1;
+    for (int k = 0; k < count; ++k) {
+        SQS_REQUIRE(n_of[k] >= 1 && n_of[k] <= kMaxN, "packing %d: n=%d out of 1..%d", k, n_of[k], kMaxN);
+        row0[(size_t)k + 1] = row0[(size_t)k] + n_of[k];
+        nmax = std::max(nmax, n_of[k]);
+    }
+    const int64_t rows = row0[(size_t)count];
+    for (int64_t i = 0; i < 3 * rows; ++i) SQS_REQUIRE(std::isfinite(xya[i]), "non-finite coordinate at %lld", (long long)i);
+    size_t tot = 0;
+    auto seg = [&](size_t b) { size_t o = tot; tot += (b + 255) & ~(size_t)255; return o; };
+    const size_t o_n = seg(sizeof(int32_t) * count), o_r = seg(sizeof(int64_t) * count);
+    const size_t o_x = seg(sizeof(double) * 3 * (size_t)rows), o_res = seg(sizeof(double) * 3 * count);
+    if (int r = ctx->d_polish.reserve(tot)) return r;
+    char* D = (char*)ctx->d_polish.p;
+    SQS_CUDA(cudaMemcpyAsync(D + o_n, n_of, sizeof(int32_t) * count, cudaMemcpyHostToDevice, ctx->stream));
+    SQS_CUDA(cudaMemcpyAsync(D + o_r, row0.data(), sizeof(int64_t) * count, cudaMemcpyHostToDevice, ctx->stream));
+    SQS_CUDA(cudaMemcpyAsync(D + o_x, xya, sizeof(double) * 3 * (size_t)rows, cudaMemcpyHostToDevice, ctx->stream));
+    if (int r = launch_polish_states(ctx->stream, count, (const int32_t*)(D + o_n), (const int64_t*)(D + o_r), iters,
+                                     (double*)(D + o_x), (double*)(D + o_res), polish_smem_bytes(nmax)))
+        return r;
+    ctx->launches += 1;
+    std::vector<double> res(3 * (size_t)count);
+    SQS_CUDA(cudaMemcpyAsync(xya_out, D + o_x, sizeof(double) * 3 * (size_t)rows, cudaMemcpyDeviceToHost, ctx->stream));
+    SQS_CUDA(cudaMemcpyAsync(res.data(), D + o_res, sizeof(double) * res.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    SQS_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (int k = 0; k < count; ++k) {
+        out[k].L_in = res[3 * (size_t)k];
+        out[k].L_out = res[3 * (size_t)k + 1];
+        out[k].iterations = (int32_t)res[3 * (size_t)k + 2];
+        out[k].improved = out[k].L_out < out[k].L_in;
+    }
+    return SQS_OK;
+}

@@ -29,6 +29,8 @@ int launch_anneal(cudaStream_t stream, int njobs, int cs, int Rl, size_t smem, c
 int launch_polish(cudaStream_t stream, int njobs, const int32_t* job_list, const JobDev* jdev, JobMut* jmut,
                   double* best, size_t smem);
 size_t polish_smem_bytes(int n);
+int launch_polish_states(cudaStream_t stream, int count, const int32_t* n_of, const int64_t* row0, int iters,
+                         double* xya, double* res, size_t smem);
 
 void put(char* dst, size_t cap, const std::string& s);
 // Validate one job and fill its device records (offsets left to the caller).

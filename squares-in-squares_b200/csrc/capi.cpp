@@ -115,6 +115,7 @@ int sqs_ctx_destroy(sqs_ctx* ctx) {
     ctx->d_anneal.release();
     ctx->d_cert.release();
     ctx->d_tune.release();
+    ctx->d_polish.release();
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SQS_OK;

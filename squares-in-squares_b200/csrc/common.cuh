@@ -67,6 +67,7 @@ struct sqs_ctx {
     sqs::DevBuf d_in, d_side, d_out, d_grad, d_cand, d_misc, d_anneal;
     sqs::DevBuf d_cert;  // the certifier's per-square interval cache
     sqs::DevBuf d_tune;  // the annealer autotuner's trial state
+    sqs::DevBuf d_polish;  // standalone polish batches
 };
 
 namespace sqs {

@@ -169,6 +169,81 @@ __device__ void trig_of(int n, const double3* q, double2* cs) {
     __syncthreads();
 }
 
+// Shared-memory views of one polish CTA.
+struct PolishBufs {
+    double3* q0;  // accepted state of the descent
+    double3* q;   // trial state
+    double3* g;   // gradient at q0
+    double3* sv;  // best so far (translated, dilated)
+    double2* cs;  // cos/sin of the state being evaluated
+};
+
+__device__ __forceinline__ PolishBufs polish_bufs(unsigned char* dyn, int n) {
+    PolishBufs b;
+    b.q0 = reinterpret_cast<double3*>(dyn);
+    b.q = b.q0 + n;
+    b.g = b.q + n;
+    b.sv = b.g + n;
+    b.cs = reinterpret_cast<double2*>(b.sv + n);
+    return b;
+}
+
+// Descend the energy of state q0 at side Lt until it vanishes (at most
+// *budget gradient steps, each with up to 8 backtracking trials).
+__device__ void descend(int n, const PolishBufs& B, double Lt, int* budget, double* red) {
+    trig_of(n, B.q0, B.cs);
+    double E = energy(n, B.q0, B.cs, Lt, B.g, red);
+    double alpha = 0.05;
+    while (*budget > 0 && E > 1e-26) {
+        --*budget;
+        bool moved = false;
+        for (int ls = 0; ls < 8 && !moved; ++ls) {
+            for (int i = threadIdx.x; i < n; i += kPT) {
+                const double3 p = B.q0[i], d = B.g[i];
+                B.q[i] = make_double3(p.x - alpha * d.x, p.y - alpha * d.y, wrap_q(p.z - alpha * d.z));
+            }
+            __syncthreads();
+            trig_of(n, B.q, B.cs);
+            const double En = energy(n, B.q, B.cs, Lt, nullptr, red);
+            if (En < E) {
+                E = En;
+                moved = true;
+                alpha = fmin(alpha * 1.5, 0.5);
+                for (int i = threadIdx.x; i < n; i += kPT) B.q0[i] = B.q[i];
+                __syncthreads();
+            } else {
+                alpha *= 0.3;
+            }
+        }
+        if (!moved) break;
+        E = energy(n, B.q0, B.cs, Lt, B.g, red);  // cs holds the trig of q == q0
+    }
+    trig_of(n, B.q0, B.cs);
+}
+
+// Compress-and-descend attempts on the certified state sv of side *Lb
+// (delta shrinking by 0.3 after every attempt that does not certify a
+// smaller side); sv and *Lb are updated in place.
+__device__ void polish_loop(int n, const PolishBufs& B, double* Lb, int* budget, double* red) {
+    double delta = 1e-4;
+    for (int attempt = 0; attempt < 12 && *budget > 0 && delta > 1e-9; ++attempt) {
+        const double f = 1.0 - delta, Lt = *Lb * f;
+        for (int i = threadIdx.x; i < n; i += kPT) B.q0[i] = make_double3(B.sv[i].x * f, B.sv[i].y * f, B.sv[i].z);
+        __syncthreads();
+        descend(n, B, Lt, budget, red);
+        double lam = 0, x0 = 0, y0 = 0;
+        const double Lc = cert_side_all(n, B.q0, B.cs, red, lam, x0, y0);
+        if (Lc < *Lb) {
+            *Lb = Lc;
+            for (int i = threadIdx.x; i < n; i += kPT)
+                B.sv[i] = make_double3(B.q0[i].x * lam - x0, B.q0[i].y * lam - y0, B.q0[i].z);
+            __syncthreads();
+        } else {
+            delta *= 0.3;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kPT) polish_kernel(const int32_t* __restrict__ job_list,
                                                      const JobDev* __restrict__ jdev, JobMut* __restrict__ jmut,
                                                      double* __restrict__ best) {
@@ -179,65 +254,96 @@ __global__ void __launch_bounds__(kPT) polish_kernel(const int32_t* __restrict__
     const int n = jd.n;
     double Lb = jmut[job].best_L;
     if (jd.polish_iters <= 0 || Lb >= 1e29 || jmut[job].status < 0) return;
-    double3* q0 = reinterpret_cast<double3*>(dyn);  // accepted state of the descent
-    double3* q = q0 + n;                            // trial state
-    double3* g = q + n;                             // gradient at q0
-    double3* sv = g + n;                            // best so far (translated, dilated)
-    double2* cs = reinterpret_cast<double2*>(sv + n);  // cos/sin of the state being evaluated
+    const PolishBufs B = polish_bufs(dyn, n);
     double* b = best + jd.best_off;
-    for (int i = threadIdx.x; i < n; i += kPT) sv[i] = make_double3(b[3 * i], b[3 * i + 1], b[3 * i + 2]);
+    for (int i = threadIdx.x; i < n; i += kPT) B.sv[i] = make_double3(b[3 * i], b[3 * i + 1], b[3 * i + 2]);
     __syncthreads();
-    double delta = 1e-4;
     int budget = jd.polish_iters;
-    for (int attempt = 0; attempt < 12 && budget > 0 && delta > 1e-9; ++attempt) {
-        const double f = 1.0 - delta, Lt = Lb * f;
-        for (int i = threadIdx.x; i < n; i += kPT) q0[i] = make_double3(sv[i].x * f, sv[i].y * f, sv[i].z);
-        __syncthreads();
-        trig_of(n, q0, cs);
-        double E = energy(n, q0, cs, Lt, g, red);
-        double alpha = 0.05;
-        while (budget > 0 && E > 1e-26) {
-            --budget;
-            bool moved = false;
-            for (int ls = 0; ls < 8 && !moved; ++ls) {
-                for (int i = threadIdx.x; i < n; i += kPT) {
-                    const double3 p = q0[i], d = g[i];
-                    q[i] = make_double3(p.x - alpha * d.x, p.y - alpha * d.y, wrap_q(p.z - alpha * d.z));
-                }
-                __syncthreads();
-                trig_of(n, q, cs);
-                const double En = energy(n, q, cs, Lt, nullptr, red);
-                if (En < E) {
-                    E = En;
-                    moved = true;
-                    alpha = fmin(alpha * 1.5, 0.5);
-                    for (int i = threadIdx.x; i < n; i += kPT) q0[i] = q[i];
-                    __syncthreads();
-                } else {
-                    alpha *= 0.3;
-                }
-            }
-            if (!moved) break;
-            E = energy(n, q0, cs, Lt, g, red);  // cs holds the trig of q == q0
-        }
-        trig_of(n, q0, cs);
-        double lam = 0, x0 = 0, y0 = 0;
-        const double Lc = cert_side_all(n, q0, cs, red, lam, x0, y0);
-        if (Lc < Lb) {
-            Lb = Lc;
-            for (int i = threadIdx.x; i < n; i += kPT)
-                sv[i] = make_double3(q0[i].x * lam - x0, q0[i].y * lam - y0, q0[i].z);
-            __syncthreads();
-        } else {
-            delta *= 0.3;
-        }
-    }
+    polish_loop(n, B, &Lb, &budget, red);
     for (int i = threadIdx.x; i < n; i += kPT) {
-        b[3 * i] = sv[i].x;
-        b[3 * i + 1] = sv[i].y;
-        b[3 * i + 2] = sv[i].z;
+        b[3 * i] = B.sv[i].x;
+        b[3 * i + 1] = B.sv[i].y;
+        b[3 * i + 2] = B.sv[i].z;
     }
     if (threadIdx.x == 0) jmut[job].best_L = Lb;
+}
+
+// Standalone polish of arbitrary states (state k: n_of[k] rows at
+// xya + 3 * row0[k], polished in place).  The input's dilation-certified
+// side is the incumbent; an input too overlapped to certify (dilation above
+// 1.008) first has its centres spread by that dilation (at most 1.5x) and
+// descends the energy at its bounding-box side scaled alike.
+// res[k] = {L_in, L_out, iterations used}.
+__global__ void __launch_bounds__(kPT) polish_states_kernel(const int32_t* __restrict__ n_of,
+                                                            const int64_t* __restrict__ row0, int iters,
+                                                            double* __restrict__ xya, double* __restrict__ res) {
+    extern __shared__ __align__(16) unsigned char dyn[];
+    __shared__ double red[kPT / 32];
+    const int k = blockIdx.x;
+    const int n = n_of[k];
+    double* st = xya + 3 * row0[k];
+    const PolishBufs B = polish_bufs(dyn, n);
+    for (int i = threadIdx.x; i < n; i += kPT) B.q0[i] = make_double3(st[3 * i], st[3 * i + 1], wrap_q(st[3 * i + 2]));
+    __syncthreads();
+    trig_of(n, B.q0, B.cs);
+    int budget = iters;
+    double lam = 0, x0 = 0, y0 = 0;
+    double Lb = cert_side_all(n, B.q0, B.cs, red, lam, x0, y0);
+    const double L_in = Lb;
+    if (Lb >= 1e29) {
+        // bounding box of the input, translated to the origin, as the side
+        double a0 = 1e300, a1 = -1e300, b0 = 1e300, b1 = -1e300;
+        for (int i = threadIdx.x; i < n; i += kPT) {
+            const double r = 0.5 * (fabs(B.cs[i].x) + fabs(B.cs[i].y));
+            a0 = fmin(a0, B.q0[i].x - r);
+            a1 = fmax(a1, B.q0[i].x + r);
+            b0 = fmin(b0, B.q0[i].y - r);
+            b1 = fmax(b1, B.q0[i].y + r);
+        }
+        a0 = -block_max(-a0, red);
+        a1 = block_max(a1, red);
+        b0 = -block_max(-b0, red);
+        b1 = block_max(b1, red);
+        // spread the centres by the dilation that would separate the close
+        // pairs (at most 1.5x) so the descent has room to remove the overlaps
+        const double f = fmin(fmax(lam, 1.0), 1.5);
+        for (int i = threadIdx.x; i < n; i += kPT)
+            B.q0[i] = make_double3((B.q0[i].x - a0) * f, (B.q0[i].y - b0) * f, B.q0[i].z);
+        __syncthreads();
+        descend(n, B, fmax(a1 - a0, b1 - b0) * f, &budget, red);
+        Lb = cert_side_all(n, B.q0, B.cs, red, lam, x0, y0);
+    }
+    if (Lb < 1e29) {
+        for (int i = threadIdx.x; i < n; i += kPT)
+            B.sv[i] = make_double3(B.q0[i].x * lam - x0, B.q0[i].y * lam - y0, B.q0[i].z);
+        __syncthreads();
+        polish_loop(n, B, &Lb, &budget, red);
+        for (int i = threadIdx.x; i < n; i += kPT) {
+            st[3 * i] = B.sv[i].x;
+            st[3 * i + 1] = B.sv[i].y;
+            st[3 * i + 2] = B.sv[i].z;
+        }
+    }
+    if (threadIdx.x == 0) {
+        res[3 * k] = L_in;
+        res[3 * k + 1] = Lb;
+        res[3 * k + 2] = (double)(iters - budget);
+    }
+}
+
+int launch_polish_states(cudaStream_t stream, int count, const int32_t* n_of, const int64_t* row0, int iters,
+                         double* xya, double* res, size_t smem) {
+    static bool attr_done[64] = {false};
+    int dev = 0;
+    SQS_CUDA(cudaGetDevice(&dev));
+    if (!attr_done[dev & 63]) {
+        SQS_CUDA(cudaFuncSetAttribute(polish_states_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        attr_done[dev & 63] = true;
+    }
+    if (count <= 0) return SQS_OK;
+    polish_states_kernel<<<count, kPT, smem, stream>>>(n_of, row0, iters, xya, res);
+    SQS_CUDA(cudaGetLastError());
+    return SQS_OK;
 }
 
 int launch_polish(cudaStream_t stream, int njobs, const int32_t* job_list, const JobDev* jdev, JobMut* jmut,

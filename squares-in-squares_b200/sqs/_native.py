@@ -62,6 +62,11 @@ class Tuning(C.Structure):
                 ("trials", C.c_int32), ("cell_side", C.c_double), ("us_per_sweep", C.c_double)]
 
 
+class PolishResult(C.Structure):
+    """sqs_polish_result (include/sqs.h)."""
+    _fields_ = [("L_in", C.c_double), ("L_out", C.c_double), ("iterations", C.c_int32), ("improved", C.c_int32)]
+
+
 JOB_AUTOTUNE = 1
 TUNE_LATENCY = 1
 
@@ -100,6 +105,8 @@ SIGNATURES: dict[str, tuple] = {
     "sqs_server_step": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "sqs_server_poll": (C.c_int, [_vp, C.c_int64, C.POINTER(JobResult), C.POINTER(C.c_double)]),
     "sqs_server_cancel": (C.c_int, [_vp, C.c_int64]),
+    "sqs_polish_batch": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_double), C.c_int,
+                                   C.POINTER(C.c_double), C.POINTER(PolishResult)]),
     "sqs_autotune": (C.c_int, [_vp, C.POINTER(Job), C.c_int, C.POINTER(Tuning)]),
     "sqs_server_info": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_size_t)]),
 }

@@ -13,6 +13,12 @@ Outputs (committed):
   sat_pairs.json      random unit-square pairs with the reference's FP64
                       pair() energy and gradient (seeded.cu:92) and boundary()
                       (seeded.cu:96) values, computed by oracle/_ref.
+  candidates.json     the reference's saved search outputs (cuda/results/
+                      raw{5,10,11,17,50}.json: n and the raw state q) and the
+                      test inputs of tests/test_cuda_demo.py, with the result
+                      of its certified_candidate (demo.py:25-40) and certify_q
+                      (polish.py:52-65): the 50-decimal side and the dilation,
+                      or the ValueError message.
 """
 from __future__ import annotations
 
@@ -35,6 +41,7 @@ from squares.core import evaluate, grid, kaggle_roundtrip, prepare_kaggle  # noq
 from squares.optimizer import tilted_five  # noqa: E402
 from scheduler import goebel, strip_construction  # noqa: E402
 import demo  # noqa: E402
+import polish as ref_polish  # noqa: E402
 import oracle as O  # noqa: E402
 
 
@@ -131,7 +138,29 @@ def main():
         b = ref.ref_boundary(pp.ctypes.data_as(dp), 1.3, gb.ctypes.data_as(dp))
         recs.append(dict(p=p.tolist(), q=q.tolist(), e=e, g=g.tolist(), wall_L=1.3, wall=b, wall_g=gb.tolist()))
     (HERE / "sat_pairs.json").write_text(json.dumps(recs) + "\n")
-    print(f"{len(kept)} certifier cases, {len(recs)} SAT pairs")
+
+    cands = []
+    for n in (5, 10, 11, 17, 50):
+        raw = json.loads((REF / "cuda" / "results" / f"raw{n}.json").read_text())
+        cands.append(dict(name=f"raw{n}", n=n, q=raw["q"]))
+    cands += [dict(name="separated_pair", n=2, q=[[.5, .5, 0], [1.5, .5, 0]]),
+              dict(name="empty", n=2, q=[]),
+              dict(name="coincident", n=2, q=[[.5, .5, 0], [.5, .5, 0]]),
+              dict(name="nan", n=2, q=[[float("nan"), 0, 0], [1, 0, 0]])]
+    for c in cands:
+        raw = dict(n=c["n"], q=c["q"])
+        try:
+            rows, side, dil = demo.certified_candidate(raw)
+            c["candidate"] = dict(L=str(demo.certify(c["n"], rows)), side=side, dilation=dil)
+        except ValueError as e:
+            c["candidate"] = dict(error=str(e))
+        try:
+            rows, side, dil = ref_polish.certify_q(c["q"])
+            c["certify_q"] = dict(L=str(demo.certify(c["n"], rows)), side=side, dilation=dil)
+        except ValueError as e:
+            c["certify_q"] = dict(error=str(e))
+    (HERE / "candidates.json").write_text(json.dumps(cands, indent=1).replace("NaN", "\"nan\"") + "\n")
+    print(f"{len(kept)} certifier cases, {len(recs)} SAT pairs, {len(cands)} candidates")
 
 
 if __name__ == "__main__":

@@ -106,3 +106,23 @@ def test_roundtrip_matches_reference(oracle):
     for v in list(rng.uniform(-100, 100, 200)) + [0.1, 1.0, 3.0, 1e-20, 123456789.0]:
         for s in (repr(float(v)), f"{v:.25f}", f"{v:.3e}"):
             assert oracle.roundtrip(s) == oracle.roundtrip(s, "ref")
+
+
+def _ladder_rows(q, dilation):
+    return [dict(square_id=str(i), x=format(float(x) * dilation, ".17g"), y=format(float(y) * dilation, ".17g"),
+                 angle=format(float(a), ".17g")) for i, (x, y, a) in enumerate(q)]
+
+
+def test_candidate_ladders_match_golden(oracle):
+    """certified_candidate / certify_q results of the reference (its saved
+    search outputs and demo-test inputs) reproduced by the oracle certifier
+    on the same dilated rows."""
+    cands = json.loads((GOLDEN / "candidates.json").read_text())
+    assert len(cands) == 9
+    for c in cands:
+        for key in ("candidate", "certify_q"):
+            want = c[key]
+            if "error" in want:
+                continue
+            ok, L, reason, _ = oracle.certify(c["n"], _ladder_rows(c["q"], want["dilation"]))
+            assert ok and L == want["L"], (c["name"], key, reason)
