@@ -3,7 +3,8 @@
     python squares-in-squares_b200/build.py [--force] [--verbose]
 
 Objects go to squares-in-squares_b200/_build/, the library to
-squares-in-squares_b200/sqs/libsqs.so, ptxas resource usage (registers,
+squares-in-squares_b200/sqs/libsqs.so, the drop-in executables (packing,
+seeded, certifier) to squares-in-squares_b200/bin/, ptxas resource usage (registers,
 spills, shared memory) to _build/ptxas.log.  Only sources whose mtime (or
 that of any header) changed are recompiled.
 """
@@ -21,6 +22,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "sqs" / "libsqs.so"
+BIN = PKG / "bin"
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
                "--expt-relaxed-constexpr", "-I", str(ROOT / "include")]
@@ -74,7 +76,34 @@ def build(force: bool = False, verbose: bool = False) -> Path:
             raise RuntimeError("link of libsqs.so failed")
     log = "".join(p.read_text() for p in sorted(BUILD.glob("*.ptxas.log")))
     (BUILD / "ptxas.log").write_text(log)
+    build_cli(force, verbose)
     return LIB
+
+
+# Drop-in executables of the reference's search and certifier programs, on
+# top of libsqs.so (found next to them through the run path).
+CLI = {
+    "packing": ("search.cpp", []),
+    "seeded": ("search.cpp", ["-DSQS_FLAVOR_SEEDED"]),
+    "certifier": ("certifier.cpp", []),
+}
+
+
+def build_cli(force: bool = False, verbose: bool = False) -> None:
+    BIN.mkdir(exist_ok=True)
+    for name, (src, defs) in CLI.items():
+        exe, s = BIN / name, PKG / "cli" / src
+        newest = max(s.stat().st_mtime, LIB.stat().st_mtime, (ROOT / "include" / "sqs.h").stat().st_mtime)
+        if not force and exe.exists() and exe.stat().st_mtime >= newest:
+            continue
+        cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", *defs, "-I", str(ROOT / "include"), str(s),
+               "-o", str(exe), "-L", str(LIB.parent), "-lsqs", "-Wl,-rpath,$ORIGIN/../sqs"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError(f"build of {name} failed")
 
 
 def main():

@@ -1,0 +1,218 @@
+// Drop-in for the reference's search programs, on the batched GPU annealer:
+//
+//   packing seed.txt epochs steps chains random_seed output.json   (packing.cu:768-868)
+//   seeded  seed.txt epochs steps chains seed output.json          (seeded.cu:831-983)
+//
+// Same argument checks (epochs 0..100000, steps 0..4096, chains 0..4096 and
+// a multiple of 8; 0 = automatic), same seed-file format ("n L" then n lines
+// "x y angle", n <= 1000, 0 < L <= 64), same validated environment variables
+// (an out-of-range value prints "invalid NAME" and exits 2), exit code 2 on
+// any error, and the same single-line JSON report with the best state in
+// "q".  Callers that run these programs (cuda/batch.py, scheduler.run_gpu,
+// cpp_loop.case, full_run, demo.main) and read their JSON
+// (demo.certified_candidate, seeded.certify_raw, batch.merge,
+// autotune.summarize) work unchanged.
+//
+// Mapping onto sqs_anneal_batch:
+//   * every ladder of 8 chains is one job of 8 replicas (temperature rungs);
+//     the chains/8 jobs run side by side in one batched call, each with its
+//     own seed, and the report takes the job with the smallest certified side;
+//   * a reference step is one proposal per chain, so a job runs
+//     ceil(epochs * steps / n) sweeps of n proposals per replica, and
+//     exchanges replicas once per epoch's worth of sweeps;
+//   * the absolute shrink step becomes a relative one (shrink / L);
+//   * chains = 0 (or *_AUTOTUNE=1 with chains >= 64) takes one ladder per SM,
+//     capped at *_MAX_CHAINS, as the reference sizes chains to a wave;
+//     *_AUTOTUNE=1 also lets the launch autotuner pick each job's shape;
+//   * temperatures: packing uses PACK_TMIN..PACK_TMAX; seeded uses the
+//     reference's fixed 1e-11..SEED_TMAX ladder;
+//   * SEED_POLISH is the job's polish budget (packing polishes 200 steps);
+//   * the angle proposal width is 2.5 x the move width (PACK_ROTATION,
+//     SEED_COLLECTIVE and SEED_STRUCTURED are validated and reported, like
+//     PACK_ROTATION in the reference, but do not change the search).
+// "target_L" is the FP64 dilation-certified side of the best state and "q"
+// that state (the packing the interval certifier accepted); when no ladder
+// finds a certified state the seed is reported with its side, as the
+// reference does.
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <string>
+#include <vector>
+
+#include "sqs.h"
+
+#if defined(SQS_FLAVOR_SEEDED)
+static const char* kName = "seeded";
+static const char* kPrefix = "SEED_";
+#else
+static const char* kName = "packing";
+static const char* kPrefix = "PACK_";
+#endif
+
+// packing parses its variables as float (packing.cu:153-156), seeded as
+// double (seeded.cu:819-829); both reject trailing text and out-of-range
+// values with "invalid NAME" and exit code 2.
+static double env(const char* suffix, double def, double lo, double hi) {
+    const std::string name = std::string(kPrefix) + suffix;
+    const char* s = std::getenv(name.c_str());
+    if (!s) return def;
+    char* end = nullptr;
+#if defined(SQS_FLAVOR_SEEDED)
+    const double v = std::strtod(s, &end);
+#else
+    const float vf = std::strtof(s, &end);
+    const double v = vf;
+    lo = (float)lo;
+    hi = (float)hi;
+#endif
+    if (*end || !std::isfinite(v) || v < lo || v > hi) {
+        std::cerr << "invalid " << name << "\n";
+        std::exit(2);
+    }
+    return v;
+}
+
+static int fail(const char* what) {
+    std::cerr << kName << ": " << what << ": " << sqs_last_error() << "\n";
+    return 2;
+}
+
+int main(int argc, char** argv) {
+    if (argc != 7) {
+        std::cerr << kName << " seed.txt epochs steps chains " << (std::strcmp(kName, "packing") ? "seed" : "random_seed")
+                  << " output.json\n";
+        return 2;
+    }
+    int epochs = std::atoi(argv[2]), steps = std::atoi(argv[3]), chains = std::atoi(argv[4]), n = 0;
+    if (epochs < 0 || epochs > 100000 || steps < 0 || steps > 4096 || chains < 0 || chains > 4096 ||
+        (chains > 0 && chains % 8))
+        return 2;
+    double L = 0;
+    std::ifstream in(argv[1]);
+    in >> n >> L;
+    if (!in || n < 1 || n > 1000 || !std::isfinite(L) || L <= 0 || L > 64) return 2;
+    std::vector<double> seed(3 * (size_t)n);
+    for (int i = 0; i < n; ++i) {
+        in >> seed[3 * i] >> seed[3 * i + 1] >> seed[3 * i + 2];
+        if (!in || !std::isfinite(seed[3 * i]) || !std::isfinite(seed[3 * i + 1]) || !std::isfinite(seed[3 * i + 2]))
+            return 2;
+    }
+#if defined(SQS_FLAVOR_SEEDED)
+    const double shrink = env("SHRINK", .001, 1e-7, .1);
+    const double tmax = env("TMAX", .0001, 1e-11, .1);
+    const double tmin = std::min(1e-11, tmax);
+    const double mv = env("MOVE", .02, 1e-6, .3);
+    const int collective = (int)env("COLLECTIVE", 1, 0, 1);
+    const int polish = (int)env("POLISH", 200, 0, 4096);
+    const int structured = (int)env("STRUCTURED", 1, 0, 1);
+    const int autotune = (int)env("AUTOTUNE", 1, 0, 1);
+    const int max_chains = (int)env("MAX_CHAINS", 768, 8, 4096);
+#else
+    const double tmin = env("TMIN", 1e-11, 1e-12, 1.0);
+    const double tmax = env("TMAX", 1e-4, 1e-12, 1.0);
+    const double mv = env("MOVE", .02, .000001, .3);
+    (void)env("ROTATION", .12, .000001, 1.57);
+    if (tmax < tmin) return 2;
+    const double shrink = env("SHRINK", .001, .000001, .1);
+    const int autotune = (int)env("AUTOTUNE", 1, 0, 1);
+    const int max_chains = (int)env("MAX_CHAINS", 768, 8, 4096);
+    const int polish = 200;
+#endif
+    const unsigned long long rng_seed = std::strtoull(argv[5], nullptr, 10);
+
+    sqs_ctx* ctx = nullptr;
+    if (sqs_ctx_create(0, &ctx) != SQS_OK) return fail("device");
+    char dev[256] = {0};
+    int sms = 0;
+    if (sqs_ctx_device_info(ctx, dev, (int)sizeof dev, &sms) != SQS_OK) return fail("device info");
+    const int wave_chains = std::max(8, (sms * 8 / 8) * 8);
+    if (chains == 0 || (autotune && chains >= 64)) {
+        const int target = chains == 0 ? wave_chains : std::max(chains, std::min(wave_chains, max_chains));
+        chains = ((std::min(target, max_chains) + 7) / 8) * 8;
+    }
+    if (epochs == 0) epochs = n <= 64 ? 50 : (n <= 256 ? 40 : 30);
+    if (steps == 0) steps = n <= 64 ? 64 : (n <= 256 ? 48 : 32);
+#if !defined(SQS_FLAVOR_SEEDED)
+    epochs = epochs > 120 ? std::min(epochs, 80) : epochs;  // packing.cu:805
+#endif
+    const long long proposals_per_chain = (long long)epochs * steps;
+    const int sweeps = (int)std::max<long long>(1, (proposals_per_chain + n - 1) / n);
+    const int per_epoch = std::max(1, (int)std::lround((double)steps / (double)n));
+    const int ladders = chains / 8;
+
+    std::vector<sqs_job> jobs((size_t)ladders);
+    std::vector<std::vector<double>> outs((size_t)ladders, std::vector<double>(3 * (size_t)n));
+    std::vector<double*> ptrs((size_t)ladders);
+    for (int k = 0; k < ladders; ++k) {
+        sqs_job& j = jobs[(size_t)k];
+        std::memset(&j, 0, sizeof j);
+        j.n = n;
+        j.replicas = 8;
+        j.sweeps = sweeps;
+        j.exchange_every = per_epoch;
+        j.polish_iters = polish;
+        j.flags = autotune ? SQS_JOB_AUTOTUNE : 0;
+        j.L0 = L;
+        j.tmin = tmin;
+        j.tmax = tmax;
+        j.sigma_xy = mv;
+        j.sigma_a = std::min(1.0, 2.5 * mv);
+        j.shrink = std::min(0.1, shrink / L);
+        j.seed = rng_seed + 0x9E3779B97F4A7C15ull * (unsigned long long)k;
+        j.xya = seed.data();
+        ptrs[(size_t)k] = outs[(size_t)k].data();
+    }
+    std::vector<sqs_job_result> res((size_t)ladders);
+    const auto t0 = std::chrono::steady_clock::now();
+    if (sqs_anneal_batch(ctx, jobs.data(), ladders, 0, ptrs.data(), res.data()) != SQS_OK) return fail("anneal");
+    const double seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+
+    double bestL = L;
+    const double* best = seed.data();
+    long long proposals = 0, accepted = 0, xatt = 0, xacc = 0;
+    int shrinks = 0, feasible = 0;
+    for (int k = 0; k < ladders; ++k) {
+        const sqs_job_result& r = res[(size_t)k];
+        proposals += r.proposals;
+        accepted += r.accepted;
+        xatt += r.exchange_attempts;
+        xacc += r.exchange_accepts;
+        shrinks += r.shrinks;
+        feasible += r.improvements;
+        if (r.certified && r.L_polished < bestL) {
+            bestL = r.L_polished;
+            best = outs[(size_t)k].data();
+        }
+    }
+    sqs_ctx_destroy(ctx);
+
+    std::ofstream out(argv[6]);
+    if (!out) return 2;
+    out << std::setprecision(17);
+#if defined(SQS_FLAVOR_SEEDED)
+    out << "{\"n\":" << n << ",\"target_L\":" << bestL << ",\"seconds\":" << seconds << ",\"shrinks\":" << shrinks
+        << ",\"epochs\":" << epochs << ",\"steps\":" << steps << ",\"chains\":" << chains << ",\"device\":\"" << dev
+        << "\"" << ",\"sm_count\":" << sms << ",\"blocks_per_sm\":" << 1 << ",\"wave_chains\":" << wave_chains
+        << ",\"collective\":" << collective << ",\"polish\":" << polish << ",\"structured\":" << structured
+        << ",\"proposals\":" << proposals << ",\"accepted\":" << accepted << ",\"exchange_attempts\":" << xatt
+        << ",\"exchange_accepts\":" << xacc << ",\"q\":[";
+#else
+    out << "{\"n\":" << n << ",\"target_L\":" << bestL << ",\"seconds\":" << seconds
+        << ",\"chain_steps\":" << (long long)chains * epochs * steps << ",\"proposals\":" << proposals
+        << ",\"feasible_checkpoints\":" << std::max(1, feasible) << ",\"shrinks\":" << shrinks
+        << ",\"chains\":" << chains << ",\"sm_count\":" << sms << ",\"blocks_per_sm\":" << 1
+        << ",\"wave_chains\":" << wave_chains << ",\"device\":\"" << dev << "\",\"q\":[";
+#endif
+    for (int i = 0; i < n; ++i) {
+        if (i) out << ",";
+        out << "[" << best[3 * i] << "," << best[3 * i + 1] << "," << best[3 * i + 2] << "]";
+    }
+    out << "]}\n";
+    return out ? 0 : 2;
+}
