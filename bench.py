@@ -207,6 +207,23 @@ def cpu_pairs_per_s(x32, s32, seconds: float, configs_per_step: int | None = Non
     return done_pairs / el, kind, threads, sample, k, el
 
 
+def accuracy(d_e, d_g, x32, s32, configs: int = 64) -> dict:
+    """FP32 energies and gradients of the last launch against the FP64
+    all-pairs energy of the same FP32 inputs (the oracle restatement of
+    seeded.cu:92-162) on the first `configs` configurations."""
+    import numpy as np
+
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    e = d_e.download()[:configs].astype(np.float64)
+    g = d_g.download()[:configs].astype(np.float64)
+    eo, go, _ = O.total_batch(x32[:configs].astype(np.float64), s32[:configs].astype(np.float64))
+    rel = np.abs(e - eo) / np.maximum(np.abs(eo), 1e-30)
+    return dict(configs=configs, max_rel_energy_error=float(rel.max()), mean_rel_energy_error=float(rel.mean()),
+                max_abs_grad_error=float(np.abs(g - go).max()), vs="FP64 all-pairs oracle on the same FP32 inputs")
+
+
 def run_reference(args, D: Dist):
     if D.rank != 0:
         return
@@ -317,6 +334,8 @@ def run_sqs(args, D: Dist):
         pairs_per_step=pairs_per_step,
         clocks=clk,
     )
+    if D.rank == 0:
+        line["accuracy"] = accuracy(d_e, d_g, x32, s32)
     if D.rank == 0 and D.world == 1 and not args.no_cpu_baseline:
         val, kind, cores, sample, _, _ = cpu_pairs_per_s(x32, s32, args.cpu_seconds)
         line["cpu_baseline"] = dict(value=val, unit=UNIT, cores=cores, kind=kind, sample=sample)
@@ -432,10 +451,14 @@ def bench_served_sweep(ctx, rates: str):
 
 
 def bench_batched(ctx, sweeps: int = 50, instances: int = 512):
-    """Batched PT-SA, one launch: 512 instances, n uniform in [20, 400]
-    (seeded), 32 replicas on 1e-4..5e-2, sigma 0.02 / 0.05 rad, exchange every
-    10 sweeps, FP64 recompute of each best; a bounded sweep budget."""
-    import math
+    """Batched PT-SA: 512 instances, n uniform in [20, 400] (seeded), 32
+    replicas on 1e-4..5e-2, sigma 0.02 / 0.05 rad, exchange every 10 sweeps,
+    FP64 recompute of each best; a bounded sweep budget.  Launch shapes and
+    cell sides from the autotuner (tuned once per job class before timing);
+    the default fixed shape and the slice loop replayed as a CUDA graph
+    (slices of one exchange interval) are timed beside the single launch."""
+    from collections import Counter
+    from dataclasses import replace
 
     import numpy as np
 
@@ -447,15 +470,34 @@ def bench_batched(ctx, sweeps: int = 50, instances: int = 512):
         n = int(rng.integers(20, 401))
         xya, L0 = jittered_grid(n, seed=k)
         jobs.append(AnnealJob(xya, L0=L0, replicas=32, sweeps=sweeps, exchange_every=10, tmin=1e-4, tmax=5e-2,
-                              sigma_xy=0.02, sigma_a=0.05, seed=k, polish_iters=0))
-    anneal_batch(jobs[:4], ctx=ctx)  # warm-up
+                              sigma_xy=0.02, sigma_a=0.05, seed=k, polish_iters=0, autotune=True))
     t0 = time.perf_counter()
-    res = anneal_batch(jobs, ctx=ctx)
-    dt = time.perf_counter() - t0
+    anneal_batch([replace(j, sweeps=10) for j in jobs], ctx=ctx)  # tunes every job class, warms up
+    tune_s = time.perf_counter() - t0
+
+    def timed(js, slice_sweeps=0):
+        g0 = ctx.graph_replays()
+        t = time.perf_counter()
+        res = anneal_batch(js, ctx=ctx, slice_sweeps=slice_sweeps)
+        return res, time.perf_counter() - t, ctx.graph_replays() - g0
+
+    res, dt, _ = timed(jobs)
+    fixed, _, _ = timed([replace(j, autotune=False) for j in jobs])
+    graph, _, replays = timed(jobs, slice_sweeps=10)
     props = sum(r["proposals"] for r in res)
     dev_s = res[0]["device_ms"] / 1e3
+    fixed_s = fixed[0]["device_ms"] / 1e3
+    graph_s = graph[0]["device_ms"] / 1e3
+    same = all(a[k] == b[k] == c[k] for a, b, c in zip(res, fixed, graph) for k in ("L_cert", "proposals", "accepted"))
+    shapes = Counter(f"{r['launch']['cluster_ctas']}x{r['launch']['replicas_per_cta']}/"
+                     f"{r['launch']['cell_side']:.2f}" for r in res)
     return dict(workload=f"{instances} instances, n U[20,400], 32 replicas, {sweeps} sweeps",
                 proposals=props, seconds=dt, device_seconds=dev_s, proposals_per_s=props / dev_s,
+                fixed_shape=dict(device_seconds=fixed_s, proposals_per_s=props / fixed_s),
+                graph_slices=dict(slice_sweeps=10, graph_replays=replays, device_seconds=graph_s,
+                                  proposals_per_s=props / graph_s),
+                same_results_all_three=same, tuned_shapes=dict(shapes.most_common()), tune_seconds=tune_s,
+                overflows=sum(r["launch"]["overflows"] for r in res),
                 squares=int(sum(j.n for j in jobs)) * 32, certified=sum(r["certified"] for r in res))
 
 
