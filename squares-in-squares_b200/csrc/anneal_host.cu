@@ -148,6 +148,30 @@ void fill_result(const sqs_job& J, const JobDev& d, const JobMut& m, float dev_m
 // (cuda/polish.py:52-65): the first centre dilation in 1+1e-10 .. 1+1e-6
 // under which the GPU certifier accepts the packing.  `best[k]` is job k's
 // n x 3 FP64 state; results go to out[k] and, when certified, xya_out[k].
+int launch_groups(sqs_ctx* ctx, const std::vector<Group>& groups, const JobDev* jdev, JobMut* jmut, float4* pos,
+                  double* best, int slice) {
+    if (groups.size() == 1) {
+        const Group& g = groups[0];
+        return launch_anneal(ctx->stream, g.njobs, g.cs, g.Rl, g.smem, g.list, jdev, jmut, pos, best, slice);
+    }
+    const int na = (int)std::min<size_t>(sqs_ctx::kAux, groups.size());
+    SQS_CUDA(cudaEventRecord(ctx->fork, ctx->stream));
+    for (int a = 0; a < na; ++a) SQS_CUDA(cudaStreamWaitEvent(ctx->aux[a], ctx->fork, 0));
+    int rc = SQS_OK;
+    for (size_t k = 0; k < groups.size() && rc == SQS_OK; ++k) {
+        const Group& g = groups[k];
+        rc = launch_anneal(ctx->aux[k % sqs_ctx::kAux], g.njobs, g.cs, g.Rl, g.smem, g.list, jdev, jmut, pos, best,
+                           slice);
+    }
+    // join every side stream, also after a failed launch, so the main stream
+    // (and a capture in progress) never keeps a dangling branch
+    for (int a = 0; a < na; ++a) {
+        SQS_CUDA(cudaEventRecord(ctx->join[a], ctx->aux[a]));
+        SQS_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->join[a], 0));
+    }
+    return rc;
+}
+
 // ------------------------------------------------------------ autotuner
 // Candidate launch shapes of a job: every cluster size that divides the
 // replica count and fits, for each cell side; each is timed on the job's own
@@ -271,28 +295,63 @@ static int autotune(sqs_ctx* ctx, const sqs_job& job, int mode, sqs_tuning& out)
             }
         }
     }
-    const int sweeps = std::max(2, std::min(100, (2000 + J.n - 1) / J.n));
-    const int xe = std::min(J.exchange_every, sweeps);
-    Plan best{};
-    float best_ms = 1e30f;
+    // a trial is a whole number of exchange intervals (the job's own
+    // checkpoint frequency), about 2,000 proposals per replica
+    const int xe = J.exchange_every;
+    const int want = std::max(2, std::min(100, (2000 + J.n - 1) / J.n));
+    const int sweeps = std::max(xe, (want + xe - 1) / xe * xe);
+    struct Cand {
+        Plan p;
+        float per_copy;  // throughput mode: device time per job in a full wave; latency mode: time alone
+    };
+    std::vector<Cand> cands;
+    Plan def;
+    const bool has_def = plan_job(J.n, J.replicas, J.L0, kCellSide, 1, def);
     int trials = 0;
+    auto time_plan = [&](const Plan& p, int reps, float* per_copy) -> int {
+        int copies = 1;
+        if (int r = copies_for(J, p, mode, &copies)) return r;
+        float ms = 0.f;
+        if (int r = trial_ms(ctx, J, p, copies, sweeps, xe, reps, &ms)) return r;
+        trials += reps;
+        *per_copy = ms / (float)copies;
+        return SQS_OK;
+    };
+    // screen every shape once ...
     for (float cell : kTuneCells) {
         for (int cs = 1; cs <= 16; ++cs) {
             Plan p;
             if (!plan_job(J.n, J.replicas, J.L0, cell, cs, p) || p.cs != cs) continue;
-            int copies = 1;
-            if (int r = copies_for(J, p, mode, &copies)) return r;
-            float ms = 0.f;
-            if (int r = trial_ms(ctx, J, p, copies, sweeps, xe, 2, &ms)) return r;
-            trials += 2;
-            const float per_copy = ms / (float)copies;  // throughput: time per job
-            if (per_copy < best_ms) {
-                best_ms = per_copy;
-                best = p;
-            }
+            Cand c{p, 0.f};
+            if (int r = time_plan(p, 1, &c.per_copy)) return r;
+            cands.push_back(c);
         }
     }
-    SQS_REQUIRE(best_ms < 1e29f, "autotune: no launch shape fits n=%d with %d replicas", J.n, J.replicas);
+    SQS_REQUIRE(!cands.empty(), "autotune: no launch shape fits n=%d with %d replicas", J.n, J.replicas);
+    std::sort(cands.begin(), cands.end(), [](const Cand& a, const Cand& b) { return a.per_copy < b.per_copy; });
+    // ... then time the two fastest and the default again and keep the best
+    // of each; a shape replaces the default only when it is 3% faster
+    auto same = [](const Plan& a, const Plan& b) { return a.cs == b.cs && a.cell == b.cell; };
+    float def_ms = 1e30f;
+    for (size_t k = 0; k < cands.size(); ++k) {
+        const bool is_def = has_def && same(cands[k].p, def);
+        if (k >= 2 && !is_def) continue;
+        float t = 0.f;
+        if (int r = time_plan(cands[k].p, 2, &t)) return r;
+        cands[k].per_copy = std::min(cands[k].per_copy, t);
+        if (is_def) def_ms = cands[k].per_copy;
+    }
+    Plan best = cands[0].p;
+    float best_ms = cands[0].per_copy;
+    for (size_t k = 1; k < std::min<size_t>(2, cands.size()); ++k)
+        if (cands[k].per_copy < best_ms) {
+            best_ms = cands[k].per_copy;
+            best = cands[k].p;
+        }
+    if (has_def && def_ms < 1e29f && !same(best, def) && best_ms > 0.97f * def_ms) {
+        best = def;
+        best_ms = def_ms;
+    }
     int xe_best = job.exchange_every;
     if (tune_xe) {
         // checkpoint cost c and sweep cost s from T sweeps with 1 and with T checkpoints
@@ -489,21 +548,18 @@ extern "C" int sqs_anneal_batch(sqs_ctx* ctx, const sqs_job* jobs, int njobs, in
     cudaEvent_t e0 = ctx->ev[62], e1 = ctx->ev[63];
     SQS_CUDA(cudaEventRecord(e0, ctx->stream));
     const int rounds = std::max(1, (max_sweeps + slice - 1) / slice);
-    auto one_round = [&]() -> int {
-        for (size_t g = 0; g < keys.size(); ++g) {
-            if (int r = launch_anneal(ctx->stream, (int)spans[g].second, keys[g].first, keys[g].second, smems[g],
-                                      d_list + spans[g].first, d_jd, d_jm, d_pos, d_best, slice))
-                return r;
-        }
-        return SQS_OK;
-    };
+    std::vector<Group> launch;
+    for (size_t g = 0; g < keys.size(); ++g)
+        launch.push_back(Group{(int)spans[g].second, keys[g].first, keys[g].second, smems[g], d_list + spans[g].first});
+    auto one_round = [&]() -> int { return launch_groups(ctx, launch, d_jd, d_jm, d_pos, d_best, slice); };
     if (rounds < 3) {
         for (int k = 0; k < rounds; ++k)
             if (int r = one_round()) return r;
     } else {
         // the slice loop as a CUDA graph: one round (a launch per cluster
-        // shape) captured once and replayed; every launch reads its jobs'
-        // progress from device memory, so the replays need no host updates
+        // shape, concurrent branches) captured once and replayed; every
+        // launch reads its jobs' progress from device memory, so the replays
+        // need no host updates
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         SQS_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));

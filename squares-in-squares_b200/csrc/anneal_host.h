@@ -23,6 +23,19 @@ struct Shape {
 };
 
 int prime_anneal();
+
+// One launch of the anneal kernel: the jobs job_list[0 .. njobs) sharing a
+// cluster shape, with the shared memory of the largest.
+struct Group {
+    int njobs, cs, Rl;
+    size_t smem;
+    const int32_t* list;
+};
+// Launch every group for one slice.  Several groups run concurrently on the
+// context's side streams, forked from and joined back to its main stream
+// (under stream capture they become parallel branches of the graph).
+int launch_groups(sqs_ctx* ctx, const std::vector<Group>& groups, const JobDev* jdev, JobMut* jmut, float4* pos,
+                  double* best, int slice);
 int anneal_max_clusters(int cs, int Rl, size_t smem, int* out);
 int launch_anneal(cudaStream_t stream, int njobs, int cs, int Rl, size_t smem, const int32_t* job_list,
                   const JobDev* jdev, JobMut* jmut, float4* pos, double* best, int slice);

@@ -90,6 +90,11 @@ int sqs_ctx_create(int device, sqs_ctx** out) {
     std::strncpy(c->name, prop.name, sizeof(c->name) - 1);
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     for (int i = 0; e == cudaSuccess && i < 64; ++i) e = cudaEventCreate(&c->ev[i]);
+    for (int i = 0; e == cudaSuccess && i < sqs_ctx::kAux; ++i) {
+        e = cudaStreamCreateWithFlags(&c->aux[i], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         sqs::set_error("context set-up: %s", cudaGetErrorString(e));
         sqs_ctx_destroy(c);
@@ -105,6 +110,12 @@ int sqs_ctx_destroy(sqs_ctx* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
+    for (int i = 0; i < sqs_ctx::kAux; ++i) {
+        if (ctx->aux[i]) cudaStreamSynchronize(ctx->aux[i]);
+        if (ctx->aux[i]) cudaStreamDestroy(ctx->aux[i]);
+        if (ctx->join[i]) cudaEventDestroy(ctx->join[i]);
+    }
+    if (ctx->fork) cudaEventDestroy(ctx->fork);
     if (ctx->flush) cudaFree(ctx->flush);
     ctx->d_in.release();
     ctx->d_side.release();

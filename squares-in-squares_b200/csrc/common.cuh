@@ -59,6 +59,11 @@ struct sqs_ctx {
     char name[256] = {0};
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[64] = {};
+    // side streams that run independent launch groups concurrently, forked
+    // from and joined back to `stream` with events (kAux of them)
+    static constexpr int kAux = 4;
+    cudaStream_t aux[kAux] = {};
+    cudaEvent_t fork = nullptr, join[kAux] = {};
     void* flush = nullptr;
     size_t flush_bytes = 0;
     int64_t launches = 0;

@@ -238,15 +238,16 @@ extern "C" int sqs_server_step(sqs_server* s, int* in_flight) {
     if (!lists.empty()) {
         SQS_CUDA(cudaMemcpyAsync(s->d_list, lists.data(), sizeof(int32_t) * lists.size(), cudaMemcpyHostToDevice,
                                  s->ctx->stream));
+        std::vector<Group> launch;
         size_t gi = 0;
         for (auto& g : groups) {
-            if (int r = launch_anneal(s->ctx->stream, (int)spans[gi].second, g.first.first, g.first.second,
-                                      (size_t)(rb[g.first] * g.first.second), s->d_list + spans[gi].first, s->d_jd,
-                                      s->d_jm, (float4*)s->arena, (double*)s->arena, s->slice))
-                return r;
-            s->ctx->launches += 1;
+            launch.push_back(Group{(int)spans[gi].second, g.first.first, g.first.second,
+                                   (size_t)(rb[g.first] * g.first.second), s->d_list + spans[gi].first});
             ++gi;
         }
+        if (int r = launch_groups(s->ctx, launch, s->d_jd, s->d_jm, (float4*)s->arena, (double*)s->arena, s->slice))
+            return r;
+        s->ctx->launches += (int64_t)launch.size();
         SQS_CUDA(cudaMemcpyAsync(s->h_jm.data(), s->d_jm, sizeof(JobMut) * (size_t)s->max_active,
                                  cudaMemcpyDeviceToHost, s->ctx->stream));
         SQS_CUDA(cudaStreamSynchronize(s->ctx->stream));
