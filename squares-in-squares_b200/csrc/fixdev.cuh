@@ -199,14 +199,43 @@ FX_HEAVY Fix<F> mul(const Fix<F>& a, const Fix<F>& b, int rnd) {
     return r;
 }
 
+FX_HD uint64_t mulhi64(uint64_t a, uint64_t b) {
+#ifdef __CUDA_ARCH__
+    return __umul64hi(a, b);
+#else
+    return (uint64_t)(((unsigned __int128)a * b) >> 64);
+#endif
+}
+
+// Division of t < 2^64 by a divisor d fixed across many calls, through the
+// reciprocal m = floor((2^64 - 1) / d) computed once: q = floor(t m / 2^64)
+// never exceeds t / d and falls short of it by less than 3, so at most two
+// corrections make the quotient and remainder exact.  (Division by an
+// invariant integer through multiplication, after Granlund and Montgomery.)
+struct Recip {
+    uint64_t m;
+    uint64_t d;
+};
+FX_HD Recip recip(uint32_t d) { return Recip{~0ull / d, d}; }
+FX_HD uint64_t div_rem(uint64_t t, const Recip& R, uint64_t& rem) {
+    uint64_t q = mulhi64(t, R.m);
+    uint64_t r = t - q * R.d;
+    while (r >= R.d) {
+        ++q;
+        r -= R.d;
+    }
+    rem = r;
+    return q;
+}
+
 template <int F>
 FX_HEAVY Fix<F> div_small(const Fix<F>& a, uint32_t den) {  // half-up on the remainder
     Fix<F> r;
+    const Recip R = recip(den);
     uint64_t rem = 0;
     for (int i = 0; i <= F; ++i) {
-        const uint64_t t = rem * B9 + a.d[i];
-        r.d[i] = (uint32_t)(t / den);
-        rem = t % den;
+        const uint64_t t = rem * B9 + a.d[i];  // rem < den < 2^32: t < 2^64
+        r.d[i] = (uint32_t)div_rem(t, R, rem);
     }
     r.neg = a.neg;
     if (rem * 2 >= den) bump(r);
@@ -225,18 +254,42 @@ template <int F>
 FX_HD Iv<F> isub(const Iv<F>& a, const Iv<F>& b) { return {sub(a.lo, b.hi), sub(a.hi, b.lo)}; }
 template <int F>
 FX_HD Iv<F> ineg(const Iv<F>& a) { return {neg(a.hi), neg(a.lo)}; }
+// 1: the interval is >= 0; -1: it is <= 0; 0: it straddles zero.
+template <int F>
+FX_HD int sign_class(const Iv<F>& a) {
+    if (!a.lo.neg) return 1;
+    if (a.hi.neg || is_zero(a.hi)) return -1;
+    return 0;
+}
+
+// Interval product: the lower bound is the smallest of the four endpoint
+// products rounded toward -inf, the upper the largest rounded toward +inf
+// (the reference's imul).  Directed rounding is monotone, so the smallest
+// rounded product is the rounded smallest product: the sign cases below pick
+// the endpoints that give the exact extremes and round only those, with the
+// same bounds as rounding all four products both ways.
 template <int F>
 FX_HEAVY Iv<F> imul(const Iv<F>& a, const Iv<F>& b) {
-    Iv<F> r{mul(a.lo, b.lo, -1), mul(a.lo, b.lo, +1)};
-    const Fix<F>* x[2] = {&a.lo, &a.hi};
-    const Fix<F>* y[2] = {&b.lo, &b.hi};
-    for (int k = 1; k < 4; ++k) {
-        const Fix<F> dn = mul(*x[k >> 1], *y[k & 1], -1);
-        const Fix<F> up = mul(*x[k >> 1], *y[k & 1], +1);
-        if (cmp(dn, r.lo) < 0) r.lo = dn;
-        if (cmp(up, r.hi) > 0) r.hi = up;
+    const int sa = sign_class(a), sb = sign_class(b);
+    const Fix<F>*lx, *ly, *hx, *hy;  // endpoints of the extreme products
+    if (sa == 0 && sb == 0) {
+        const Fix<F> d1 = mul(a.lo, b.hi, -1), d2 = mul(a.hi, b.lo, -1);
+        const Fix<F> u1 = mul(a.lo, b.lo, +1), u2 = mul(a.hi, b.hi, +1);
+        return Iv<F>{cmp(d1, d2) <= 0 ? d1 : d2, cmp(u1, u2) >= 0 ? u1 : u2};
     }
-    return r;
+    if (sa > 0) {
+        if (sb > 0) { lx = &a.lo; ly = &b.lo; hx = &a.hi; hy = &b.hi; }
+        else if (sb < 0) { lx = &a.hi; ly = &b.lo; hx = &a.lo; hy = &b.hi; }
+        else { lx = &a.hi; ly = &b.lo; hx = &a.hi; hy = &b.hi; }
+    } else if (sa < 0) {
+        if (sb > 0) { lx = &a.lo; ly = &b.hi; hx = &a.hi; hy = &b.lo; }
+        else if (sb < 0) { lx = &a.hi; ly = &b.hi; hx = &a.lo; hy = &b.lo; }
+        else { lx = &a.lo; ly = &b.hi; hx = &a.lo; hy = &b.lo; }
+    } else {
+        if (sb > 0) { lx = &a.lo; ly = &b.hi; hx = &a.hi; hy = &b.hi; }
+        else { lx = &a.hi; ly = &b.lo; hx = &a.lo; hy = &b.lo; }
+    }
+    return Iv<F>{mul(*lx, *ly, -1), mul(*hx, *hy, +1)};
 }
 
 // ------------------------------------------------------------ decimal literals
