@@ -300,12 +300,16 @@ __device__ long long full_energy_cta(const Rep& R, int n, const Grid& g, float L
     return block_sum_ll(e, red);
 }
 
-// The quench of the coldest replica by the whole CTA: the same Jacobi
-// descent with backtracking as `quench`, one thread per square.  Integer
-// sums make the result identical to a single warp's.
+// The quench of the coldest replica by the whole CTA, one thread per square:
+// Jacobi gradient descent on the overlap energy with a backtracking step
+// (up to 6 trials per iteration), at most `iters` iterations, ending early at
+// zero energy, when no trial improves, or after three accepted steps in a
+// row that each gained less than 0.1%.  Gradients and energies are integer
+// sums, so the result does not depend on the CTA's width.
 __device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters, float4* grad, float4* saved,
                                 long long E, long long* red) {
     float alpha = 0.05f;
+    int stall = 0;  // consecutive accepted steps that gained less than 0.1%
     for (int it = 0; it < iters && E > 0; ++it) {
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
             const float4 P = R.sq[i];
@@ -339,7 +343,13 @@ __device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters
             saved[i] = make_float4(P.x, P.y, R.ang[i], 0.f);
         }
         __syncthreads();
-        for (int tries = 0; tries < 6; ++tries) {
+        // Trial steps move every coordinate by at most 0.1, so each partner
+        // within the pair cut-off of a moved square still sits in one of the
+        // 3 x 3 cells around it on the lists built for the saved state
+        // (1.4142 + 0.1 < 1.59 <= cell side): trial energies use those lists,
+        // and the lists are rebuilt only for an accepted step.
+        bool moved = false;
+        for (int tries = 0; tries < 6 && !moved; ++tries) {
             for (int i = threadIdx.x; i < n; i += blockDim.x) {
                 const float4 d = grad[i], o = saved[i];
                 const float sx = fminf(0.1f, fmaxf(-0.1f, alpha * d.x));
@@ -353,15 +363,29 @@ __device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters
                 R.ang[i] = a;
             }
             __syncthreads();
-            const bool fits = build_cells_cta(R, n, g);
-            const long long En = fits ? full_energy_cta(R, n, g, L, red) : E;
-            if (fits && En < E) {
+            const long long En = full_energy_cta(R, n, g, L, red);
+            if (En < E && build_cells_cta(R, n, g)) {
+                stall = En > E - E / 1000 ? stall + 1 : 0;  // less than 0.1% gained
                 E = En;
                 alpha = fminf(alpha * 1.3f, 0.2f);
-                break;
+                moved = true;
+            } else {
+                if (En < E) {  // the better state overflows a cell: lists back to the saved state
+                    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                        const float4 o = saved[i];
+                        float sn, cs;
+                        sincosf(o.z, &sn, &cs);
+                        R.sq[i] = make_float4(o.x, o.y, cs, sn);
+                        R.ang[i] = o.z;
+                    }
+                    __syncthreads();
+                    build_cells_cta(R, n, g);  // the saved state fitted
+                }
+                alpha *= 0.3f;
             }
-            alpha *= 0.3f;
-            if (tries == 5) {  // no improvement: restore the saved state
+        }
+        if (!moved || stall >= 3) {
+            if (!moved) {  // no improvement: restore the saved state (its lists are current)
                 for (int i = threadIdx.x; i < n; i += blockDim.x) {
                     const float4 o = saved[i];
                     float sn, cs;
@@ -370,9 +394,8 @@ __device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters
                     R.ang[i] = o.z;
                 }
                 __syncthreads();
-                build_cells_cta(R, n, g);
-                it = iters;
             }
+            break;
         }
     }
     return E;
