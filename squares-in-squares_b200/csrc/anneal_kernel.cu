@@ -106,34 +106,39 @@ __device__ bool build_cells(const Rep& R, int n, const Grid& g, int lane) {
 // `fn(j)` for every candidate t = lane, lane + 32, ...
 template <typename Fn>
 __device__ __forceinline__ void for_block(const Rep& R, const Grid& g, int cx, int cy, int lane, Fn&& fn) {
-    int cnt = 0, cell = 0;
-    if (lane < 9) {
-        const int x = cx + lane % 3 - 1, y = cy + lane / 3 - 1;
-        if (x >= 0 && x < g.G && y >= 0 && y < g.G) {
-            cell = y * g.G + x;
-            cnt = R.cnt[cell];
-        }
-    }
-    int incl = cnt;
-#pragma unroll
-    for (int o = 1; o < 16; o <<= 1) {
-        const int v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-    }
-    const int total = __shfl_sync(0xffffffffu, incl, 8);
+    // Every lane reads the nine cell counts (broadcast shared loads) and
+    // forms their running sum; slot t of the block belongs to the first cell
+    // whose running count exceeds t.  Lanes take slots 32 apart.
     int ends[9], cells[9];
+    int run = 0;
 #pragma unroll
     for (int c = 0; c < 9; ++c) {
-        ends[c] = __shfl_sync(0xffffffffu, incl, c);
-        cells[c] = __shfl_sync(0xffffffffu, cell, c);
+        const int x = cx + c % 3 - 1, y = cy + c / 3 - 1;
+        const bool in = x >= 0 && x < g.G && y >= 0 && y < g.G;
+        cells[c] = in ? y * g.G + x : 0;
+        run += in ? (int)R.cnt[cells[c]] : 0;
+        ends[c] = run;
     }
-    for (int t = lane; t < total; t += 32) {
+    for (int t = lane; t < run; t += 32) {
         int c = 0, start = 0;
 #pragma unroll
         for (int k = 0; k < 8; ++k)
             if (t >= ends[k]) { c = k + 1; start = ends[k]; }
         fn((int)R.slot[cells[c] * kCellK + (t - start)]);
     }
+}
+
+// Warp sum of the fixed-point energy change of one proposal: each lane's
+// term is split as hi * 2^20 + lo (0 <= lo < 2^20) and both parts are summed
+// with 32-bit warp reductions.  Exact while every lane's term is below 2^46
+// in magnitude: a proposal's lane holds a few pair terms of at most
+// 1.5 * 2^40 each (and lane 0 the wall change), far inside that.
+__device__ __forceinline__ long long warp_sum_dq(long long v) {
+    const unsigned lo = (unsigned)(v & 0xFFFFF);
+    const int hi = (int)(v >> 20);
+    const unsigned slo = __reduce_add_sync(0xffffffffu, lo);
+    const int shi = __reduce_add_sync(0xffffffffu, hi);
+    return (long long)shi * 1048576ll + (long long)slo;
 }
 
 __device__ __forceinline__ long long qe(float e) { return __float2ll_rn(e * kEScale); }
@@ -488,74 +493,86 @@ __global__ void __launch_bounds__(1024) anneal_kernel(const int32_t* __restrict_
     const int sweep_end = min(jd.sweeps_total, sweep0 + slice_sweeps);
     for (int sweep = sweep0; sweep < sweep_end; ++sweep) {
         if (active) {
-            for (int k = 0; k < n; ++k) {
-                const uint64_t ev = (uint64_t)sweep * (uint64_t)n + (uint64_t)k;
-                U4 rr{0u, 0u, 0u, 0u};
-                if (lane < 2) rr = philox4x32_10(U4{(uint32_t)ev, (uint32_t)(ev >> 32), (uint32_t)r, (uint32_t)lane}, k0, k1);
-                const uint32_t a0 = __shfl_sync(0xffffffffu, rr.x, 0), a1 = __shfl_sync(0xffffffffu, rr.y, 0);
-                const uint32_t a2 = __shfl_sync(0xffffffffu, rr.z, 0), a3 = __shfl_sync(0xffffffffu, rr.w, 0);
-                const uint32_t b0 = __shfl_sync(0xffffffffu, rr.x, 1), b1 = __shfl_sync(0xffffffffu, rr.y, 1);
-                const int i = (int)(((uint64_t)a0 * (uint64_t)n) >> 32);
-                const float rad1 = sqrtf(-2.f * __logf(u01(a1)));
-                float sn1, cs1;
-                __sincosf(6.2831853f * u01(a2), &sn1, &cs1);
-                const float rad2 = sqrtf(-2.f * __logf(u01(a3)));
-                const float n2 = rad2 * __cosf(6.2831853f * u01(b0));
-                const float dx = fminf(kMaxStep, fmaxf(-kMaxStep, jd.sigma_xy * rad1 * cs1));
-                const float dy = fminf(kMaxStep, fmaxf(-kMaxStep, jd.sigma_xy * rad1 * sn1));
-                const float da = jd.sigma_a * n2;
-                const float4 P = rep.sq[i];
-                // keep centres in [0.5, L - 0.5] without ever moving a square
-                // further than the clamped step (it may start outside)
-                const float nx = fminf(fmaxf(P.x, L - 0.5f), fmaxf(fminf(P.x, 0.5f), P.x + dx));
-                const float ny = fminf(fmaxf(P.y, L - 0.5f), fmaxf(fminf(P.y, 0.5f), P.y + dy));
-                float na = rep.ang[i] + da;
-                na = na - kHalfPiF * floorf(na * (1.0f / kHalfPiF));
-                if (!(na >= 0.f && na < kHalfPiF)) na = 0.f;
-                float ns, nc;
-                sincosf(na, &ns, &nc);
-                const int ocx = g.cx(P.x), ocy = g.cx(P.y);
-                long long dq = 0;
-                if (lane == 0) dq = qe(wall_e(nx, ny, nc, ns, L)) - qe(wall_e(P.x, P.y, P.z, P.w, L));
-                for_block(rep, g, ocx, ocy, lane, [&](int j) {
-                    if (j == i) return;
-                    const float4 Q = rep.sq[j];
-                    const float ex = Q.x - nx, ey = Q.y - ny;
-                    if (ex * ex + ey * ey < kPairCut2) dq += qe(sat_pair_energy(ex, ey, nc, ns, Q.z, Q.w));
-                    const float fx = Q.x - P.x, fy = Q.y - P.y;
-                    if (fx * fx + fy * fy < kPairCut2) dq -= qe(sat_pair_energy(fx, fy, P.z, P.w, Q.z, Q.w));
-                });
-                dq = warp_sum_ll(dq);
-                const float de = (float)dq * (1.0f / kEScale);
-                bool acc = dq <= 0 || u01(b1) < __expf(-de * invT);
-                const int ncx = g.cx(nx), ncy = g.cx(ny);
-                const int oc = ocy * g.G + ocx, ncell = ncy * g.G + ncx;
-                if (acc && oc != ncell && rep.cnt[ncell] >= kCellK) {
-                    acc = false;
-                    ++ovf;
+            for (int kb = 0; kb < n; kb += 32) {
+                // Lane l draws proposal kb + l of this sweep: two Philox blocks
+                // keyed by (sweep * n + k, replica, 0 / 1), Box-Muller for the
+                // centre step and the angle step, the uniform of the
+                // Metropolis test.  Each proposal then broadcasts its draws.
+                int di = 0;
+                float ddx = 0.f, ddy = 0.f, dda = 0.f, du = 0.f;
+                if (kb + lane < n) {
+                    const uint64_t ev = (uint64_t)sweep * (uint64_t)n + (uint64_t)(kb + lane);
+                    const U4 ra = philox4x32_10(U4{(uint32_t)ev, (uint32_t)(ev >> 32), (uint32_t)r, 0u}, k0, k1);
+                    const U4 rb = philox4x32_10(U4{(uint32_t)ev, (uint32_t)(ev >> 32), (uint32_t)r, 1u}, k0, k1);
+                    di = (int)(((uint64_t)ra.x * (uint64_t)n) >> 32);
+                    const float rad1 = sqrtf(-2.f * __logf(u01(ra.y)));
+                    float sn1, cs1;
+                    __sincosf(6.2831853f * u01(ra.z), &sn1, &cs1);
+                    const float rad2 = sqrtf(-2.f * __logf(u01(ra.w)));
+                    const float n2 = rad2 * __cosf(6.2831853f * u01(rb.x));
+                    ddx = fminf(kMaxStep, fmaxf(-kMaxStep, jd.sigma_xy * rad1 * cs1));
+                    ddy = fminf(kMaxStep, fmaxf(-kMaxStep, jd.sigma_xy * rad1 * sn1));
+                    dda = jd.sigma_a * n2;
+                    du = u01(rb.y);
                 }
-                ++props;
-                if (acc) {
-                    ++accs;
-                    E += dq;
-                    if (lane == 0) {
-                        rep.sq[i] = make_float4(nx, ny, nc, ns);
-                        rep.ang[i] = na;
-                        if (oc != ncell) {
-                            const int m = rep.cnt[oc];
-                            for (int q = 0; q < m; ++q) {
-                                if (rep.slot[oc * kCellK + q] == (uint16_t)i) {
-                                    rep.slot[oc * kCellK + q] = rep.slot[oc * kCellK + m - 1];
-                                    break;
+                const int kn = min(32, n - kb);
+                for (int q = 0; q < kn; ++q) {
+                    const int i = __shfl_sync(0xffffffffu, di, q);
+                    const float dx = __shfl_sync(0xffffffffu, ddx, q), dy = __shfl_sync(0xffffffffu, ddy, q);
+                    const float da = __shfl_sync(0xffffffffu, dda, q), u_acc = __shfl_sync(0xffffffffu, du, q);
+                    const float4 P = rep.sq[i];
+                    // keep centres in [0.5, L - 0.5] without ever moving a square
+                    // further than the clamped step (it may start outside)
+                    const float nx = fminf(fmaxf(P.x, L - 0.5f), fmaxf(fminf(P.x, 0.5f), P.x + dx));
+                    const float ny = fminf(fmaxf(P.y, L - 0.5f), fmaxf(fminf(P.y, 0.5f), P.y + dy));
+                    float na = rep.ang[i] + da;
+                    na = na - kHalfPiF * floorf(na * (1.0f / kHalfPiF));
+                    if (!(na >= 0.f && na < kHalfPiF)) na = 0.f;
+                    float ns, nc;
+                    sincosf(na, &ns, &nc);
+                    const int ocx = g.cx(P.x), ocy = g.cx(P.y);
+                    long long dq = 0;
+                    if (lane == 0) dq = qe(wall_e(nx, ny, nc, ns, L)) - qe(wall_e(P.x, P.y, P.z, P.w, L));
+                    for_block(rep, g, ocx, ocy, lane, [&](int j) {
+                        if (j == i) return;
+                        const float4 Q = rep.sq[j];
+                        const float ex = Q.x - nx, ey = Q.y - ny;
+                        if (ex * ex + ey * ey < kPairCut2) dq += qe(sat_pair_energy(ex, ey, nc, ns, Q.z, Q.w));
+                        const float fx = Q.x - P.x, fy = Q.y - P.y;
+                        if (fx * fx + fy * fy < kPairCut2) dq -= qe(sat_pair_energy(fx, fy, P.z, P.w, Q.z, Q.w));
+                    });
+                    dq = warp_sum_dq(dq);
+                    const float de = (float)dq * (1.0f / kEScale);
+                    bool acc = dq <= 0 || u_acc < __expf(-de * invT);
+                    const int ncx = g.cx(nx), ncy = g.cx(ny);
+                    const int oc = ocy * g.G + ocx, ncell = ncy * g.G + ncx;
+                    if (acc && oc != ncell && rep.cnt[ncell] >= kCellK) {
+                        acc = false;
+                        ++ovf;
+                    }
+                    ++props;
+                    if (acc) {
+                        ++accs;
+                        E += dq;
+                        if (lane == 0) {
+                            rep.sq[i] = make_float4(nx, ny, nc, ns);
+                            rep.ang[i] = na;
+                            if (oc != ncell) {
+                                const int m = rep.cnt[oc];
+                                for (int q = 0; q < m; ++q) {
+                                    if (rep.slot[oc * kCellK + q] == (uint16_t)i) {
+                                        rep.slot[oc * kCellK + q] = rep.slot[oc * kCellK + m - 1];
+                                        break;
+                                    }
                                 }
+                                rep.cnt[oc] = (uint8_t)(m - 1);
+                                rep.slot[ncell * kCellK + rep.cnt[ncell]] = (uint16_t)i;
+                                rep.cnt[ncell] = (uint8_t)(rep.cnt[ncell] + 1);
                             }
-                            rep.cnt[oc] = (uint8_t)(m - 1);
-                            rep.slot[ncell * kCellK + rep.cnt[ncell]] = (uint16_t)i;
-                            rep.cnt[ncell] = (uint8_t)(rep.cnt[ncell] + 1);
                         }
                     }
+                    __syncwarp();
                 }
-                __syncwarp();
             }
         }
         // ---- checkpoint: best-state search, shrink, replica exchange.  Only at
