@@ -439,8 +439,19 @@ def bench_plain_pt(ctx):
     t0 = time.perf_counter()
     r = anneal_batch([job], ctx=ctx)[0]
     dt = time.perf_counter() - t0
-    return dict(workload="n=10, 8 replicas, 20,000 sweeps", seconds=dt, certified=r["certified"], L=r["L"],
-                proposals=r["proposals"], proposals_per_s=r["proposals"] / dt, shrinks=r["shrinks"])
+    res = dict(workload="n=10, 8 replicas, 20,000 sweeps", seconds=dt, certified=r["certified"], L=r["L"],
+               proposals=r["proposals"], proposals_per_s=r["proposals"] / dt, shrinks=r["shrinks"])
+    # the same job on one host core: the CPU annealer of the oracle (O(n)
+    # FP64 energy change per proposal, as the reference's search computes it)
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    t0 = time.perf_counter()
+    (c,), used = O.ptsa_batch([job], threads=1)
+    cs = time.perf_counter() - t0
+    res["cpu_baseline"] = dict(proposals_per_s=c["proposals"] / cs, seconds=cs, cores=used, kind="port",
+                               best_certified_side=c["best_L"], sample="the whole job (20,000 sweeps)")
+    return res
 
 
 def bench_served_sweep(ctx, rates: str):
@@ -491,7 +502,19 @@ def bench_batched(ctx, sweeps: int = 50, instances: int = 512):
     same = all(a[k] == b[k] == c[k] for a, b, c in zip(res, fixed, graph) for k in ("L_cert", "proposals", "accepted"))
     shapes = Counter(f"{r['launch']['cluster_ctas']}x{r['launch']['replicas_per_cta']}/"
                      f"{r['launch']['cell_side']:.2f}" for r in res)
+    # CPU baseline: the oracle's annealer on all host threads, a bounded
+    # sample of the same jobs (the first 48 instances, 10 sweeps each)
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    sample = [replace(j, sweeps=10) for j in jobs[:48]]
+    t0 = time.perf_counter()
+    cres, used = O.ptsa_batch(sample, threads=os.cpu_count() or 1)
+    cs = time.perf_counter() - t0
+    cpu = dict(proposals_per_s=sum(c["proposals"] for c in cres) / cs, seconds=cs, cores=used, kind="port",
+               sample="first 48 of the instances, 10 sweeps each")
     return dict(workload=f"{instances} instances, n U[20,400], 32 replicas, {sweeps} sweeps",
+                cpu_baseline=cpu, speedup_vs_cpu=(props / dev_s) / cpu["proposals_per_s"],
                 proposals=props, seconds=dt, device_seconds=dev_s, proposals_per_s=props / dev_s,
                 fixed_shape=dict(device_seconds=fixed_s, proposals_per_s=props / fixed_s),
                 graph_slices=dict(slice_sweeps=10, graph_replays=replays, device_seconds=graph_s,

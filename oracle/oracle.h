@@ -17,6 +17,18 @@ int sqo_total_batch(int configs, int n, const double* xya, const double* L,
                     double* energy, double* grad, int64_t* cand, int threads);
 /* ptsa_oracle.c: dilation-certified side of a state and the CPU PT-SA */
 double sqo_certified_side(int n, const double* xya, double* best_out, double* lam_out);
+typedef struct sqo_job {
+    int n, replicas, sweeps, exchange_every;
+    double L0, tmin, tmax, sigma_xy, sigma_a, shrink;
+    uint64_t seed;
+    const double* xya;
+} sqo_job;
+typedef struct sqo_job_out {
+    double best_L;
+    long long proposals, accepted, xatt, xacc;
+    int shrinks, pad;
+} sqo_job_out;
+int sqo_ptsa_batch(int njobs, const sqo_job* jobs, sqo_job_out* out, int threads);
 /* certify_oracle.cpp: interval certifier of one packing */
 int sqo_certify(int n, int rows, const int* sid, const char* const* xs, const char* const* ys,
                 const char* const* as, char* L_out, int L_cap, char* reason_out, int reason_cap,

@@ -54,6 +54,8 @@ def lib():
                                   C.c_char_p, C.c_int, _dp]
         L.sqo_roundtrip.restype = None
         L.sqo_roundtrip.argtypes = [C.c_char_p, C.c_char_p, C.c_int]
+        L.sqo_ptsa_batch.restype = C.c_int
+        L.sqo_ptsa_batch.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int]
         L.sqo_certify_batch.restype = C.c_int
         L.sqo_certify_batch.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_void_p,
                                         C.c_int, C.c_void_p, C.c_void_p]
@@ -142,6 +144,31 @@ def certified_side(xya):
     lam = C.c_double(0)
     L = lib().sqo_certified_side(n, _ptr(xya, _dp), _ptr(best, _dp), C.byref(lam))
     return L, lam.value, best
+
+
+class _Job(C.Structure):
+    _fields_ = [("n", C.c_int), ("replicas", C.c_int), ("sweeps", C.c_int), ("exchange_every", C.c_int),
+                ("L0", C.c_double), ("tmin", C.c_double), ("tmax", C.c_double), ("sigma_xy", C.c_double),
+                ("sigma_a", C.c_double), ("shrink", C.c_double), ("seed", C.c_uint64), ("xya", _dp)]
+
+
+class _JobOut(C.Structure):
+    _fields_ = [("best_L", C.c_double), ("proposals", C.c_longlong), ("accepted", C.c_longlong),
+                ("xatt", C.c_longlong), ("xacc", C.c_longlong), ("shrinks", C.c_int), ("pad", C.c_int)]
+
+
+def ptsa_batch(jobs, threads=None):
+    """CPU parallel tempering (sqo_ptsa_batch) of jobs given as objects with
+    the fields of sqs.anneal.AnnealJob; returns (list of dicts, threads used)."""
+    keep = [np.ascontiguousarray(j.xya, dtype=np.float64) for j in jobs]
+    arr = (_Job * max(1, len(jobs)))()
+    for k, (j, x) in enumerate(zip(jobs, keep)):
+        arr[k] = _Job(x.shape[0], j.replicas, j.sweeps, j.exchange_every, j.L0, j.tmin, j.tmax, j.sigma_xy,
+                      j.sigma_a, j.shrink, j.seed & 0xFFFFFFFFFFFFFFFF, x.ctypes.data_as(_dp))
+    out = (_JobOut * max(1, len(jobs)))()
+    used = lib().sqo_ptsa_batch(len(jobs), C.addressof(arr), C.addressof(out), threads or os.cpu_count() or 1)
+    return [dict(best_L=o.best_L, proposals=o.proposals, accepted=o.accepted, exchange_attempts=o.xatt,
+                 exchange_accepts=o.xacc, shrinks=o.shrinks) for o in out[:len(jobs)]], used
 
 
 # ---------------------------------------------------------------- certifier

@@ -126,3 +126,24 @@ def test_candidate_ladders_match_golden(oracle):
                 continue
             ok, L, reason, _ = oracle.certify(c["n"], _ladder_rows(c["q"], want["dilation"]))
             assert ok and L == want["L"], (c["name"], key, reason)
+
+
+def test_cpu_parallel_tempering_baseline(oracle):
+    """The CPU annealer (the timed CPU baseline of the search workloads)
+    shrinks a loose grid to a dilation-certified side below its start, its
+    counters add up, and it is deterministic in its seed."""
+    from types import SimpleNamespace as NS
+    rng = np.random.default_rng(3)
+    n, w = 9, 3
+    xy = np.stack([np.arange(n) % w + 0.5, np.arange(n) // w + 0.5], 1) * 1.1
+    xya = np.concatenate([xy, rng.uniform(0, 0.05, (n, 1))], 1)
+    job = NS(xya=xya, replicas=4, sweeps=400, exchange_every=10, L0=3.3, tmin=1e-4, tmax=1e-2, sigma_xy=0.02,
+             sigma_a=0.05, shrink=0.002, seed=7)
+    (a,), used = oracle.ptsa_batch([job], threads=2)
+    (b,), _ = oracle.ptsa_batch([job], threads=1)
+    assert used == 1 and a == b
+    assert a["proposals"] == 4 * 400 * n and 0 < a["accepted"] < a["proposals"]
+    assert a["exchange_attempts"] > 0 and a["shrinks"] >= 1
+    assert 3.0 <= a["best_L"] < 3.3
+    many, used = oracle.ptsa_batch([job] * 3, threads=3)
+    assert used == 3 and all(m == a for m in many)
