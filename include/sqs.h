@@ -164,6 +164,28 @@ typedef struct sqs_job {
  * because its target cell was full can, and sqs_job_result.overflows counts
  * those. */
 #define SQS_JOB_AUTOTUNE 1
+/* Move-set options, each a counterpart of the reference search's moves:
+ *  ADAPT       step size per replica scaled by its rung (0.15 .. 2 x sigma
+ *              from the coldest to the hottest rung), by an adaptation factor
+ *              that every 16 proposals moves toward 25% acceptance
+ *              (x exp((rate - 0.25) / 2), kept in [0.1, 4]), by 3.5 on every
+ *              16th proposal, and a cooling cycle of 200 exchange rounds that
+ *              scales temperatures by 0.002^(k/199) and steps by its square
+ *              root (seeded.cu:493-494, 506-507, 614-618);
+ *  COLLECTIVE  6 proposals in 7 move a set of squares around the drawn one:
+ *              its row, its column, a disc of radius^2 2.5, its orientation
+ *              class, its diagonal strips, or all tilted squares, translated
+ *              (and rotated about it for the disc and the class), judged on
+ *              the full energy (seeded.cu:547-613);
+ *  KICK        at every exchange round an overlapped replica has its squares
+ *              jittered (more where their energy is higher) and, every other
+ *              round, its worst square moved to the emptiest point of an 8 x 8
+ *              probe grid (seeded.cu:721-778).
+ * All draws are counter-based, so a job stays reproducible and independent
+ * of batching, slicing and launch shape. */
+#define SQS_JOB_ADAPT 2
+#define SQS_JOB_COLLECTIVE 4
+#define SQS_JOB_KICK 8
 /* Pin the launch shape instead: a cluster of `cs` CTAs (1..16; it must
  * divide the replica count and fit) and cell side index k (0: 1.59, 1: 1.75,
  * 2: 1.95, 3: 2.2).  Same trajectory as any other shape (see above). */

@@ -27,9 +27,12 @@
 //   * temperatures: packing uses PACK_TMIN..PACK_TMAX; seeded uses the
 //     reference's fixed 1e-11..SEED_TMAX ladder;
 //   * SEED_POLISH is the job's polish budget (packing polishes 200 steps);
-//   * the angle proposal width is 2.5 x the move width (PACK_ROTATION,
-//     SEED_COLLECTIVE and SEED_STRUCTURED are validated and reported, like
-//     PACK_ROTATION in the reference, but do not change the search).
+//   * the move set is the reference's: step adaptation with the cooling
+//     cycle and kicks of overlapped replicas always, collective moves
+//     always for packing and under SEED_COLLECTIVE for seeded;
+//   * the angle proposal width is 2.5 x the move width (PACK_ROTATION and
+//     SEED_STRUCTURED are validated and reported, like PACK_ROTATION in the
+//     reference, but do not change the search).
 // "target_L" is the FP64 dilation-certified side of the best state and "q"
 // that state (the packing the interval certifier accepted); when no ladder
 // finds a certified state the seed is reported with its side, as the
@@ -123,6 +126,7 @@ int main(int argc, char** argv) {
     const int autotune = (int)env("AUTOTUNE", 1, 0, 1);
     const int max_chains = (int)env("MAX_CHAINS", 768, 8, 4096);
     const int polish = 200;
+    const int collective = 1;  // packing always mixes collective moves in (packing.cu:525)
 #endif
     const unsigned long long rng_seed = std::strtoull(argv[5], nullptr, 10);
 
@@ -157,7 +161,7 @@ int main(int argc, char** argv) {
         j.sweeps = sweeps;
         j.exchange_every = per_epoch;
         j.polish_iters = polish;
-        j.flags = autotune ? SQS_JOB_AUTOTUNE : 0;
+        j.flags = (autotune ? SQS_JOB_AUTOTUNE : 0) | SQS_JOB_ADAPT | SQS_JOB_KICK | (collective ? SQS_JOB_COLLECTIVE : 0);
         j.L0 = L;
         j.tmin = tmin;
         j.tmax = tmax;

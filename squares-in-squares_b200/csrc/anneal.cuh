@@ -25,8 +25,11 @@ struct JobDev {
     int64_t pos_off;                  // float4 index of replica 0, square 0
     int64_t best_off;                 // double index of the best state (n x 3)
     int64_t scr_off;                  // float4 index of the job's quench scratch (2n)
-    int32_t quench_iters, pad2;       // gradient steps of the coldest replica per checkpoint
+    int32_t quench_iters, flags;      // gradient steps of the coldest replica per checkpoint; kMove* bits
 };
+
+// Move-set options of a job (the same bits as SQS_JOB_ADAPT, _COLLECTIVE, _KICK).
+enum : int32_t { kMoveAdapt = 2, kMoveCollective = 4, kMoveKick = 8 };
 
 // Per job, advanced by every slice.
 struct JobMut {
@@ -40,6 +43,8 @@ struct JobMut {
     uint64_t proposals, accepted, xatt, xacc;
     int32_t perm[kMaxR];              // rung (temperature index) of each replica
     int64_t E[kMaxR];                 // energy of each replica, fixed point (kEScale units)
+    float adapt[kMaxR];               // step-size adaptation factor of each replica (kMoveAdapt)
+    int32_t win[kMaxR];               // accepted proposals in its current window of 16
 };
 
 // Energies are accumulated as integers in units of 2^-40: every pair and

@@ -104,11 +104,16 @@ int prepare_job(const sqs_job& J, int j, JobDev& d, JobMut& m, Plan& p, const Sh
     d.cell = p.cell;
     d.seed = J.seed;
     d.quench_iters = 64;
+    d.flags = J.flags & (kMoveAdapt | kMoveCollective | kMoveKick);
     std::memset(&m, 0, sizeof m);
     m.L = (float)J.L0;
     m.best_L = 1e30;
     m.status = J.sweeps == 0 ? kFinished : kRunning;
-    for (int r = 0; r < J.replicas; ++r) m.perm[r] = r;
+    for (int r = 0; r < J.replicas; ++r) {
+        m.perm[r] = r;
+        m.adapt[r] = 1.0f;
+        m.win[r] = 0;
+    }
     return SQS_OK;
 }
 
@@ -152,7 +157,7 @@ int launch_groups(sqs_ctx* ctx, const std::vector<Group>& groups, const JobDev* 
                   double* best, int slice) {
     if (groups.size() == 1) {
         const Group& g = groups[0];
-        return launch_anneal(ctx->stream, g.njobs, g.cs, g.Rl, g.smem, g.list, jdev, jmut, pos, best, slice);
+        return launch_anneal(ctx->stream, g.njobs, g.cs, g.Rl, g.smem, g.moves, g.list, jdev, jmut, pos, best, slice);
     }
     const int na = (int)std::min<size_t>(sqs_ctx::kAux, groups.size());
     SQS_CUDA(cudaEventRecord(ctx->fork, ctx->stream));
@@ -160,7 +165,7 @@ int launch_groups(sqs_ctx* ctx, const std::vector<Group>& groups, const JobDev* 
     int rc = SQS_OK;
     for (size_t k = 0; k < groups.size() && rc == SQS_OK; ++k) {
         const Group& g = groups[k];
-        rc = launch_anneal(ctx->aux[k % sqs_ctx::kAux], g.njobs, g.cs, g.Rl, g.smem, g.list, jdev, jmut, pos, best,
+        rc = launch_anneal(ctx->aux[k % sqs_ctx::kAux], g.njobs, g.cs, g.Rl, g.smem, g.moves, g.list, jdev, jmut, pos, best,
                            slice);
     }
     // join every side stream, also after a failed launch, so the main stream
@@ -240,7 +245,7 @@ static int trial_ms(sqs_ctx* ctx, const sqs_job& J0, const Plan& p, int copies, 
             SQS_CUDA(cudaMemcpyAsync(D + o_pos + sizeof(float4) * (size_t)pe * c, pos.data(), sizeof(float4) * pos.size(),
                                      cudaMemcpyHostToDevice, ctx->stream));
         SQS_CUDA(cudaEventRecord(ctx->ev[60], ctx->stream));
-        if (int r = launch_anneal(ctx->stream, copies, p.cs, p.Rl, (size_t)(p.rb * p.Rl), (const int32_t*)(D + o_list),
+        if (int r = launch_anneal(ctx->stream, copies, p.cs, p.Rl, (size_t)(p.rb * p.Rl), d.flags != 0, (const int32_t*)(D + o_list),
                                   (const JobDev*)(D + o_jd), (JobMut*)(D + o_jm), (float4*)(D + o_pos),
                                   (double*)(D + o_best), sweeps))
             return r;
@@ -259,7 +264,7 @@ static int copies_for(const sqs_job& J, const Plan& p, int mode, int* copies) {
     *copies = 1;
     if (mode & SQS_TUNE_LATENCY) return SQS_OK;
     int waves = 1;
-    if (int r = anneal_max_clusters(p.cs, p.Rl, (size_t)(p.rb * p.Rl), &waves)) return r;
+    if (int r = anneal_max_clusters(p.cs, p.Rl, (size_t)(p.rb * p.Rl), (J.flags & (SQS_JOB_ADAPT | SQS_JOB_COLLECTIVE | SQS_JOB_KICK)) != 0, &waves)) return r;
     const size_t per = sizeof(float4) * (size_t)job_pos_elems(J) + sizeof(double) * 3 * (size_t)J.n + 1024;
     *copies = (int)std::max<int64_t>(1, std::min<int64_t>(waves, (int64_t)(kTuneBytes / per)));
     return SQS_OK;
@@ -389,7 +394,7 @@ static int autotune(sqs_ctx* ctx, const sqs_job& job, int mode, sqs_tuning& out)
 int resolve_job(sqs_ctx* ctx, const sqs_job& job, int mode, sqs_job& eff, Shape& shape) {
     eff = job;
     shape = Shape{};
-    SQS_REQUIRE((job.flags & ~0xfff01) == 0, "unknown job flags 0x%x", (unsigned)job.flags);
+    SQS_REQUIRE((job.flags & ~0xfff0f) == 0, "unknown job flags 0x%x", (unsigned)job.flags);
     const int pin_cs = (job.flags >> 8) & 0xff, pin_cell = (job.flags >> 16) & 0xf;
     if (pin_cs || pin_cell) {
         SQS_REQUIRE(!(job.flags & SQS_JOB_AUTOTUNE), "SQS_JOB_AUTOTUNE and a pinned shape exclude each other");
@@ -520,19 +525,21 @@ extern "C" int sqs_anneal_batch(sqs_ctx* ctx, const sqs_job* jobs, int njobs, in
                                  ctx->stream));
         SQS_CUDA(cudaStreamSynchronize(ctx->stream));  // host vectors go out of scope
     }
-    // launch groups: jobs sharing (cluster size, replicas per CTA); shared memory of the largest
-    std::map<std::pair<int, int>, std::vector<int32_t>> groups;
-    for (int j = 0; j < njobs; ++j) groups[{plan[(size_t)j].cs, plan[(size_t)j].Rl}].push_back(j);
+    // launch groups: jobs sharing (cluster size, replicas per CTA, kernel
+    // instance); shared memory of the largest
+    std::map<std::tuple<int, int, int>, std::vector<int32_t>> groups;
+    for (int j = 0; j < njobs; ++j)
+        groups[{plan[(size_t)j].cs, plan[(size_t)j].Rl, (int)(jd[(size_t)j].flags != 0)}].push_back(j);
     std::vector<int32_t> lists;
     std::vector<std::pair<size_t, size_t>> spans;  // (start, count) in lists
     std::vector<size_t> smems;
-    std::vector<std::pair<int, int>> keys;
+    std::vector<std::tuple<int, int, int>> keys;
     for (auto& kv : groups) {
         int64_t rb = 0;
         for (int j : kv.second) rb = std::max(rb, plan[(size_t)j].rb);
         spans.push_back({lists.size(), kv.second.size()});
         lists.insert(lists.end(), kv.second.begin(), kv.second.end());
-        smems.push_back((size_t)(rb * kv.first.second));
+        smems.push_back((size_t)(rb * std::get<1>(kv.first)));
         keys.push_back(kv.first);
     }
     SQS_CUDA(cudaMemcpyAsync(d_list, lists.data(), sizeof(int32_t) * lists.size(), cudaMemcpyHostToDevice,
@@ -550,7 +557,8 @@ extern "C" int sqs_anneal_batch(sqs_ctx* ctx, const sqs_job* jobs, int njobs, in
     const int rounds = std::max(1, (max_sweeps + slice - 1) / slice);
     std::vector<Group> launch;
     for (size_t g = 0; g < keys.size(); ++g)
-        launch.push_back(Group{(int)spans[g].second, keys[g].first, keys[g].second, smems[g], d_list + spans[g].first});
+        launch.push_back(Group{(int)spans[g].second, std::get<0>(keys[g]), std::get<1>(keys[g]), smems[g],
+                               d_list + spans[g].first, std::get<2>(keys[g]) != 0});
     auto one_round = [&]() -> int { return launch_groups(ctx, launch, d_jd, d_jm, d_pos, d_best, slice); };
     if (rounds < 3) {
         for (int k = 0; k < rounds; ++k)

@@ -30,14 +30,15 @@ struct Group {
     int njobs, cs, Rl;
     size_t smem;
     const int32_t* list;
+    bool moves;  // the jobs use move-set options (the kernel instance with them)
 };
 // Launch every group for one slice.  Several groups run concurrently on the
 // context's side streams, forked from and joined back to its main stream
 // (under stream capture they become parallel branches of the graph).
 int launch_groups(sqs_ctx* ctx, const std::vector<Group>& groups, const JobDev* jdev, JobMut* jmut, float4* pos,
                   double* best, int slice);
-int anneal_max_clusters(int cs, int Rl, size_t smem, int* out);
-int launch_anneal(cudaStream_t stream, int njobs, int cs, int Rl, size_t smem, const int32_t* job_list,
+int anneal_max_clusters(int cs, int Rl, size_t smem, bool moves, int* out);
+int launch_anneal(cudaStream_t stream, int njobs, int cs, int Rl, size_t smem, bool moves, const int32_t* job_list,
                   const JobDev* jdev, JobMut* jmut, float4* pos, double* best, int slice);
 int launch_polish(cudaStream_t stream, int njobs, const int32_t* job_list, const JobDev* jdev, JobMut* jmut,
                   double* best, size_t smem);

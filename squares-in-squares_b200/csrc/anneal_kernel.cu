@@ -406,6 +406,203 @@ __device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters
     return E;
 }
 
+__device__ __forceinline__ float wrap_quarter_f(float a) {
+    a = a - kHalfPiF * floorf(a * (1.0f / kHalfPiF));
+    return (a >= 0.f && a < kHalfPiF) ? a : 0.f;
+}
+
+// Collective proposal (one warp, one replica): the set of squares the mode
+// selects around square `c` -- 1 its row (|dy| < 0.55), 2 its column
+// (|dx| < 0.55), 3 the disc dx^2 + dy^2 < 2.5, 4 its orientation class
+// (angles within 0.06 modulo pi/2), 5 its diagonal strips (|dx +- dy| < 0.85),
+// 6 every tilted square (0.04 < a < 1.53) -- is translated by (tx, ty)
+// (mode 6: by +-(tx, ty) alternating with the square index), rotated about
+// the drawn square by `th` for modes 3 and 4, and every moved square turned by
+// `th` (seeded.cu:547-613).  Centres stay in [0.5, L - 0.5].  The move is
+// judged on the full fixed-point energy; a rejected move (or one that
+// overflows a cell) is undone from `save`, the replica's own HBM slot, which
+// holds nothing else while a slice runs.  Returns whether it was accepted;
+// *ovf counts overflows.
+__device__ __noinline__ bool collective_move(const Rep& rep, const Grid& g, int n, float L, int lane, int mode, int c,
+                                             float tx, float ty, float th, float u, float invT, long long& E,
+                                             float4* __restrict__ save, int* ovf) {
+    const float cx = rep.sq[c].x, cy = rep.sq[c].y, ca = rep.ang[c];
+    float st, ct;
+    sincosf(th, &st, &ct);
+    __syncwarp();
+    for (int s = lane; s < n; s += 32) {
+        const float4 P = rep.sq[s];
+        const float a = rep.ang[s];
+        const float ex = P.x - cx, ey = P.y - cy, da = a - ca;
+        const bool take = mode == 1   ? fabsf(ey) < 0.55f
+                          : mode == 2 ? fabsf(ex) < 0.55f
+                          : mode == 3 ? ex * ex + ey * ey < 2.5f
+                          : mode == 4 ? (fabsf(da) < 0.06f || fabsf(da) > kHalfPiF - 0.06f)
+                          : mode == 5 ? (fabsf(ex + ey) < 0.85f || fabsf(ex - ey) < 0.85f)
+                                      : (a > 0.04f && a < 1.53f);
+        save[s] = make_float4(P.x, P.y, a, take ? 1.f : 0.f);
+        if (take) {
+            float nx, ny;
+            if (mode == 3 || mode == 4) {
+                nx = cx + ct * ex - st * ey + tx;
+                ny = cy + st * ex + ct * ey + ty;
+            } else if (mode == 6) {
+                const float sg = (s & 1) ? 1.f : -1.f;
+                nx = P.x + sg * tx;
+                ny = P.y + sg * ty;
+            } else {
+                nx = P.x + tx;
+                ny = P.y + ty;
+            }
+            nx = fminf(L - 0.5f, fmaxf(0.5f, nx));
+            ny = fminf(L - 0.5f, fmaxf(0.5f, ny));
+            const float na = wrap_quarter_f(a + th);
+            float sn, cs;
+            sincosf(na, &sn, &cs);
+            rep.sq[s] = make_float4(nx, ny, cs, sn);
+            rep.ang[s] = na;
+        }
+    }
+    __syncwarp();
+    const bool fits = build_cells(rep, n, g, lane);
+    bool acc = false;
+    if (fits) {
+        const long long En = full_energy(rep, n, g, L, lane);
+        const long long dq = En - E;
+        acc = dq <= 0 || u < __expf(-((float)dq * (1.0f / kEScale)) * invT);
+        if (acc) E = En;
+    } else {
+        ++*ovf;
+    }
+    if (!acc) {
+        for (int s = lane; s < n; s += 32) {
+            const float4 o = save[s];
+            if (o.w != 0.f) {
+                float sn, cs;
+                sincosf(o.z, &sn, &cs);
+                rep.sq[s] = make_float4(o.x, o.y, cs, sn);
+                rep.ang[s] = o.z;
+            }
+        }
+        __syncwarp();
+        build_cells(rep, n, g, lane);  // the saved state fitted
+    }
+    return acc;
+}
+
+// Kick of an overlapped replica at an exchange round (seeded.cu:721-778):
+// every square's energy (its wall term and its pairs); on odd rounds, when
+// the worst square's energy exceeds 1e-5, that square moves to the probe of
+// an 8 x 8 grid over [0.55, L - 0.55]^2 farthest from every other centre
+// (jittered by up to 0.05, a fresh angle); then every square is jittered,
+// by up to 0.08 / 0.18 rad where its energy exceeds 1e-6 and 0.008 / 0.015
+// elsewhere.  Draws are Philox blocks keyed by (round, square, replica).
+// Returns the new energy (the old one if a cell would overflow, the state
+// then restored from `save`).
+__device__ __noinline__ long long kick_replica(const Rep& rep, const Grid& g, int n, float L, int lane, int r,
+                                               int round, uint32_t k0, uint32_t k1, long long E,
+                                               float4* __restrict__ save) {
+    float wmax = -1.f;
+    int worst = 0x7fffffff;
+    for (int s = lane; s < n; s += 32) {
+        const float4 P = rep.sq[s];
+        float e = wall_e(P.x, P.y, P.z, P.w, L);
+        const int cxs = g.cx(P.x), cys = g.cx(P.y);
+        for (int dyc = -1; dyc <= 1; ++dyc) {
+            for (int dxc = -1; dxc <= 1; ++dxc) {
+                const int x = cxs + dxc, y = cys + dyc;
+                if (x < 0 || x >= g.G || y < 0 || y >= g.G) continue;
+                const int cell = y * g.G + x, m = rep.cnt[cell];
+                for (int k = 0; k < m; ++k) {
+                    const int j = rep.slot[cell * kCellK + k];
+                    if (j == s) continue;
+                    const float4 Q = rep.sq[j];
+                    const float dx = Q.x - P.x, dy = Q.y - P.y;
+                    if (dx * dx + dy * dy < kPairCut2) e += sat_pair_energy(dx, dy, P.z, P.w, Q.z, Q.w);
+                }
+            }
+        }
+        save[s] = make_float4(P.x, P.y, rep.ang[s], e);
+        if (e > wmax) {
+            wmax = e;
+            worst = s;
+        }
+    }
+    // warp arg-max (ties: the smaller index)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float om = __shfl_xor_sync(0xffffffffu, wmax, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, worst, o);
+        if (om > wmax || (om == wmax && oi < worst)) {
+            wmax = om;
+            worst = oi;
+        }
+    }
+    if ((round & 1) && wmax > 1e-5f && worst < n) {
+        float bd = -1.f;
+        int bp = 64;
+        for (int p = lane; p < 64; p += 32) {
+            const float vx = 0.55f + (L - 1.1f) * ((float)(p % 8) + 0.5f) / 8.f;
+            const float vy = 0.55f + (L - 1.1f) * ((float)(p / 8) + 0.5f) / 8.f;
+            float d2 = 1e9f;
+            for (int j = 0; j < n; ++j) {
+                if (j == worst) continue;
+                const float dx = vx - rep.sq[j].x, dy = vy - rep.sq[j].y;
+                d2 = fminf(d2, dx * dx + dy * dy);
+            }
+            if (d2 > bd) {
+                bd = d2;
+                bp = p;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float od = __shfl_xor_sync(0xffffffffu, bd, o);
+            const int op = __shfl_xor_sync(0xffffffffu, bp, o);
+            if (od > bd || (od == bd && op < bp)) {
+                bd = od;
+                bp = op;
+            }
+        }
+        if (lane == 0) {
+            const U4 q = philox4x32_10(U4{(uint32_t)round, 0xffffu, (uint32_t)r, 3u}, k0, k1);
+            const float vx = 0.55f + (L - 1.1f) * ((float)(bp % 8) + 0.5f) / 8.f;
+            const float vy = 0.55f + (L - 1.1f) * ((float)(bp / 8) + 0.5f) / 8.f;
+            const float na = wrap_quarter_f(u01(q.z) * kHalfPiF);
+            float sn, cs;
+            sincosf(na, &sn, &cs);
+            rep.sq[worst] = make_float4(fminf(L - 0.5f, fmaxf(0.5f, vx + 0.05f * (2.f * u01(q.x) - 1.f))),
+                                        fminf(L - 0.5f, fmaxf(0.5f, vy + 0.05f * (2.f * u01(q.y) - 1.f))), cs, sn);
+            rep.ang[worst] = na;
+        }
+        __syncwarp();
+    }
+    for (int s = lane; s < n; s += 32) {
+        const float hot = save[s].w > 1e-6f;
+        const float axy = hot ? 0.08f : 0.008f, aa = hot ? 0.18f : 0.015f;
+        const U4 q = philox4x32_10(U4{(uint32_t)round, (uint32_t)s, (uint32_t)r, 2u}, k0, k1);
+        const float4 P = rep.sq[s];
+        const float na = wrap_quarter_f(rep.ang[s] + aa * (2.f * u01(q.z) - 1.f));
+        float sn, cs;
+        sincosf(na, &sn, &cs);
+        rep.sq[s] = make_float4(fminf(L - 0.48f, fmaxf(0.48f, P.x + axy * (2.f * u01(q.x) - 1.f))),
+                                fminf(L - 0.48f, fmaxf(0.48f, P.y + axy * (2.f * u01(q.y) - 1.f))), cs, sn);
+        rep.ang[s] = na;
+    }
+    __syncwarp();
+    if (build_cells(rep, n, g, lane)) return full_energy(rep, n, g, L, lane);
+    for (int s = lane; s < n; s += 32) {
+        const float4 o = save[s];
+        float sn, cs;
+        sincosf(o.z, &sn, &cs);
+        rep.sq[s] = make_float4(o.x, o.y, cs, sn);
+        rep.ang[s] = o.z;
+    }
+    __syncwarp();
+    build_cells(rep, n, g, lane);
+    return E;
+}
+
 struct CtaShared {
     JobDev jd;
     JobMut jm;
@@ -422,6 +619,9 @@ struct CtaShared {
     long long qE;              // energy of the replica quenched by this CTA
 };
 
+// MOVES: whether the move-set options (adaptation, collective moves, kicks)
+// are compiled in; jobs without them run the leaner instance.
+template <bool MOVES>
 __global__ void __launch_bounds__(1024) anneal_kernel(const int32_t* __restrict__ job_list,
                                                       const JobDev* __restrict__ jdev, JobMut* __restrict__ jmut,
                                                       float4* __restrict__ pos, double* __restrict__ best,
@@ -487,7 +687,14 @@ __global__ void __launch_bounds__(1024) anneal_kernel(const int32_t* __restrict_
     }
     unsigned long long props = 0, accs = 0;
     int ovf = 0;
-    float invT = active ? 1.0f / S.temps[S.jm.perm[r]] : 0.f;
+    // move-set options: step adaptation with a cooling cycle of 200 exchange
+    // rounds (temperatures x 0.002^(k/199), steps x its square root)
+    const bool adaptive = MOVES && (jd.flags & kMoveAdapt) != 0;
+    float adapt = (MOVES && active) ? S.jm.adapt[r] : 1.f;
+    int win = (MOVES && active) ? S.jm.win[r] : 0;
+    float cool = adaptive ? powf(0.002f, (float)(S.jm.xround % 200) / 199.f) : 1.f;
+    float invT = active ? 1.0f / (S.temps[S.jm.perm[r]] * cool) : 0.f;
+    float4* save = pos + jd.pos_off + (int64_t)r * n;  // this replica's HBM slot: free while the slice runs
 
     const int sweep0 = S.jm.sweep;
     const int sweep_end = min(jd.sweeps_total, sweep0 + slice_sweeps);
@@ -510,16 +717,34 @@ __global__ void __launch_bounds__(1024) anneal_kernel(const int32_t* __restrict_
                     __sincosf(6.2831853f * u01(ra.z), &sn1, &cs1);
                     const float rad2 = sqrtf(-2.f * __logf(u01(ra.w)));
                     const float n2 = rad2 * __cosf(6.2831853f * u01(rb.x));
-                    ddx = fminf(kMaxStep, fmaxf(-kMaxStep, jd.sigma_xy * rad1 * cs1));
-                    ddy = fminf(kMaxStep, fmaxf(-kMaxStep, jd.sigma_xy * rad1 * sn1));
+                    ddx = jd.sigma_xy * rad1 * cs1;
+                    ddy = jd.sigma_xy * rad1 * sn1;
                     dda = jd.sigma_a * n2;
                     du = u01(rb.y);
+                    if (MOVES && (jd.flags & kMoveCollective)) di |= (int)(rb.z % 7u) << 16;  // move mode
                 }
                 const int kn = min(32, n - kb);
                 for (int q = 0; q < kn; ++q) {
-                    const int i = __shfl_sync(0xffffffffu, di, q);
-                    const float dx = __shfl_sync(0xffffffffu, ddx, q), dy = __shfl_sync(0xffffffffu, ddy, q);
-                    const float da = __shfl_sync(0xffffffffu, dda, q), u_acc = __shfl_sync(0xffffffffu, du, q);
+                    const int dpk = __shfl_sync(0xffffffffu, di, q);
+                    const int i = dpk & 0xffff, mode = dpk >> 16;
+                    const float sdx = __shfl_sync(0xffffffffu, ddx, q), sdy = __shfl_sync(0xffffffffu, ddy, q);
+                    const float sda = __shfl_sync(0xffffffffu, dda, q), u_acc = __shfl_sync(0xffffffffu, du, q);
+                    float sc = 1.f;  // step scale (adaptive moves)
+                    const int pidx = kb + q;
+                    if (adaptive) {
+                        const int rung = S.jm.perm[r];
+                        sc = adapt * (R > 1 ? 0.15f + 1.85f * (float)rung / (float)(R - 1) : 1.f) * sqrtf(cool);
+                        if ((((uint64_t)sweep * (uint64_t)n + (uint64_t)pidx) & 15u) == 0) sc *= 3.5f;
+                    }
+                    const float dx = fminf(kMaxStep, fmaxf(-kMaxStep, sdx * sc));
+                    const float dy = fminf(kMaxStep, fmaxf(-kMaxStep, sdy * sc));
+                    const float da = sda * sc;
+                    bool acc;
+                    if (MOVES && mode != 0) {
+                        acc = collective_move(rep, g, n, L, lane, mode, i, dx, dy, da, u_acc, invT, E, save, &ovf);
+                        ++props;
+                        accs += acc;
+                    } else {
                     const float4 P = rep.sq[i];
                     // keep centres in [0.5, L - 0.5] without ever moving a square
                     // further than the clamped step (it may start outside)
@@ -543,7 +768,7 @@ __global__ void __launch_bounds__(1024) anneal_kernel(const int32_t* __restrict_
                     });
                     dq = warp_sum_dq(dq);
                     const float de = (float)dq * (1.0f / kEScale);
-                    bool acc = dq <= 0 || u_acc < __expf(-de * invT);
+                    acc = dq <= 0 || u_acc < __expf(-de * invT);
                     const int ncx = g.cx(nx), ncy = g.cx(ny);
                     const int oc = ocy * g.G + ocx, ncell = ncy * g.G + ncx;
                     if (acc && oc != ncell && rep.cnt[ncell] >= kCellK) {
@@ -569,6 +794,14 @@ __global__ void __launch_bounds__(1024) anneal_kernel(const int32_t* __restrict_
                                 rep.slot[ncell * kCellK + rep.cnt[ncell]] = (uint16_t)i;
                                 rep.cnt[ncell] = (uint8_t)(rep.cnt[ncell] + 1);
                             }
+                        }
+                    }
+                    }
+                    if (adaptive) {  // every 16 proposals: steer toward 25% acceptance
+                        win += acc;
+                        if ((((uint64_t)sweep * (uint64_t)n + (uint64_t)pidx + 1u) & 15u) == 0) {
+                            adapt = fmaxf(0.1f, fminf(4.0f, adapt * expf(((float)win / 16.f - 0.25f) * 0.5f)));
+                            win = 0;
                         }
                     }
                     __syncwarp();
@@ -648,7 +881,7 @@ __global__ void __launch_bounds__(1024) anneal_kernel(const int32_t* __restrict_
                     const int a = holder[k], b = holder[k + 1];
                     const U4 u = philox4x32_10(U4{(uint32_t)S.jm.xround, (uint32_t)k, 0u, 0x7fffffffu}, k0, k1);
                     const float d = (1.0f / S.temps[k] - 1.0f / S.temps[k + 1]) *
-                                    ((float)(Eall[a] - Eall[b]) * (1.0f / kEScale));
+                                    ((float)(Eall[a] - Eall[b]) * (1.0f / kEScale)) / cool;
                     S.jm.xatt += 1;
                     if (d >= 0.f || u01(u.x) < expf(d)) {
                         S.jm.xacc += 1;
@@ -663,8 +896,9 @@ __global__ void __launch_bounds__(1024) anneal_kernel(const int32_t* __restrict_
         }
         cluster.sync();
         __syncthreads();
+        if (adaptive) cool = powf(0.002f, (float)(S.jm.xround % 200) / 199.f);
         if (active) {
-            invT = 1.0f / S.temps[S.jm.perm[r]];
+            invT = 1.0f / (S.temps[S.jm.perm[r]] * cool);
             if (S.decision_win == r) {
                 // new best: dilated, translated to the origin, angles in [0, pi/2)
                 double* dst = best + jd.best_off;
@@ -706,6 +940,10 @@ __global__ void __launch_bounds__(1024) anneal_kernel(const int32_t* __restrict_
                 return;
             }
         }
+        // overlapped replicas are kicked (the round just completed decides
+        // whether the worst square is also moved)
+        if (MOVES && active && (jd.flags & kMoveKick) && E > qe(1e-12f))
+            E = kick_replica(rep, g, n, L, lane, r, S.jm.xround, k0, k1, E, save);
     }
 
     // ---- write the slice back
@@ -714,6 +952,10 @@ __global__ void __launch_bounds__(1024) anneal_kernel(const int32_t* __restrict_
         for (int i = lane; i < n; i += 32) dst[i] = make_float4(rep.sq[i].x, rep.sq[i].y, rep.ang[i], 0.f);
         if (lane == 0) {
             jmut[job].E[r] = E;
+            if (MOVES) {
+                jmut[job].adapt[r] = adapt;
+                jmut[job].win[r] = win;
+            }
             atomicAdd(reinterpret_cast<unsigned long long*>(&jmut[job].proposals), props);
             atomicAdd(reinterpret_cast<unsigned long long*>(&jmut[job].accepted), accs);
             if (ovf) atomicAdd(&jmut[job].overflows, ovf);
@@ -741,52 +983,54 @@ int prime_anneal() {
     int dev = 0;
     SQS_CUDA(cudaGetDevice(&dev));
     if (!attr_done[dev & 63]) {
-        cudaFuncAttributes fa;
-        SQS_CUDA(cudaFuncGetAttributes(&fa, anneal_kernel));
-        SQS_CUDA(cudaFuncSetAttribute(anneal_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      232448 - (int)fa.sharedSizeBytes));
-        SQS_CUDA(cudaFuncSetAttribute(anneal_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        for (int v = 0; v < 2; ++v) {
+            const void* fn = v ? (const void*)anneal_kernel<true> : (const void*)anneal_kernel<false>;
+            cudaFuncAttributes fa;
+            SQS_CUDA(cudaFuncGetAttributes(&fa, fn));
+            SQS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          232448 - (int)fa.sharedSizeBytes));
+            SQS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        }
         attr_done[dev & 63] = true;
     }
     return SQS_OK;
 }
 
-// Clusters of this shape that can be resident at once (one wave).
-int anneal_max_clusters(int cs, int Rl, size_t smem, int* out) {
-    if (int r = prime_anneal()) return r;
+static cudaLaunchConfig_t anneal_config(int clusters, int cs, int Rl, size_t smem, cudaStream_t stream,
+                                        cudaLaunchAttribute* attr) {
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)cs, 1, 1);
+    cfg.gridDim = dim3((unsigned)(clusters * cs), 1, 1);
     cfg.blockDim = dim3((unsigned)(Rl * 32), 1, 1);
     cfg.dynamicSmemBytes = smem;
-    cudaLaunchAttribute attr[1];
+    cfg.stream = stream;
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = (unsigned)cs;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    return cfg;
+}
+
+// Clusters of this shape that can be resident at once (one wave).
+int anneal_max_clusters(int cs, int Rl, size_t smem, bool moves, int* out) {
+    if (int r = prime_anneal()) return r;
+    cudaLaunchAttribute attr[1];
+    const cudaLaunchConfig_t cfg = anneal_config(1, cs, Rl, smem, nullptr, attr);
     int num = 0;
-    SQS_CUDA(cudaOccupancyMaxActiveClusters(&num, anneal_kernel, &cfg));
+    if (moves) SQS_CUDA(cudaOccupancyMaxActiveClusters(&num, anneal_kernel<true>, &cfg));
+    else SQS_CUDA(cudaOccupancyMaxActiveClusters(&num, anneal_kernel<false>, &cfg));
     *out = num;
     return SQS_OK;
 }
 
-int launch_anneal(cudaStream_t stream, int njobs, int cs, int Rl, size_t smem, const int32_t* job_list,
+int launch_anneal(cudaStream_t stream, int njobs, int cs, int Rl, size_t smem, bool moves, const int32_t* job_list,
                   const JobDev* jdev, JobMut* jmut, float4* pos, double* best, int slice) {
     if (int r = prime_anneal()) return r;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)(njobs * cs), 1, 1);
-    cfg.blockDim = dim3((unsigned)(Rl * 32), 1, 1);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = stream;
     cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = (unsigned)cs;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    SQS_CUDA(cudaLaunchKernelEx(&cfg, anneal_kernel, job_list, jdev, jmut, pos, best, slice));
+    const cudaLaunchConfig_t cfg = anneal_config(njobs, cs, Rl, smem, stream, attr);
+    if (moves) SQS_CUDA(cudaLaunchKernelEx(&cfg, anneal_kernel<true>, job_list, jdev, jmut, pos, best, slice));
+    else SQS_CUDA(cudaLaunchKernelEx(&cfg, anneal_kernel<false>, job_list, jdev, jmut, pos, best, slice));
     return SQS_OK;
 }
 

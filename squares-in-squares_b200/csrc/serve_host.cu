@@ -26,6 +26,7 @@
 #include <cstring>
 #include <deque>
 #include <map>
+#include <tuple>
 #include <unordered_map>
 #include <vector>
 
@@ -220,12 +221,12 @@ extern "C" int sqs_server_step(sqs_server* s, int* in_flight) {
     if (int r = enter(s->ctx)) return r;
     if (int r = admit(s)) return r;
     // one slice for every admitted job, one launch per cluster shape
-    std::map<std::pair<int, int>, std::vector<int32_t>> groups;
-    std::map<std::pair<int, int>, int64_t> rb;
+    std::map<std::tuple<int, int, int>, std::vector<int32_t>> groups;
+    std::map<std::tuple<int, int, int>, int64_t> rb;
     for (int k = 0; k < s->max_active; ++k) {
         if (s->slot_job[(size_t)k] < 0) continue;
         const SJob& j = s->jobs[s->slot_job[(size_t)k]];
-        const auto key = std::make_pair(j.plan.cs, j.plan.Rl);
+        const auto key = std::make_tuple(j.plan.cs, j.plan.Rl, (int)(j.jd.flags != 0));
         groups[key].push_back(k);
         rb[key] = std::max(rb[key], j.plan.rb);
     }
@@ -241,8 +242,9 @@ extern "C" int sqs_server_step(sqs_server* s, int* in_flight) {
         std::vector<Group> launch;
         size_t gi = 0;
         for (auto& g : groups) {
-            launch.push_back(Group{(int)spans[gi].second, g.first.first, g.first.second,
-                                   (size_t)(rb[g.first] * g.first.second), s->d_list + spans[gi].first});
+            launch.push_back(Group{(int)spans[gi].second, std::get<0>(g.first), std::get<1>(g.first),
+                                   (size_t)(rb[g.first] * std::get<1>(g.first)), s->d_list + spans[gi].first,
+                                   std::get<2>(g.first) != 0});
             ++gi;
         }
         if (int r = launch_groups(s->ctx, launch, s->d_jd, s->d_jm, (float4*)s->arena, (double*)s->arena, s->slice))

@@ -68,6 +68,9 @@ class PolishResult(C.Structure):
 
 
 JOB_AUTOTUNE = 1
+JOB_ADAPT = 2
+JOB_COLLECTIVE = 4
+JOB_KICK = 8
 TUNE_LATENCY = 1
 
 

@@ -36,6 +36,9 @@ class AnnealJob:
     seed: int = 42
     polish_iters: int = 200
     autotune: bool = False          # launch shape / cell side (and exchange_every=0) from the autotuner
+    adapt: bool = False             # step adaptation, rung-scaled steps, cooling cycle (SQS_JOB_ADAPT)
+    collective: bool = False        # row / column / disc / class / diagonal / tilted set moves (SQS_JOB_COLLECTIVE)
+    kick: bool = False              # kick and reseed of overlapped replicas at exchange rounds (SQS_JOB_KICK)
     cluster: int = 0                # pinned cluster size (0: default / tuned)
     cell_index: int = 0             # pinned cell side index (0: 1.59, 1: 1.75, 2: 1.95, 3: 2.2)
     n: int = field(init=False)
@@ -45,9 +48,15 @@ class AnnealJob:
         self.n = self.xya.shape[0]
 
 
+def _flags(j: AnnealJob) -> int:
+    return ((N.JOB_AUTOTUNE if j.autotune else 0) | (N.JOB_ADAPT if j.adapt else 0) |
+            (N.JOB_COLLECTIVE if j.collective else 0) | (N.JOB_KICK if j.kick else 0) |
+            (j.cluster << 8) | (j.cell_index << 16))
+
+
 def _cjob(j: AnnealJob) -> N.Job:
     return N.Job(n=j.n, replicas=j.replicas, sweeps=j.sweeps, exchange_every=j.exchange_every,
-                 polish_iters=j.polish_iters, flags=(N.JOB_AUTOTUNE if j.autotune else 0) | (j.cluster << 8) | (j.cell_index << 16), L0=j.L0, tmin=j.tmin, tmax=j.tmax, sigma_xy=j.sigma_xy,
+                 polish_iters=j.polish_iters, flags=_flags(j), L0=j.L0, tmin=j.tmin, tmax=j.tmax, sigma_xy=j.sigma_xy,
                  sigma_a=j.sigma_a, shrink=j.shrink, seed=j.seed & 0xFFFFFFFFFFFFFFFF,
                  xya=j.xya.ctypes.data_as(C.POINTER(C.c_double)))
 

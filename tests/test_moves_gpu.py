@@ -1,0 +1,63 @@
+"""The reference's richer move set on the GPU annealer: step adaptation with
+the cooling cycle (SQS_JOB_ADAPT), collective set moves (SQS_JOB_COLLECTIVE)
+and kicks of overlapped replicas (SQS_JOB_KICK).  Each option runs to a
+certified packing, changes the trajectory, and keeps a job's result
+independent of batching, slicing and launch shape."""
+from __future__ import annotations
+
+from dataclasses import replace
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ("L", "L_cert", "L_polished", "proposals", "accepted", "shrinks", "improvements",
+        "exchange_attempts", "exchange_accepts", "q")
+OPTIONS = [dict(adapt=True), dict(collective=True), dict(kick=True), dict(adapt=True, collective=True, kick=True)]
+
+
+def _job(n=40, seed=13, sweeps=200, replicas=16, **kw):
+    from sqs.anneal import AnnealJob, jittered_grid
+    xya, L0 = jittered_grid(n, seed=seed)
+    args = dict(L0=L0, replicas=replicas, sweeps=sweeps, exchange_every=10, tmin=1e-4, tmax=5e-2, seed=seed,
+                polish_iters=50)
+    args.update(kw)
+    return AnnealJob(xya, **args)
+
+
+@pytest.mark.parametrize("opts", OPTIONS, ids=lambda o: "+".join(o))
+def test_move_options_are_reproducible(ctx, oracle, opts):
+    from sqs.anneal import anneal_batch
+    job = _job(**opts)
+    plain = anneal_batch([_job()], ctx=ctx)[0]
+    alone = anneal_batch([job], ctx=ctx)[0]
+    assert alone["status"] == 0, alone["reason"]
+    assert alone["proposals"] == 16 * 200 * 40
+    assert alone["launch"]["overflows"] == 0
+    assert alone["q"] != plain["q"] or alone["accepted"] != plain["accepted"]  # the option acts
+    if alone["certified"]:
+        ok, L, reason, _ = oracle.certify(40, alone["rows"])
+        assert ok and L == alone["L"], reason
+    mixed = anneal_batch([_job(n=25, seed=2), job, _job(n=60, seed=5, **opts)], ctx=ctx)[1]
+    sliced = anneal_batch([job], ctx=ctx, slice_sweeps=50)[0]
+    wide = anneal_batch([replace(job, cluster=4)], ctx=ctx)[0]
+    for k in KEYS:
+        assert mixed[k] == alone[k], ("mixed", k)
+        assert sliced[k] == alone[k], ("sliced", k)
+        assert wide[k] == alone[k], ("cluster 4", k)
+
+
+def test_adaptation_steers_acceptance(ctx):
+    from sqs.anneal import AnnealJob, anneal_batch, jittered_grid
+    # an exact 6 x 6 grid at side 6: every square touches its neighbours, so
+    # large fixed steps at low temperature are almost always rejected; the
+    # adapted steps shrink (down to the factor's floor of 0.1 on the coldest
+    # rungs) and are accepted many times more often
+    xya, _ = jittered_grid(36, jitter=0.0, angle_hi=1e-9, seed=1)
+    args = dict(L0=6.0, replicas=8, sweeps=300, exchange_every=10, tmin=1e-6, tmax=1e-4, sigma_xy=0.1,
+                sigma_a=0.3, seed=4, polish_iters=0)
+    fixed = anneal_batch([AnnealJob(xya, **args)], ctx=ctx)[0]
+    adapt = anneal_batch([AnnealJob(xya, adapt=True, **args)], ctx=ctx)[0]
+    rf = fixed["accepted"] / fixed["proposals"]
+    ra = adapt["accepted"] / adapt["proposals"]
+    assert ra > 10 * rf and 0.005 < ra < 0.6, (rf, ra)
