@@ -154,6 +154,9 @@ typedef struct sqs_job {
     double shrink;           /* relative shrink of the side after each improvement*/
     uint64_t seed;
     const double* xya;       /* initial state, n rows of (x, y, angle), host      */
+    const double* xya_rep;   /* optional: replicas * n rows, each replica's own
+                                start (e.g. from sqs_portfolio); NULL: every
+                                replica starts from xya                          */
 } sqs_job;
 
 /* Launch shape, cell side and (when the job leaves it at 0) exchange
@@ -224,6 +227,21 @@ typedef struct sqs_job_result {
  * tuned for latency when njobs == 1, for throughput otherwise. */
 int sqs_anneal_batch(sqs_ctx* ctx, const sqs_job* jobs, int njobs, int slice_sweeps, double* const* xya_out,
                      sqs_job_result* out);
+
+/* Initial states of `chains` search chains (out: chains * n rows of x, y,
+ * angle), the reference's structured portfolio (build_portfolio,
+ * seeded.cu:233-425): by chain b's group b % 8 within its ladder b / 8, the
+ * seed, one of up to 64 corner-triangle + 45-degree-band topologies that fit
+ * n to n + 4 squares in a side within [sqrt n - 0.05, L + 0.15], a corner
+ * grid with tilted edge rows, or corner anchors with a rotated grid.
+ * structured = 0 copies the seed to every chain.  jitter != 0 then applies
+ * the per-chain jitter of structured_init (seeded.cu:427-451: none for group
+ * 0, 1e-4 * 100^u for group 1, 0.03 otherwise) from rng_seed with this
+ * library's generator.  Host only; the layouts before the jitter equal the
+ * reference's bit for bit.  The chains of ladder k are the replicas of an
+ * 8-replica job (sqs_job.xya_rep). */
+int sqs_portfolio(int n, double L, const double* seed_xya, int chains, int structured, uint64_t rng_seed, int jitter,
+                  double* out);
 
 /* FP64 gradient polish of `count` packings, one CTA each, all pairs.
  * Packing k has n_of[k] rows (1..1000) of (x, y, angle) in xya, packings

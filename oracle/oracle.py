@@ -77,6 +77,8 @@ def ref_seeded():
         L.ref_pair_smooth.argtypes = [_dp, _dp, _dp]
         L.ref_boundary.restype = C.c_double
         L.ref_boundary.argtypes = [_dp, C.c_double, _dp]
+        L.ref_build_portfolio.restype = C.c_int
+        L.ref_build_portfolio.argtypes = [C.c_int, C.c_int, C.c_double, _dp, C.c_int, _dp]
         L.ref_total_batch.restype = C.c_int
         L.ref_total_batch.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp, C.c_int]
         _REF_SEEDED = L
@@ -135,6 +137,25 @@ def ref_total_batch(xya, L, grad=True, threads=None):
     used = ref_seeded().ref_total_batch(configs, n, _ptr(xya, _dp), _ptr(L, _dp), _ptr(e, _dp),
                                         _ptr(g, _dp), threads)
     return e, g, used
+
+
+def ref_portfolio(n, L, seed_xya, chains, structured=1):
+    """The reference's build_portfolio (seeded.cu:233-425): (chains, n, 3)."""
+    seed = np.ascontiguousarray(seed_xya, dtype=np.float64)
+    out = np.zeros((chains, n, 3))
+    ref_seeded().ref_build_portfolio(n, chains, float(L), _ptr(seed, _dp), structured, _ptr(out, _dp))
+    return out
+
+
+def ref_portfolio_packing(n, L, seed_xya, chains):
+    """The `packing` program's portfolio (dpack::build_portfolio): (chains, n, 3)."""
+    lib_ = C.CDLL(str(HERE / "_ref" / "libref_packing.so"))
+    lib_.ref_build_portfolio_packing.restype = C.c_int
+    lib_.ref_build_portfolio_packing.argtypes = [C.c_int, C.c_int, C.c_double, _dp, _dp]
+    seed = np.ascontiguousarray(seed_xya, dtype=np.float64)
+    out = np.zeros((chains, n, 3))
+    lib_.ref_build_portfolio_packing(n, chains, float(L), _ptr(seed, _dp), _ptr(out, _dp))
+    return out
 
 
 def certified_side(xya):

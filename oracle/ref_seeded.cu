@@ -70,3 +70,19 @@ extern "C" int ref_total_batch(int configs, int n, const double* xya, const doub
     for (auto& th : pool) th.join();
     return threads;
 }
+
+// The reference's structured initial portfolio (build_portfolio, host code
+// in seeded.cu) for `chains` chains: out[b][i] = (x, y, angle), before the
+// device-side jitter of structured_init.
+extern "C" int ref_build_portfolio(int n, int chains, double L, const double* seed_xya, int structured,
+                                   double* out) {
+    std::vector<P> seed((size_t)n), h;
+    for (int i = 0; i < n; ++i) seed[(size_t)i] = P{seed_xya[3 * i], seed_xya[3 * i + 1], seed_xya[3 * i + 2]};
+    build_portfolio(n, chains, L, seed, structured, 0ull, h);
+    for (size_t k = 0; k < h.size(); ++k) {
+        out[3 * k] = h[k].x;
+        out[3 * k + 1] = h[k].y;
+        out[3 * k + 2] = h[k].a;
+    }
+    return (int)h.size();
+}

@@ -30,9 +30,11 @@
 //   * the move set is the reference's: step adaptation with the cooling
 //     cycle and kicks of overlapped replicas always, collective moves
 //     always for packing and under SEED_COLLECTIVE for seeded;
-//   * the angle proposal width is 2.5 x the move width (PACK_ROTATION and
-//     SEED_STRUCTURED are validated and reported, like PACK_ROTATION in the
-//     reference, but do not change the search).
+//   * chains start from the structured portfolio (sqs_portfolio, the
+//     reference's build_portfolio and structured_init), always for packing
+//     and under SEED_STRUCTURED for seeded;
+//   * the angle proposal width is 2.5 x the move width (PACK_ROTATION is
+//     validated and reported but, as in the reference, not used).
 // "target_L" is the FP64 dilation-certified side of the best state and "q"
 // that state (the packing the interval certifier accepted); when no ladder
 // finds a certified state the seed is reported with its side, as the
@@ -127,6 +129,7 @@ int main(int argc, char** argv) {
     const int max_chains = (int)env("MAX_CHAINS", 768, 8, 4096);
     const int polish = 200;
     const int collective = 1;  // packing always mixes collective moves in (packing.cu:525)
+    const int structured = 1;  // and always starts from the portfolio (packing.cu:806, 821)
 #endif
     const unsigned long long rng_seed = std::strtoull(argv[5], nullptr, 10);
 
@@ -150,6 +153,11 @@ int main(int argc, char** argv) {
     const int per_epoch = std::max(1, (int)std::lround((double)steps / (double)n));
     const int ladders = chains / 8;
 
+    // every chain's start: the structured portfolio (the seed on every chain
+    // when SEED_STRUCTURED=0); ladder k's 8 chains are job k's replicas
+    std::vector<double> starts(3 * (size_t)n * (size_t)chains);
+    if (sqs_portfolio(n, L, seed.data(), chains, structured, rng_seed, 1, starts.data()) != SQS_OK)
+        return fail("portfolio");
     std::vector<sqs_job> jobs((size_t)ladders);
     std::vector<std::vector<double>> outs((size_t)ladders, std::vector<double>(3 * (size_t)n));
     std::vector<double*> ptrs((size_t)ladders);
@@ -170,6 +178,7 @@ int main(int argc, char** argv) {
         j.shrink = std::min(0.1, shrink / L);
         j.seed = rng_seed + 0x9E3779B97F4A7C15ull * (unsigned long long)k;
         j.xya = seed.data();
+        j.xya_rep = starts.data() + 3 * (size_t)n * 8 * (size_t)k;
         ptrs[(size_t)k] = outs[(size_t)k].data();
     }
     std::vector<sqs_job_result> res((size_t)ladders);

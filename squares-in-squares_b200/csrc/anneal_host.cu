@@ -83,6 +83,9 @@ int prepare_job(const sqs_job& J, int j, JobDev& d, JobMut& m, Plan& p, const Sh
     SQS_REQUIRE(J.polish_iters >= 0 && J.polish_iters <= 100000, "job %d: polish_iters out of range", j);
     SQS_REQUIRE(J.xya != nullptr, "job %d: null initial state", j);
     for (int i = 0; i < 3 * J.n; ++i) SQS_REQUIRE(std::isfinite(J.xya[i]), "job %d: non-finite initial coordinate", j);
+    if (J.xya_rep)
+        for (int64_t i = 0; i < 3 * (int64_t)J.n * J.replicas; ++i)
+            SQS_REQUIRE(std::isfinite(J.xya_rep[i]), "job %d: non-finite replica start", j);
     const bool tuned = shape && shape->cs > 0;
     SQS_REQUIRE(plan_job(J.n, J.replicas, J.L0, tuned ? shape->cell : kCellSide, tuned ? shape->cs : 1, p),
                 "job %d: n=%d with %d replicas does not fit a cluster of <= 16 CTAs", j, J.n, J.replicas);
@@ -120,10 +123,12 @@ int prepare_job(const sqs_job& J, int j, JobDev& d, JobMut& m, Plan& p, const Sh
 int64_t job_pos_elems(const sqs_job& J) { return (int64_t)J.replicas * J.n + 2 * (int64_t)J.n; }
 
 void init_replicas(const sqs_job& J, float4* dst) {
-    for (int r = 0; r < J.replicas; ++r)
+    for (int r = 0; r < J.replicas; ++r) {
+        const double* src = J.xya_rep ? J.xya_rep + 3 * (size_t)r * J.n : J.xya;
         for (int i = 0; i < J.n; ++i)
             dst[(int64_t)r * J.n + i] =
-                make_float4((float)J.xya[3 * i], (float)J.xya[3 * i + 1], (float)wrap_quarter(J.xya[3 * i + 2]), 0.f);
+                make_float4((float)src[3 * i], (float)src[3 * i + 1], (float)wrap_quarter(src[3 * i + 2]), 0.f);
+    }
 }
 
 void fill_result(const sqs_job& J, const JobDev& d, const JobMut& m, float dev_ms, sqs_job_result& o) {

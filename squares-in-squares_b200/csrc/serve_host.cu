@@ -45,7 +45,7 @@ struct SJob {
     int slot = -1;
     bool cancel = false;
     sqs_job job{};
-    std::vector<double> xya;
+    std::vector<double> xya, xya_rep;  // copies of the initial state(s)
     JobDev jd{};
     JobMut jm{};
     Plan plan{};
@@ -198,6 +198,10 @@ extern "C" int sqs_server_submit(sqs_server* s, const sqs_job* job, int64_t* id)
     if (int r = resolve_job(s->ctx, *job, 0, j.job, shape)) return r;
     j.xya.assign(job->xya, job->xya + 3 * (size_t)std::max(0, job->n));
     j.job.xya = j.xya.data();
+    if (job->xya_rep) {
+        j.xya_rep.assign(job->xya_rep, job->xya_rep + 3 * (size_t)std::max(0, job->n) * (size_t)std::max(0, job->replicas));
+        j.job.xya_rep = j.xya_rep.data();
+    }
     if (int r = prepare_job(j.job, 0, j.jd, j.jm, j.plan, &shape)) return r;
     SQS_REQUIRE(job_bytes(j.job) <= s->arena_bytes, "job state (%zu bytes) exceeds the server's HBM budget",
                 job_bytes(j.job));
@@ -206,7 +210,8 @@ extern "C" int sqs_server_submit(sqs_server* s, const sqs_job* job, int64_t* id)
     const int64_t key = j.id;
     s->jobs.emplace(key, std::move(j));
     SJob& stored = s->jobs[key];
-    stored.job.xya = stored.xya.data();  // the vector moved with the record
+    stored.job.xya = stored.xya.data();  // the vectors moved with the record
+    if (stored.job.xya_rep) stored.job.xya_rep = stored.xya_rep.data();
     if (stored.jm.status != kRunning) {   // zero-sweep job: nothing to anneal
         stored.state = kDone;
         fill_result(stored.job, stored.jd, stored.jm, 0.f, stored.res);

@@ -41,7 +41,7 @@ class Job(C.Structure):
     _fields_ = [("n", C.c_int32), ("replicas", C.c_int32), ("sweeps", C.c_int32), ("exchange_every", C.c_int32),
                 ("polish_iters", C.c_int32), ("flags", C.c_int32), ("L0", C.c_double), ("tmin", C.c_double),
                 ("tmax", C.c_double), ("sigma_xy", C.c_double), ("sigma_a", C.c_double), ("shrink", C.c_double),
-                ("seed", C.c_uint64), ("xya", C.POINTER(C.c_double))]
+                ("seed", C.c_uint64), ("xya", C.POINTER(C.c_double)), ("xya_rep", C.POINTER(C.c_double))]
 
 
 class JobResult(C.Structure):
@@ -108,6 +108,8 @@ SIGNATURES: dict[str, tuple] = {
     "sqs_server_step": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "sqs_server_poll": (C.c_int, [_vp, C.c_int64, C.POINTER(JobResult), C.POINTER(C.c_double)]),
     "sqs_server_cancel": (C.c_int, [_vp, C.c_int64]),
+    "sqs_portfolio": (C.c_int, [C.c_int, C.c_double, C.POINTER(C.c_double), C.c_int, C.c_int, C.c_uint64, C.c_int,
+                                C.POINTER(C.c_double)]),
     "sqs_polish_batch": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_double), C.c_int,
                                    C.POINTER(C.c_double), C.POINTER(PolishResult)]),
     "sqs_autotune": (C.c_int, [_vp, C.POINTER(Job), C.c_int, C.POINTER(Tuning)]),

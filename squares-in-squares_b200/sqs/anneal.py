@@ -41,11 +41,14 @@ class AnnealJob:
     kick: bool = False              # kick and reseed of overlapped replicas at exchange rounds (SQS_JOB_KICK)
     cluster: int = 0                # pinned cluster size (0: default / tuned)
     cell_index: int = 0             # pinned cell side index (0: 1.59, 1: 1.75, 2: 1.95, 3: 2.2)
+    xya_rep: np.ndarray | None = None  # (replicas, n, 3) per-replica starts, e.g. from portfolio()
     n: int = field(init=False)
 
     def __post_init__(self):
         self.xya = np.ascontiguousarray(self.xya, dtype=np.float64).reshape(-1, 3)
         self.n = self.xya.shape[0]
+        if self.xya_rep is not None:
+            self.xya_rep = np.ascontiguousarray(self.xya_rep, dtype=np.float64).reshape(self.replicas, self.n, 3)
 
 
 def _flags(j: AnnealJob) -> int:
@@ -58,7 +61,8 @@ def _cjob(j: AnnealJob) -> N.Job:
     return N.Job(n=j.n, replicas=j.replicas, sweeps=j.sweeps, exchange_every=j.exchange_every,
                  polish_iters=j.polish_iters, flags=_flags(j), L0=j.L0, tmin=j.tmin, tmax=j.tmax, sigma_xy=j.sigma_xy,
                  sigma_a=j.sigma_a, shrink=j.shrink, seed=j.seed & 0xFFFFFFFFFFFFFFFF,
-                 xya=j.xya.ctypes.data_as(C.POINTER(C.c_double)))
+                 xya=j.xya.ctypes.data_as(C.POINTER(C.c_double)),
+                 xya_rep=j.xya_rep.ctypes.data_as(C.POINTER(C.c_double)) if j.xya_rep is not None else None)
 
 
 def anneal_batch(jobs: list[AnnealJob], *, ctx: N.Context | None = None, slice_sweeps: int = 0) -> list[dict]:
@@ -116,3 +120,17 @@ def jittered_grid(n: int, jitter: float = 0.05, angle_hi: float = 0.1, seed: int
     i = np.arange(n)
     xy = np.stack([i % w + 0.5, i // w + 0.5], axis=1) + rng.uniform(-jitter, jitter, (n, 2))
     return np.concatenate([xy, rng.uniform(0.0, angle_hi, (n, 1))], axis=1), float(w)
+
+
+def portfolio(seed_xya, L: float, chains: int, *, structured: bool = True, seed: int = 0,
+              jitter: bool = True) -> np.ndarray:
+    """Initial states of `chains` search chains, (chains, n, 3): the
+    reference's structured portfolio (sqs_portfolio; seeded.cu:233-451).
+    Chains 8k .. 8k + 7 are the replicas of the k-th 8-replica job."""
+    seed_xya = np.ascontiguousarray(seed_xya, dtype=np.float64).reshape(-1, 3)
+    n = seed_xya.shape[0]
+    out = np.zeros((chains, n, 3))
+    N.check(N.lib().sqs_portfolio(n, float(L), seed_xya.ctypes.data_as(C.POINTER(C.c_double)), chains,
+                                  int(structured), seed & 0xFFFFFFFFFFFFFFFF, int(jitter),
+                                  out.ctypes.data_as(C.POINTER(C.c_double))))
+    return out

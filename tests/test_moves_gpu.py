@@ -61,3 +61,28 @@ def test_adaptation_steers_acceptance(ctx):
     rf = fixed["accepted"] / fixed["proposals"]
     ra = adapt["accepted"] / adapt["proposals"]
     assert ra > 10 * rf and 0.005 < ra < 0.6, (rf, ra)
+
+
+def test_replicas_start_from_a_portfolio(ctx):
+    """Per-replica starts (sqs_job.xya_rep) from the structured portfolio: the
+    job's result is the same alone, sliced and served, and differs from
+    starting every replica at the seed."""
+    from sqs.anneal import anneal_batch, portfolio
+    from sqs.serve import Server
+    base = _job(n=30, seed=21, sweeps=150, replicas=8)
+    starts = portfolio(base.xya, base.L0, 8, seed=3)
+    job = replace(base, xya_rep=starts)
+    alone = anneal_batch([job], ctx=ctx)[0]
+    plain = anneal_batch([base], ctx=ctx)[0]
+    assert alone["status"] == 0
+    assert alone["q"] != plain["q"] or alone["accepted"] != plain["accepted"]
+    sliced = anneal_batch([job], ctx=ctx, slice_sweeps=30)[0]
+    with Server(ctx, hbm_bytes=64 << 20, max_active=2, slice_sweeps=30) as srv:
+        jid = srv.submit(job)
+        for _ in range(100):
+            if srv.step() == 0:
+                break
+        served = srv.poll(jid)
+    for k in KEYS:
+        assert sliced[k] == alone[k], ("sliced", k)
+        assert served[k] == alone[k], ("served", k)
