@@ -13,6 +13,8 @@ Outputs (committed):
   sat_pairs.json      random unit-square pairs with the reference's FP64
                       pair() energy and gradient (seeded.cu:92) and boundary()
                       (seeded.cu:96) values, computed by oracle/_ref.
+  optimizer.json      the rows of the reference's n = 5 construction
+                      (squares.optimizer.tilted_five, optimizer.py:13-35).
   candidates.json     the reference's saved search outputs (cuda/results/
                       raw{5,10,11,17,50}.json: n and the raw state q) and the
                       test inputs of tests/test_cuda_demo.py, with the result
@@ -159,6 +161,7 @@ def main():
             c["certify_q"] = dict(L=str(demo.certify(c["n"], rows)), side=side, dilation=dil)
         except ValueError as e:
             c["certify_q"] = dict(error=str(e))
+    (HERE / "optimizer.json").write_text(json.dumps(dict(tilted_five=tilted_five()), indent=1) + "\n")
     (HERE / "candidates.json").write_text(json.dumps(cands, indent=1).replace("NaN", "\"nan\"") + "\n")
     print(f"{len(kept)} certifier cases, {len(recs)} SAT pairs, {len(cands)} candidates")
 
