@@ -524,6 +524,61 @@ def bench_batched(ctx, sweeps: int = 50, instances: int = 512):
                 squares=int(sum(j.n for j in jobs)) * 32, certified=sum(r["certified"] for r in res))
 
 
+def bench_search(cases: str = "10:200:64:64,50:60:64:64,200:10:48:64,50:600:64:64,200:100:48:64"):
+    """The search programs head to head on the same B200: this library's
+    `seeded` drop-in and the reference's own `seeded` (built for sm_100a from
+    its sources into oracle/_ref), same seed file (grid centres + U(+-0.05)
+    jitter, angles U[0, 0.1), seed 42, side ceil(sqrt n)), epochs, steps,
+    chains and environment (SEED_AUTOTUNE=0 so both keep the chain count).
+    Reports each program's own seconds, wall time, proposals and the side the
+    official gate certifies for its raw result (demo.certified_candidate)."""
+    import subprocess
+    import tempfile
+
+    from sqs.anneal import jittered_grid
+    from sqs.demo import certified_candidate
+
+    progs = {"sqs": ROOT / "squares-in-squares_b200" / "bin" / "seeded",
+             "reference": ROOT / "oracle" / "_ref" / "seeded"}
+    env = dict(os.environ, SEED_AUTOTUNE="0")
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for case in cases.split(","):
+            n, epochs, steps, chains = (int(v) for v in case.split(":"))
+            xya, L = jittered_grid(n, seed=42)
+            seed = Path(tmp) / f"seed{n}.txt"
+            seed.write_text(f"{n} {L}\n" + "".join(f"{x:.17g} {y:.17g} {a:.17g}\n" for x, y, a in xya))
+            row = {}
+            for name, exe in progs.items():
+                if not exe.exists():
+                    row[name] = dict(unavailable=f"{exe.name} not built")
+                    continue
+                res = Path(tmp) / f"{name}{n}.json"
+                # a one-step warm-up run first, so neither program's wall time
+                # holds the first load of its binary and libraries
+                subprocess.run([str(exe), str(seed), "1", "1", "8", "7", str(res)], capture_output=True, env=env,
+                               timeout=300)
+                t0 = time.perf_counter()
+                r = subprocess.run([str(exe), str(seed), str(epochs), str(steps), str(chains), "7", str(res)],
+                                   capture_output=True, text=True, env=env, timeout=600)
+                wall = time.perf_counter() - t0
+                if r.returncode != 0:
+                    row[name] = dict(exit=r.returncode, stderr=r.stderr[-300:])
+                    continue
+                raw = json.loads(res.read_text())
+                try:
+                    _, side, dil = certified_candidate(raw)
+                except ValueError as e:
+                    side, dil = None, str(e)
+                row[name] = dict(seconds=raw["seconds"], wall_seconds=wall, proposals=raw["proposals"],
+                                 proposals_per_s=raw["proposals"] / max(raw["seconds"], 1e-9),
+                                 target_L=raw["target_L"], certified_L=side, dilation=dil, chains=raw["chains"])
+            if "seconds" in row.get("sqs", {}) and "seconds" in row.get("reference", {}):
+                row["wall_speedup"] = row["reference"]["wall_seconds"] / row["sqs"]["wall_seconds"]
+            out[f"n={n} epochs={epochs} steps={steps} chains={chains}"] = row
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -535,7 +590,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the certifier / served / plain-PT / batched sections")
-    ap.add_argument("--section", choices=("certify", "served", "plain_pt", "batched"),
+    ap.add_argument("--section", choices=("certify", "served", "plain_pt", "batched", "search"),
                     help="run only this extra section (for profiling) and print its dict")
     ap.add_argument("--batched-instances", type=int, default=512)
     ap.add_argument("--batched-sweeps", type=int, default=50)
@@ -548,7 +603,8 @@ def main():
             fn = dict(certify=lambda: bench_certify(ctx, args.cpu_seconds),
                       served=lambda: bench_served_sweep(ctx, args.served_rates),
                       plain_pt=lambda: bench_plain_pt(ctx),
-                      batched=lambda: bench_batched(ctx, args.batched_sweeps, args.batched_instances))[args.section]
+                      batched=lambda: bench_batched(ctx, args.batched_sweeps, args.batched_instances),
+                      search=lambda: bench_search())[args.section]
             print(json.dumps({args.section: fn()}), flush=True)
         return
     if args.warmup < 3:

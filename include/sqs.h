@@ -249,9 +249,10 @@ int sqs_portfolio(int n, double L, const double* seed_xya, int chains, int struc
  * xya), translated so the bounding box of the certifying dilation starts at
  * the origin.  The incumbent is the input's FP64 dilation-certified side
  * (seeded.cu:175-226: every close pair separated once the centres are
- * scaled by lambda <= 1.008); an input too overlapped for that first has
- * its centres spread by lambda (at most 1.5x) and descends its overlap
- * energy at its bounding-box side scaled alike.  Each attempt
+ * scaled by lambda <= 1.008); an input too overlapped for that first
+ * descends its overlap energy inside its own bounding box (half the budget)
+ * and, if overlaps remain, with its centres spread by lambda (at most 1.5x)
+ * in a box scaled alike.  Each attempt
  * compresses the incumbent by 1 - delta, descends the squared-penetration
  * energy (pair_cached_smooth, seeded.cu:67-90) with a backtracking line
  * search, and keeps the result when its certified side is smaller; delta

@@ -20,7 +20,8 @@
 //   * a reference step is one proposal per chain, so a job runs
 //     ceil(epochs * steps / n) sweeps of n proposals per replica, and
 //     exchanges replicas once per epoch's worth of sweeps;
-//   * the absolute shrink step becomes a relative one (shrink / L);
+//   * the absolute shrink step becomes a relative one (shrink / L), times
+//     the multiplier of the ladder's place among the reference's 8 targets;
 //   * chains = 0 (or *_AUTOTUNE=1 with chains >= 64) takes one ladder per SM,
 //     capped at *_MAX_CHAINS, as the reference sizes chains to a wave;
 //     *_AUTOTUNE=1 also lets the launch autotuner pick each job's shape;
@@ -82,6 +83,11 @@ static double env(const char* suffix, double def, double lo, double hi) {
     }
     return v;
 }
+
+// The reference shrinks the chains of a ladder toward 8 different targets,
+// L - shrink * {0.02, 0.1, 0.4, 1, 2.5, 5, 10, 20} (seeded.cu:478-481,
+// 929-933); here ladder k's job shrinks by the k % 8-th of those steps.
+static const double kShrinkMults[8] = {0.02, 0.1, 0.4, 1.0, 2.5, 5.0, 10.0, 20.0};
 
 static int fail(const char* what) {
     std::cerr << kName << ": " << what << ": " << sqs_last_error() << "\n";
@@ -175,7 +181,7 @@ int main(int argc, char** argv) {
         j.tmax = tmax;
         j.sigma_xy = mv;
         j.sigma_a = std::min(1.0, 2.5 * mv);
-        j.shrink = std::min(0.1, shrink / L);
+        j.shrink = std::min(0.1, shrink * kShrinkMults[k % 8] / L);
         j.seed = rng_seed + 0x9E3779B97F4A7C15ull * (unsigned long long)k;
         j.xya = seed.data();
         j.xya_rep = starts.data() + 3 * (size_t)n * 8 * (size_t)k;

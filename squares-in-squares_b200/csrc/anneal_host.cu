@@ -55,6 +55,8 @@ static double wrap_quarter(double a) {
 }  // namespace ann
 }  // namespace sqs
 
+extern "C" int sqs_polish_batch(sqs_ctx* ctx, int count, const int32_t* n_of, const double* xya, int iters,
+                                double* xya_out, sqs_polish_result* out);
 extern "C" int sqs_certify_batch(sqs_ctx* ctx, int count, const int32_t* n_of, const int64_t* row_start,
                                  const int32_t* square_id, const char* text, const int64_t* lit_off, int flags,
                                  sqs_verdict* out);
@@ -425,6 +427,56 @@ int resolve_job(sqs_ctx* ctx, const sqs_job& job, int mode, sqs_job& eff, Shape&
     return SQS_OK;
 }
 
+void add_rescue(std::vector<Rescue>& out, const sqs_job& J, const JobDev& d, JobMut& m, const float4* d_pos,
+                double* best) {
+    if (m.status != kFinished || m.best_L < 1e29 || J.polish_iters <= 0 || J.sweeps <= 0) return;
+    int cold = 0;
+    for (int r = 0; r < J.replicas; ++r)
+        if (m.perm[r] == 0) cold = r;
+    out.push_back(Rescue{J.n, J.polish_iters, d_pos + d.pos_off + (int64_t)cold * J.n, best, &m});
+}
+
+int rescue_uncertified(sqs_ctx* ctx, const std::vector<Rescue>& items) {
+    if (items.empty()) return SQS_OK;
+    std::vector<std::vector<float4>> raw(items.size());
+    for (size_t k = 0; k < items.size(); ++k) {
+        raw[k].resize((size_t)items[k].n);
+        SQS_CUDA(cudaMemcpyAsync(raw[k].data(), items[k].d_state, sizeof(float4) * raw[k].size(),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    SQS_CUDA(cudaStreamSynchronize(ctx->stream));
+    // one polish batch per distinct budget, so a job's result never depends
+    // on what it was batched with
+    std::map<int, std::vector<size_t>> by_iters;
+    for (size_t k = 0; k < items.size(); ++k) by_iters[items[k].iters].push_back(k);
+    for (auto& kv : by_iters) {
+        std::vector<int32_t> n_of;
+        std::vector<double> xya, out;
+        for (size_t k : kv.second) {
+            n_of.push_back(items[k].n);
+            for (const float4& p : raw[k]) {
+                xya.push_back(p.x);
+                xya.push_back(p.y);
+                xya.push_back(p.z);
+            }
+        }
+        out.resize(xya.size());
+        std::vector<sqs_polish_result> res(kv.second.size());
+        if (int r = sqs_polish_batch(ctx, (int)n_of.size(), n_of.data(), xya.data(), kv.first, out.data(), res.data()))
+            return r;
+        size_t row = 0;
+        for (size_t q = 0; q < kv.second.size(); ++q) {
+            const Rescue& it = items[kv.second[q]];
+            if (res[q].L_out < 1e29) {
+                std::memcpy(it.best, out.data() + 3 * row, sizeof(double) * 3 * (size_t)it.n);
+                it.m->best_L = res[q].L_out;
+            }
+            row += (size_t)it.n;
+        }
+    }
+    return SQS_OK;
+}
+
 int certify_states(sqs_ctx* ctx, const std::vector<int>& ns, const std::vector<const double*>& best,
                    const std::vector<sqs_job_result*>& out, const std::vector<double*>& xya_out) {
     static const double ladder[5] = {1 + 1e-10, 1 + 1e-9, 1 + 1e-8, 1 + 1e-7, 1 + 1e-6};
@@ -610,6 +662,13 @@ extern "C" int sqs_anneal_batch(sqs_ctx* ctx, const sqs_job* jobs, int njobs, in
     float dev_ms = 0.f;
     SQS_CUDA(cudaEventElapsedTime(&dev_ms, e0, e1));
 
+    // jobs that never certified a state: rescue from the coldest replica
+    {
+        std::vector<Rescue> rs;
+        for (int j = 0; j < njobs; ++j)
+            add_rescue(rs, eff[(size_t)j], jd[(size_t)j], jm[(size_t)j], d_pos, hbest.data() + jd[(size_t)j].best_off);
+        if (int r = rescue_uncertified(ctx, rs)) return r;
+    }
     // certify every best state
     std::vector<int> ns;
     std::vector<const double*> bptr;

@@ -60,6 +60,22 @@ int64_t job_pos_elems(const sqs_job& J);
 // Every replica starts from the job's initial state (angles wrapped to [0, pi/2)).
 void init_replicas(const sqs_job& J, float4* dst);
 void fill_result(const sqs_job& J, const JobDev& d, const JobMut& m, float dev_ms, sqs_job_result& o);
+// A finished job that certified no state during its anneal would return
+// nothing: its coldest replica's final state is polished from scratch
+// instead (the sqs_polish_batch path: overlaps resolved in a spread box,
+// then the compress-and-descend attempts, `iters` gradient steps), and a
+// certified side found that way becomes the job's best (*m, best[3n]).
+struct Rescue {
+    int n, iters;
+    const float4* d_state;  // the replica's final (x, y, angle, -) on the device
+    double* best;           // host, n x 3
+    JobMut* m;              // host copy of the job's record
+};
+int rescue_uncertified(sqs_ctx* ctx, const std::vector<Rescue>& items);
+// The rescue candidates among finished jobs: annealed (sweeps > 0), best
+// side still unset, polish requested.
+void add_rescue(std::vector<Rescue>& out, const sqs_job& J, const JobDev& d, JobMut& m, const float4* d_pos,
+                double* best);
 int certify_states(sqs_ctx* ctx, const std::vector<int>& ns, const std::vector<const double*>& best,
                    const std::vector<sqs_job_result*>& out, const std::vector<double*>& xya_out);
 

@@ -271,8 +271,9 @@ __global__ void __launch_bounds__(kPT) polish_kernel(const int32_t* __restrict__
 // Standalone polish of arbitrary states (state k: n_of[k] rows at
 // xya + 3 * row0[k], polished in place).  The input's dilation-certified
 // side is the incumbent; an input too overlapped to certify (dilation above
-// 1.008) first has its centres spread by that dilation (at most 1.5x) and
-// descends the energy at its bounding-box side scaled alike.
+// 1.008) first descends its energy inside its own bounding box and, if
+// overlaps remain, has its centres spread by that dilation (at most 1.5x)
+// and descends in a box scaled alike.
 // res[k] = {L_in, L_out, iterations used}.
 __global__ void __launch_bounds__(kPT) polish_states_kernel(const int32_t* __restrict__ n_of,
                                                             const int64_t* __restrict__ row0, int iters,
@@ -289,7 +290,7 @@ __global__ void __launch_bounds__(kPT) polish_states_kernel(const int32_t* __res
     int budget = iters;
     double lam = 0, x0 = 0, y0 = 0;
     double Lb = cert_side_all(n, B.q0, B.cs, red, lam, x0, y0);
-    const double L_in = Lb;
+    const double L_in = Lb, lam_in = lam;
     if (Lb >= 1e29) {
         // bounding box of the input, translated to the origin, as the side
         double a0 = 1e300, a1 = -1e300, b0 = 1e300, b1 = -1e300;
@@ -304,14 +305,29 @@ __global__ void __launch_bounds__(kPT) polish_states_kernel(const int32_t* __res
         a1 = block_max(a1, red);
         b0 = -block_max(-b0, red);
         b1 = block_max(b1, red);
-        // spread the centres by the dilation that would separate the close
-        // pairs (at most 1.5x) so the descent has room to remove the overlaps
-        const double f = fmin(fmax(lam, 1.0), 1.5);
-        for (int i = threadIdx.x; i < n; i += kPT)
-            B.q0[i] = make_double3((B.q0[i].x - a0) * f, (B.q0[i].y - b0) * f, B.q0[i].z);
+        const double side = fmax(a1 - a0, b1 - b0);
+        for (int i = threadIdx.x; i < n; i += kPT) {
+            B.sv[i] = make_double3(B.q0[i].x - a0, B.q0[i].y - b0, B.q0[i].z);  // the input, at the origin
+            B.q0[i] = B.sv[i];
+        }
         __syncthreads();
-        descend(n, B, fmax(a1 - a0, b1 - b0) * f, &budget, red);
+        // first remove the overlaps inside the input's own bounding box (half
+        // the budget); where they do not vanish there, spread the input's
+        // centres by the dilation that would separate its close pairs (at
+        // most 1.5x) and descend in a box scaled alike
+        int half = budget / 2;
+        budget -= half;
+        descend(n, B, side, &half, red);
+        budget += half;
         Lb = cert_side_all(n, B.q0, B.cs, red, lam, x0, y0);
+        if (Lb >= 1e29) {
+            const double f = fmin(fmax(lam_in, 1.0), 1.5);
+            for (int i = threadIdx.x; i < n; i += kPT)
+                B.q0[i] = make_double3(B.sv[i].x * f, B.sv[i].y * f, B.sv[i].z);
+            __syncthreads();
+            descend(n, B, side * f, &budget, red);
+            Lb = cert_side_all(n, B.q0, B.cs, red, lam, x0, y0);
+        }
     }
     if (Lb < 1e29) {
         for (int i = threadIdx.x; i < n; i += kPT)

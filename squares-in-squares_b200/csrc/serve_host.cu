@@ -285,6 +285,15 @@ extern "C" int sqs_server_step(sqs_server* s, int* in_flight) {
         SQS_CUDA(cudaMemcpyAsync(s->h_jm.data(), s->d_jm, sizeof(JobMut) * (size_t)s->max_active,
                                  cudaMemcpyDeviceToHost, s->ctx->stream));
         SQS_CUDA(cudaStreamSynchronize(s->ctx->stream));
+        {
+            std::vector<Rescue> rs;
+            for (size_t q = 0; q < fin.size(); ++q) {
+                SJob& j = s->jobs[s->slot_job[(size_t)fin[q]]];
+                if (!j.cancel)
+                    add_rescue(rs, j.job, j.jd, s->h_jm[(size_t)fin[q]], (const float4*)s->arena, best[q].data());
+            }
+            if (int r = rescue_uncertified(s->ctx, rs)) return r;
+        }
         std::vector<int> ns;
         std::vector<const double*> bptr;
         std::vector<sqs_job_result*> optr;

@@ -94,3 +94,30 @@ def test_zero_sweeps_returns_input_unimproved(ctx):
     from sqs.anneal import anneal_batch
     r = anneal_batch([plain_job(sweeps=0)], ctx=ctx)[0]
     assert r["status"] == 0 and not r["certified"] and r["proposals"] == 0
+
+
+def test_job_without_a_certified_state_is_rescued(ctx, oracle):
+    """Two sweeps at a tiny temperature leave the jittered (overlapping) grid
+    uncertified; the coldest replica's final state is then polished from
+    scratch into a certified packing -- identically alone, in a batch and
+    served -- while a job that asks for no polish returns none."""
+    from dataclasses import replace
+
+    from sqs.anneal import anneal_batch
+    from sqs.serve import Server
+    job = plain_job(n=30, seed=8, sweeps=2, replicas=8, exchange_every=1, tmin=1e-11, tmax=1e-10,
+                    polish_iters=400)
+    r = anneal_batch([job], ctx=ctx)[0]
+    assert r["status"] == 0 and r["certified"], r["reason"]
+    ok, L, reason, _ = oracle.certify(30, r["rows"])
+    assert ok and L == r["L"], reason
+    none = anneal_batch([replace(job, polish_iters=0)], ctx=ctx)[0]
+    assert not none["certified"]
+    mixed = anneal_batch([plain_job(n=12, seed=1, sweeps=50), job], ctx=ctx)[1]
+    with Server(ctx, hbm_bytes=32 << 20, max_active=2, slice_sweeps=1) as srv:
+        jid = srv.submit(job)
+        while srv.step():
+            pass
+        served = srv.poll(jid)
+    for k in KEYS:
+        assert mixed[k] == r[k] and served[k] == r[k], k
