@@ -279,31 +279,36 @@ __device__ long long block_sum_ll(long long v, long long* red) {
     return t;
 }
 
-// Full fixed-point energy with one thread per square.
+// Full fixed-point energy by the whole CTA.  Work item w is square w / 9
+// against the squares listed in cell w % 9 of its 3 x 3 block (each pair
+// counted from its lower index), so a small replica still spreads over
+// many threads.
 __device__ long long full_energy_cta(const Rep& R, int n, const Grid& g, float L, long long* red) {
     long long e = 0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    for (int w = threadIdx.x; w < 9 * n; w += blockDim.x) {
+        const int i = w / 9, c = w - 9 * i;
         const float4 P = R.sq[i];
-        e += qe(wall_e(P.x, P.y, P.z, P.w, L));
-        const int cx = g.cx(P.x), cy = g.cx(P.y);
-        for (int dy = -1; dy <= 1; ++dy) {
-            for (int dxc = -1; dxc <= 1; ++dxc) {
-                const int x = cx + dxc, y = cy + dy;
-                if (x < 0 || x >= g.G || y < 0 || y >= g.G) continue;
-                const int cell = y * g.G + x;
-                const int m = R.cnt[cell];
-                for (int k = 0; k < m; ++k) {
-                    const int j = R.slot[cell * kCellK + k];
-                    if (j <= i) continue;
-                    const float4 Q = R.sq[j];
-                    const float dx = Q.x - P.x, dy2 = Q.y - P.y;
-                    if (dx * dx + dy2 * dy2 < kPairCut2) e += qe(sat_pair_energy(dx, dy2, P.z, P.w, Q.z, Q.w));
-                }
-            }
+        if (c == 0) e += qe(wall_e(P.x, P.y, P.z, P.w, L));
+        const int x = g.cx(P.x) + c % 3 - 1, y = g.cx(P.y) + c / 3 - 1;
+        if (x < 0 || x >= g.G || y < 0 || y >= g.G) continue;
+        const int cell = y * g.G + x, m = R.cnt[cell];
+        for (int k = 0; k < m; ++k) {
+            const int j = R.slot[cell * kCellK + k];
+            if (j <= i) continue;
+            const float4 Q = R.sq[j];
+            const float dx = Q.x - P.x, dy2 = Q.y - P.y;
+            if (dx * dx + dy2 * dy2 < kPairCut2) e += qe(sat_pair_energy(dx, dy2, P.z, P.w, Q.z, Q.w));
         }
     }
     return block_sum_ll(e, red);
 }
+
+// Quench gradient sums: 32-bit integers in units of 2^-20.  A square's 3 x 3
+// block lists at most 9 x 12 partners, each term below 5.2 (and the wall
+// term below 1), so a sum stays below 6e8 < 2^31; integer atomics make the
+// sums independent of the order of the terms.
+constexpr float kQScale = 1048576.0f;
+__device__ __forceinline__ int qg(float v) { return __float2int_rn(v * kQScale); }
 
 // The quench of the coldest replica by the whole CTA, one thread per square:
 // Jacobi gradient descent on the overlap energy with a backtracking step
@@ -315,37 +320,53 @@ __device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters
                                 long long E, long long* red) {
     float alpha = 0.05f;
     int stall = 0;  // consecutive accepted steps that gained less than 0.1%
+    int4* acc = reinterpret_cast<int4*>(grad);  // the gradient buffer holds the integer sums first
     for (int it = 0; it < iters && E > 0; ++it) {
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            acc[i] = make_int4(0, 0, 0, 0);
+            saved[i] = make_float4(R.sq[i].x, R.sq[i].y, R.ang[i], 0.f);
+        }
+        __syncthreads();
+        // work item w: square w / 9 against cell w % 9 of its block
+        for (int w = threadIdx.x; w < 9 * n; w += blockDim.x) {
+            const int i = w / 9, c = w - 9 * i;
             const float4 P = R.sq[i];
-            float wx = 0.f, wy = 0.f, wa = 0.f;
-            wall_energy_grad(P.x, P.y, P.z, P.w, L, wx, wy, wa);
-            long long qx = qe(wx), qy = qe(wy), qa = qe(wa);
-            const int cx = g.cx(P.x), cy = g.cx(P.y);
-            for (int dy = -1; dy <= 1; ++dy) {
-                for (int dxc = -1; dxc <= 1; ++dxc) {
-                    const int x = cx + dxc, y = cy + dy;
-                    if (x < 0 || x >= g.G || y < 0 || y >= g.G) continue;
-                    const int cell = y * g.G + x;
-                    const int m = R.cnt[cell];
-                    for (int k = 0; k < m; ++k) {
-                        const int j = R.slot[cell * kCellK + k];
-                        if (j == i) continue;
-                        const float4 Q = R.sq[j];
-                        const float ex = Q.x - P.x, ey = Q.y - P.y;
-                        if (ex * ex + ey * ey >= kPairCut2) continue;
-                        PairGrad pg;
-                        if (sat_pair_grad(ex, ey, P.z, P.w, Q.z, Q.w, pg)) {
-                            qx += qe(pg.px);
-                            qy += qe(pg.py);
-                            qa += qe(pg.pa);
-                        }
+            int ax = 0, ay = 0, aa = 0;
+            if (c == 0) {
+                float wx = 0.f, wy = 0.f, wa = 0.f;
+                wall_energy_grad(P.x, P.y, P.z, P.w, L, wx, wy, wa);
+                ax = qg(wx);
+                ay = qg(wy);
+                aa = qg(wa);
+            }
+            const int x = g.cx(P.x) + c % 3 - 1, y = g.cx(P.y) + c / 3 - 1;
+            if (x >= 0 && x < g.G && y >= 0 && y < g.G) {
+                const int cell = y * g.G + x, m = R.cnt[cell];
+                for (int k = 0; k < m; ++k) {
+                    const int j = R.slot[cell * kCellK + k];
+                    if (j == i) continue;
+                    const float4 Q = R.sq[j];
+                    const float ex = Q.x - P.x, ey = Q.y - P.y;
+                    if (ex * ex + ey * ey >= kPairCut2) continue;
+                    PairGrad pg;
+                    if (sat_pair_grad(ex, ey, P.z, P.w, Q.z, Q.w, pg)) {
+                        ax += qg(pg.px);
+                        ay += qg(pg.py);
+                        aa += qg(pg.pa);
                     }
                 }
             }
-            grad[i] = make_float4((float)qx * (1.0f / kEScale), (float)qy * (1.0f / kEScale),
-                                  (float)qa * (1.0f / kEScale), 0.f);
-            saved[i] = make_float4(P.x, P.y, R.ang[i], 0.f);
+            if (ax | ay | aa) {
+                atomicAdd(&acc[i].x, ax);
+                atomicAdd(&acc[i].y, ay);
+                atomicAdd(&acc[i].z, aa);
+            }
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const int4 a = acc[i];
+            grad[i] = make_float4((float)a.x * (1.0f / kQScale), (float)a.y * (1.0f / kQScale),
+                                  (float)a.z * (1.0f / kQScale), 0.f);
         }
         __syncthreads();
         // Trial steps move every coordinate by at most 0.1, so each partner
