@@ -23,6 +23,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -874,12 +875,11 @@ extern "C" int sqs_certify_batch(sqs_ctx* ctx, int count, const int32_t* n_of, c
     SQS_REQUIRE(n_of && row_start && text && lit_off && out, "null host pointer");
     if (int r = upload_consts(ctx->device)) return r;
 
+    // 1. the envelope of every packing (serial, cheap): verdict defaults, row
+    //    counts, and the square offsets of those that may certify
     std::vector<int32_t> pk_n((size_t)count, 0);
     std::vector<int64_t> pk_sq0((size_t)count, 0);
     std::vector<char> live((size_t)count, 0);
-    std::vector<int64_t> raw_off;
-    std::vector<int32_t> raw_len;
-    std::string rt_text;  // round-tripped literals, when requested
     const bool do_rt = (flags & SQS_CERT_ROUNDTRIP) != 0;
     int64_t S = 0;
     for (int p = 0; p < count; ++p) {
@@ -891,44 +891,97 @@ extern "C" int sqs_certify_batch(sqs_ctx* ctx, int count, const int32_t* n_of, c
         v.score = grid_score(n);
         const int64_t r0 = row_start[p], r1 = row_start[p + 1];
         SQS_REQUIRE(r1 >= r0, "packing %d: row_start not monotone", p);
-        const std::string N = std::to_string(n);
         if (r1 - r0 != n) {
+            const std::string N = std::to_string(n);
             put(v.reason, sizeof v.reason, "n=" + N + ": expected " + N + " rows, got " + std::to_string(r1 - r0));
-            continue;
-        }
-        std::vector<int64_t> row_of((size_t)n, -1);
-        bool bad = false;
-        for (int64_t r = r0; r < r1 && !bad; ++r) {
-            const int sid = square_id ? square_id[r] : (int)(r - r0);
-            if (sid < 0 || sid >= n || row_of[(size_t)sid] >= 0) bad = true;
-            else row_of[(size_t)sid] = r;
-        }
-        if (bad) {
-            put(v.reason, sizeof v.reason, "n=" + N + ": square_ids should be 0.." + std::to_string(n - 1));
             continue;
         }
         live[(size_t)p] = 1;
         pk_n[(size_t)p] = n;
         pk_sq0[(size_t)p] = S;
-        for (int i = 0; i < n; ++i) {
-            const int64_t r = row_of[(size_t)i];
-            for (int k = 0; k < 3; ++k) {
-                const int64_t a = lit_off[3 * r + k], b = lit_off[3 * r + k + 1];
-                SQS_REQUIRE(b >= a, "literal offsets not monotone at row %lld", (long long)r);
-                if (do_rt) {
-                    const std::string t = roundtrip(text + a, (size_t)(b - a));
-                    raw_off.push_back((int64_t)rt_text.size());
-                    raw_len.push_back((int32_t)t.size());
-                    rt_text += t;
-                } else {
-                    raw_off.push_back(a);
-                    raw_len.push_back((int32_t)std::min<int64_t>(b - a, 1 << 20));
-                }
-            }
-        }
         S += n;
     }
     SQS_REQUIRE(S < (1ll << 30), "%lld squares in one call (limit 2^30)", (long long)S);
+    // 2. square ids and literal slices (round-tripped when asked), host
+    //    threads over contiguous ranges of packings with equal square counts
+    std::vector<int64_t> raw_off((size_t)(3 * S));
+    std::vector<int32_t> raw_len((size_t)(3 * S));
+    const int nt = count >= 64 ? (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency())) : 1;
+    std::vector<int> p_lo((size_t)nt + 1, count);
+    {
+        int t = 0;
+        p_lo[0] = 0;
+        for (int p = 0; p < count && t + 1 < nt; ++p)
+            if (pk_sq0[(size_t)p] >= (S * (t + 1)) / nt) p_lo[(size_t)++t] = p;
+        for (++t; t <= nt; ++t) p_lo[(size_t)t] = count;
+    }
+    std::vector<std::string> rt((size_t)nt);  // round-tripped text of each thread's packings
+    std::vector<int64_t> bad_row((size_t)nt, -1);
+    auto slice = [&](int t) {
+        std::vector<int64_t> row_of;
+        for (int p = p_lo[(size_t)t]; p < p_lo[(size_t)t + 1]; ++p) {
+            if (!live[(size_t)p]) continue;
+            const int n = pk_n[(size_t)p];
+            const int64_t r0 = row_start[p];
+            row_of.assign((size_t)n, -1);
+            bool bad = false;
+            for (int64_t r = r0; r < r0 + n && !bad; ++r) {
+                const int sid = square_id ? square_id[r] : (int)(r - r0);
+                if (sid < 0 || sid >= n || row_of[(size_t)sid] >= 0) bad = true;
+                else row_of[(size_t)sid] = r;
+            }
+            if (bad) {
+                live[(size_t)p] = 0;
+                put(out[p].reason, sizeof out[p].reason,
+                    "n=" + std::to_string(n) + ": square_ids should be 0.." + std::to_string(n - 1));
+                continue;
+            }
+            for (int i = 0; i < n; ++i) {
+                const int64_t r = row_of[(size_t)i];
+                for (int k = 0; k < 3; ++k) {
+                    const int64_t a = lit_off[3 * r + k], b = lit_off[3 * r + k + 1];
+                    if (b < a) {
+                        bad_row[(size_t)t] = r;
+                        return;
+                    }
+                    const size_t q = (size_t)(3 * (pk_sq0[(size_t)p] + i) + k);
+                    if (do_rt) {
+                        const std::string s2 = roundtrip(text + a, (size_t)(b - a));
+                        raw_off[q] = (int64_t)rt[(size_t)t].size();
+                        raw_len[q] = (int32_t)s2.size();
+                        rt[(size_t)t] += s2;
+                    } else {
+                        raw_off[q] = a;
+                        raw_len[q] = (int32_t)std::min<int64_t>(b - a, 1 << 20);
+                    }
+                }
+            }
+        }
+    };
+    if (nt == 1) {
+        slice(0);
+    } else {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nt; ++t) pool.emplace_back(slice, t);
+        for (auto& th : pool) th.join();
+    }
+    for (int t = 0; t < nt; ++t)
+        SQS_REQUIRE(bad_row[(size_t)t] < 0, "literal offsets not monotone at row %lld", (long long)bad_row[(size_t)t]);
+    std::string rt_text;  // round-tripped literals, when requested
+    if (do_rt) {
+        size_t base = 0;
+        for (int t = 0; t < nt; ++t) {
+            if (base)
+                for (int p = p_lo[(size_t)t]; p < p_lo[(size_t)t + 1]; ++p) {
+                    if (!live[(size_t)p]) continue;
+                    for (int64_t q = 3 * pk_sq0[(size_t)p]; q < 3 * (pk_sq0[(size_t)p] + pk_n[(size_t)p]); ++q)
+                        raw_off[(size_t)q] += (int64_t)base;
+                }
+            base += rt[(size_t)t].size();
+        }
+        rt_text.reserve(base);
+        for (int t = 0; t < nt; ++t) rt_text += rt[(size_t)t];
+    }
     const char* blob = do_rt ? rt_text.data() : text;
     size_t blob_bytes = do_rt ? rt_text.size() : (size_t)lit_off[3 * row_start[count]];
     if (blob_bytes == 0) blob_bytes = 1;
