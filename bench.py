@@ -579,6 +579,27 @@ def bench_search(cases: str = "10:200:64:64,50:60:64:64,200:10:48:64,50:600:64:6
     return out
 
 
+def bench_batched_fixed(ctx, sweeps: int, instances: int):
+    """The batched workload at the default launch shapes (no autotuner, one
+    call): a clean single launch per cluster shape, for profiling."""
+    import numpy as np
+
+    from sqs.anneal import AnnealJob, anneal_batch, jittered_grid
+
+    rng = np.random.default_rng(42)
+    jobs = []
+    for k in range(instances):
+        n = int(rng.integers(20, 401))
+        xya, L0 = jittered_grid(n, seed=k)
+        jobs.append(AnnealJob(xya, L0=L0, replicas=32, sweeps=sweeps, exchange_every=10, tmin=1e-4, tmax=5e-2,
+                              sigma_xy=0.02, sigma_a=0.05, seed=k, polish_iters=0))
+    res = anneal_batch(jobs, ctx=ctx)
+    props = sum(r["proposals"] for r in res)
+    dev_s = res[0]["device_ms"] / 1e3
+    return dict(workload=f"{instances} instances, n U[20,400], 32 replicas, {sweeps} sweeps, default shapes",
+                proposals=props, device_seconds=dev_s, proposals_per_s=props / dev_s)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -590,7 +611,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the certifier / served / plain-PT / batched sections")
-    ap.add_argument("--section", choices=("certify", "served", "plain_pt", "batched", "search"),
+    ap.add_argument("--section", choices=("certify", "served", "plain_pt", "batched", "batched_fixed", "search"),
                     help="run only this extra section (for profiling) and print its dict")
     ap.add_argument("--batched-instances", type=int, default=512)
     ap.add_argument("--batched-sweeps", type=int, default=50)
@@ -604,6 +625,7 @@ def main():
                       served=lambda: bench_served_sweep(ctx, args.served_rates),
                       plain_pt=lambda: bench_plain_pt(ctx),
                       batched=lambda: bench_batched(ctx, args.batched_sweeps, args.batched_instances),
+                      batched_fixed=lambda: bench_batched_fixed(ctx, args.batched_sweeps, args.batched_instances),
                       search=lambda: bench_search())[args.section]
             print(json.dumps({args.section: fn()}), flush=True)
         return

@@ -108,23 +108,29 @@ template <typename Fn>
 __device__ __forceinline__ void for_block(const Rep& R, const Grid& g, int cx, int cy, int lane, Fn&& fn) {
     // Every lane reads the nine cell counts (broadcast shared loads) and
     // forms their running sum; slot t of the block belongs to the first cell
-    // whose running count exceeds t.  Lanes take slots 32 apart.
-    int ends[9], cells[9];
+    // whose running count exceeds t.  Lanes take slots 32 apart.  The cell
+    // of slot t is rebuilt from (cx, cy) and its index in the block, so no
+    // per-lane array is indexed at run time.
+    int ends[9];
     int run = 0;
 #pragma unroll
     for (int c = 0; c < 9; ++c) {
         const int x = cx + c % 3 - 1, y = cy + c / 3 - 1;
-        const bool in = x >= 0 && x < g.G && y >= 0 && y < g.G;
-        cells[c] = in ? y * g.G + x : 0;
-        run += in ? (int)R.cnt[cells[c]] : 0;
+        const bool in = (unsigned)x < (unsigned)g.G && (unsigned)y < (unsigned)g.G;
+        run += in ? (int)R.cnt[y * g.G + x] : 0;
         ends[c] = run;
     }
     for (int t = lane; t < run; t += 32) {
         int c = 0, start = 0;
 #pragma unroll
-        for (int k = 0; k < 8; ++k)
-            if (t >= ends[k]) { c = k + 1; start = ends[k]; }
-        fn((int)R.slot[cells[c] * kCellK + (t - start)]);
+        for (int k = 0; k < 8; ++k) {
+            const bool past = t >= ends[k];
+            c = past ? k + 1 : c;
+            start = past ? ends[k] : start;
+        }
+        const int cr = (c * 43) >> 7;  // c / 3 for c < 9
+        const int cell = (cy + cr - 1) * g.G + cx + (c - 3 * cr) - 1;
+        fn((int)R.slot[cell * kCellK + (t - start)]);
     }
 }
 
