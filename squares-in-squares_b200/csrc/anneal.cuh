@@ -7,7 +7,7 @@ namespace sqs {
 namespace ann {
 
 constexpr int kMaxR = 64;            // replicas (temperature rungs) per job
-constexpr int kMaxRl = 32;           // replicas (warps) per CTA
+constexpr int kMaxRl = 16;           // replicas (warps) per CTA: 512 threads, 128 registers each
 constexpr int kCellK = 12;           // slot capacity of one cell
 constexpr float kCellSide = 1.59f;   // >= sqrt(2.000001) + largest centre move (0.12 * sqrt 2)
 constexpr float kCellSideMax = 2.2f; // largest cell side the autotuner tries

@@ -450,7 +450,7 @@ __device__ __forceinline__ float wrap_quarter_f(float a) {
 // overflows a cell) is undone from `save`, the replica's own HBM slot, which
 // holds nothing else while a slice runs.  Returns whether it was accepted;
 // *ovf counts overflows.
-__device__ __noinline__ bool collective_move(const Rep& rep, const Grid& g, int n, float L, int lane, int mode, int c,
+__device__ __forceinline__ bool collective_move(const Rep& rep, const Grid& g, int n, float L, int lane, int mode, int c,
                                              float tx, float ty, float th, float u, float invT, long long& E,
                                              float4* __restrict__ save, int* ovf) {
     const float cx = rep.sq[c].x, cy = rep.sq[c].y, ca = rep.ang[c];
@@ -526,7 +526,7 @@ __device__ __noinline__ bool collective_move(const Rep& rep, const Grid& g, int 
 // elsewhere.  Draws are Philox blocks keyed by (round, square, replica).
 // Returns the new energy (the old one if a cell would overflow, the state
 // then restored from `save`).
-__device__ __noinline__ long long kick_replica(const Rep& rep, const Grid& g, int n, float L, int lane, int r,
+__device__ __forceinline__ long long kick_replica(const Rep& rep, const Grid& g, int n, float L, int lane, int r,
                                                int round, uint32_t k0, uint32_t k1, long long E,
                                                float4* __restrict__ save) {
     float wmax = -1.f;
@@ -649,7 +649,7 @@ struct CtaShared {
 // MOVES: whether the move-set options (adaptation, collective moves, kicks)
 // are compiled in; jobs without them run the leaner instance.
 template <bool MOVES>
-__global__ void __launch_bounds__(1024) anneal_kernel(const int32_t* __restrict__ job_list,
+__global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __restrict__ job_list,
                                                       const JobDev* __restrict__ jdev, JobMut* __restrict__ jmut,
                                                       float4* __restrict__ pos, double* __restrict__ best,
                                                       int slice_sweeps) {
