@@ -37,6 +37,13 @@ namespace ann {
 
 constexpr float kHalfPiF = 1.57079632679489662f;
 
+// cos/sin of a replica's angle, wherever the state's trig is (re)computed:
+// the hardware approximation (absolute error below 4e-7 on [0, pi/2)), the
+// same function everywhere so a state's (cos, sin) never depends on where it
+// was computed (a sliced run reloads what an unsliced one kept).  The FP64
+// certified side recomputes trig from the angle itself.
+__device__ __forceinline__ void state_trig(float a, float* s, float* c) { __sincosf(a, s, c); }
+
 struct Rep {  // one replica's shared-memory view
     float4* sq;        // (x, y, cos a, sin a)
     float* ang;        // a in [0, pi/2)
@@ -390,7 +397,7 @@ __device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters
                 a = a - kHalfPiF * floorf(a * (1.0f / kHalfPiF));
                 if (!(a >= 0.f && a < kHalfPiF)) a = 0.f;
                 float sn, cs;
-                sincosf(a, &sn, &cs);
+                state_trig(a, &sn, &cs);
                 R.sq[i] = make_float4(o.x - sx, o.y - sy, cs, sn);
                 R.ang[i] = a;
             }
@@ -406,7 +413,7 @@ __device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters
                     for (int i = threadIdx.x; i < n; i += blockDim.x) {
                         const float4 o = saved[i];
                         float sn, cs;
-                        sincosf(o.z, &sn, &cs);
+                        state_trig(o.z, &sn, &cs);
                         R.sq[i] = make_float4(o.x, o.y, cs, sn);
                         R.ang[i] = o.z;
                     }
@@ -421,7 +428,7 @@ __device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters
                 for (int i = threadIdx.x; i < n; i += blockDim.x) {
                     const float4 o = saved[i];
                     float sn, cs;
-                    sincosf(o.z, &sn, &cs);
+                    state_trig(o.z, &sn, &cs);
                     R.sq[i] = make_float4(o.x, o.y, cs, sn);
                     R.ang[i] = o.z;
                 }
@@ -455,7 +462,7 @@ __device__ __forceinline__ bool collective_move(const Rep& rep, const Grid& g, i
                                              float4* __restrict__ save, int* ovf) {
     const float cx = rep.sq[c].x, cy = rep.sq[c].y, ca = rep.ang[c];
     float st, ct;
-    sincosf(th, &st, &ct);
+    state_trig(th, &st, &ct);
     __syncwarp();
     for (int s = lane; s < n; s += 32) {
         const float4 P = rep.sq[s];
@@ -485,7 +492,7 @@ __device__ __forceinline__ bool collective_move(const Rep& rep, const Grid& g, i
             ny = fminf(L - 0.5f, fmaxf(0.5f, ny));
             const float na = wrap_quarter_f(a + th);
             float sn, cs;
-            sincosf(na, &sn, &cs);
+            state_trig(na, &sn, &cs);
             rep.sq[s] = make_float4(nx, ny, cs, sn);
             rep.ang[s] = na;
         }
@@ -506,7 +513,7 @@ __device__ __forceinline__ bool collective_move(const Rep& rep, const Grid& g, i
             const float4 o = save[s];
             if (o.w != 0.f) {
                 float sn, cs;
-                sincosf(o.z, &sn, &cs);
+                state_trig(o.z, &sn, &cs);
                 rep.sq[s] = make_float4(o.x, o.y, cs, sn);
                 rep.ang[s] = o.z;
             }
@@ -597,7 +604,7 @@ __device__ __forceinline__ long long kick_replica(const Rep& rep, const Grid& g,
             const float vy = 0.55f + (L - 1.1f) * ((float)(bp / 8) + 0.5f) / 8.f;
             const float na = wrap_quarter_f(u01(q.z) * kHalfPiF);
             float sn, cs;
-            sincosf(na, &sn, &cs);
+            state_trig(na, &sn, &cs);
             rep.sq[worst] = make_float4(fminf(L - 0.5f, fmaxf(0.5f, vx + 0.05f * (2.f * u01(q.x) - 1.f))),
                                         fminf(L - 0.5f, fmaxf(0.5f, vy + 0.05f * (2.f * u01(q.y) - 1.f))), cs, sn);
             rep.ang[worst] = na;
@@ -611,7 +618,7 @@ __device__ __forceinline__ long long kick_replica(const Rep& rep, const Grid& g,
         const float4 P = rep.sq[s];
         const float na = wrap_quarter_f(rep.ang[s] + aa * (2.f * u01(q.z) - 1.f));
         float sn, cs;
-        sincosf(na, &sn, &cs);
+        state_trig(na, &sn, &cs);
         rep.sq[s] = make_float4(fminf(L - 0.48f, fmaxf(0.48f, P.x + axy * (2.f * u01(q.x) - 1.f))),
                                 fminf(L - 0.48f, fmaxf(0.48f, P.y + axy * (2.f * u01(q.y) - 1.f))), cs, sn);
         rep.ang[s] = na;
@@ -621,7 +628,7 @@ __device__ __forceinline__ long long kick_replica(const Rep& rep, const Grid& g,
     for (int s = lane; s < n; s += 32) {
         const float4 o = save[s];
         float sn, cs;
-        sincosf(o.z, &sn, &cs);
+        state_trig(o.z, &sn, &cs);
         rep.sq[s] = make_float4(o.x, o.y, cs, sn);
         rep.ang[s] = o.z;
     }
@@ -685,7 +692,7 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
         for (int i = lane; i < n; i += 32) {
             const float4 p = src[i];
             float s, c;
-            sincosf(p.z, &s, &c);
+            state_trig(p.z, &s, &c);
             rep.sq[i] = make_float4(p.x, p.y, c, s);
             rep.ang[i] = p.z;
         }
@@ -781,7 +788,7 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                     na = na - kHalfPiF * floorf(na * (1.0f / kHalfPiF));
                     if (!(na >= 0.f && na < kHalfPiF)) na = 0.f;
                     float ns, nc;
-                    sincosf(na, &ns, &nc);
+                    state_trig(na, &ns, &nc);
                     const int ocx = g.cx(P.x), ocy = g.cx(P.y);
                     long long dq = 0;
                     if (lane == 0) dq = qe(wall_e(nx, ny, nc, ns, L)) - qe(wall_e(P.x, P.y, P.z, P.w, L));
