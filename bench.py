@@ -399,32 +399,49 @@ def bench_certify(ctx, cpu_seconds: float, count: int = 10000):
     return res
 
 
-def bench_served(ctx, count: int = 48, rate: float = 200.0):
-    """Served vs plain: a Poisson stream of anneal-and-certify jobs (n
-    log-uniform in [5, 64], 16 replicas, 300 sweeps each -- a bounded budget so
-    the run ends in seconds) through the continuous-batching server, and the
-    same jobs one launch per job; same final L by construction, checked."""
+def served_jobs(count: int):
+    """Anneal-and-certify jobs of the served stream: n log-uniform in
+    [5, 1000], 16, 32 or 64 replicas, a 200-sweep budget each (a bounded
+    stand-in for the 50,000 sweeps a production job would run, so the bench
+    ends in minutes), seeded."""
     import math
 
     import numpy as np
 
     from sqs.anneal import AnnealJob, jittered_grid
-    from sqs.serve import Server, poisson_arrivals, run_plain, run_stream
 
     rng = np.random.default_rng(7)
     jobs = []
     for k in range(count):
-        n = int(round(math.exp(rng.uniform(math.log(5), math.log(64)))))
+        n = int(round(math.exp(rng.uniform(math.log(5), math.log(1000)))))
+        replicas = int(rng.choice([16, 32, 64]))
         xya, L0 = jittered_grid(n, seed=100 + k)
-        jobs.append(AnnealJob(xya, L0=L0, replicas=16, sweeps=300, exchange_every=10, tmin=1e-3, tmax=1e-1,
+        jobs.append(AnnealJob(xya, L0=L0, replicas=replicas, sweeps=200, exchange_every=10, tmin=1e-3, tmax=1e-1,
                               seed=1000 + k, polish_iters=100))
+    return jobs
+
+
+def bench_served(ctx, jobs, plain, rate: float):
+    """Served vs plain at one Poisson arrival rate: a stream of about four
+    seconds (at least 40 jobs, at most all of them) through the
+    continuous-batching server; the plain comparator serves the same jobs one
+    launch per job in arrival order, its service times measured once
+    (`plain`), its latencies from those times and the same arrivals.  The
+    same final L is checked job by job."""
+    import math
+
+    from sqs.serve import Server, plain_stats, poisson_arrivals, run_stream
+
+    count = min(len(jobs), max(40, int(math.ceil(4 * rate))))
+    sub = jobs[:count]
     arr = poisson_arrivals(count, rate, seed=3)
-    with Server(ctx, hbm_bytes=1 << 30, max_active=count, slice_sweeps=50) as srv:
-        served, s_stats = run_stream(srv, jobs, arr, timeout=300)
-    plain, p_stats = run_plain(ctx, jobs, arr)
-    same_L = all((a or {}).get("L") == (b or {}).get("L") for a, b in zip(served, plain))
-    return dict(workload=f"{count} jobs, Poisson {rate:g}/s, n log-uniform [5, 64], 16 replicas, 300 sweeps",
-                served=s_stats, plain=p_stats, equal_final_L=same_L,
+    with Server(ctx, hbm_bytes=4 << 30, max_active=count, slice_proposals=4000) as srv:
+        served, s_stats = run_stream(srv, sub, arr, timeout=600)
+    p_res, p_service = plain
+    p_stats = plain_stats(p_res[:count], p_service[:count], arr)
+    same_L = all((a or {}).get("L") == (b or {}).get("L") for a, b in zip(served, p_res[:count]))
+    return dict(workload=f"{count} jobs, Poisson {rate:g}/s, n log-uniform [5, 1000], 16/32/64 replicas, "
+                         f"200 sweeps", served=s_stats, plain=p_stats, equal_final_L=same_L,
                 served_over_plain=s_stats["certified_jobs_per_s"] / max(p_stats["certified_jobs_per_s"], 1e-12))
 
 
@@ -454,11 +471,21 @@ def bench_plain_pt(ctx):
     return res
 
 
-def bench_served_sweep(ctx, rates: str):
-    out = {}
-    for r in [float(x) for x in rates.split(",") if x]:
-        out[f"{r:g}/s"] = bench_served(ctx, rate=r)
-    return out
+def bench_served_sweep(ctx, rates: str, count: int = 240):
+    from sqs.serve import plain_service
+
+    rs = [float(x) for x in rates.split(",") if x]
+    jobs = served_jobs(count)
+    need = min(count, max(40, max(int(4 * r + 1) for r in rs)))
+    plain = plain_service(ctx, jobs[:need])
+    return {f"{r:g}/s": bench_served(ctx, jobs, plain, r) for r in rs}
+
+
+# Algorithmic FP32 work of one proposal, the cost unit 2 k * 35 + 2 * 10 flop
+# (the pair energy before and after the move against each of the k squares
+# within d^2 < 2 of the moved one, and the two wall terms), with k ~ 4 at
+# packing densities: 300 flop.
+PROPOSAL_FLOP = 2 * 4 * 35 + 2 * 10
 
 
 def bench_batched(ctx, sweeps: int = 50, instances: int = 512):
@@ -516,6 +543,8 @@ def bench_batched(ctx, sweeps: int = 50, instances: int = 512):
     return dict(workload=f"{instances} instances, n U[20,400], 32 replicas, {sweeps} sweeps",
                 cpu_baseline=cpu, speedup_vs_cpu=(props / dev_s) / cpu["proposals_per_s"],
                 proposals=props, seconds=dt, device_seconds=dev_s, proposals_per_s=props / dev_s,
+                replica_sweeps_per_s=sum(j.replicas * j.sweeps for j in jobs) / dev_s,
+                flops_per_s=props * PROPOSAL_FLOP / dev_s,
                 fixed_shape=dict(device_seconds=fixed_s, proposals_per_s=props / fixed_s),
                 graph_slices=dict(slice_sweeps=10, graph_replays=replays, device_seconds=graph_s,
                                   proposals_per_s=props / graph_s),
@@ -615,7 +644,7 @@ def main():
                     help="run only this extra section (for profiling) and print its dict")
     ap.add_argument("--batched-instances", type=int, default=512)
     ap.add_argument("--batched-sweeps", type=int, default=50)
-    ap.add_argument("--served-rates", default="50,200,1000")
+    ap.add_argument("--served-rates", default="10,50,200,1000")
     args = ap.parse_args()
     if args.section:
         from sqs import Context

@@ -295,7 +295,10 @@ int sqs_autotune(sqs_ctx* ctx, const sqs_job* job, int mode, sqs_tuning* out);
  * Jobs are admitted while a job slot is free and their state (replicas,
  * scratch, best packing) fits an HBM arena of `hbm_bytes`; every step runs
  * one slice of `slice_sweeps` sweeps for all admitted jobs side by side in
- * one launch per cluster shape, their state resident between slices, then
+ * one launch per cluster shape (slice_sweeps < 0: every job runs about
+ * -slice_sweeps proposals per replica per step -- ceil(-slice_sweeps / n)
+ * sweeps rounded up to whole exchange intervals -- so a step takes about
+ * the same time for small and large jobs), their state resident between slices, then
  * polishes, certifies and retires the finished ones so queued jobs take
  * their place.  Each job's result equals its sqs_anneal_batch result.
  * Replaces one-search-process-per-job campaigns (scheduler.run_gpu,

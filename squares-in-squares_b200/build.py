@@ -26,9 +26,11 @@ BIN = PKG / "bin"
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
                "--expt-relaxed-constexpr", "-I", str(ROOT / "include")]
-# Kernels whose double-precision results must equal a C oracle bit for bit are
-# compiled without multiply-add contraction (the host compiler contracts none).
-NO_FMA = {"certify_kernel.cu", "recompute.cu"}
+# Kernels compiled without multiply-add contraction: the certifier, whose
+# double-precision results must equal a C oracle bit for bit (the host
+# compiler contracts none), and the FP64 polish, whose neighbour-list and
+# all-pairs energies must agree bit for bit.
+NO_FMA = {"certify_kernel.cu", "polish_kernel.cu"}
 
 
 def nvcc() -> str:

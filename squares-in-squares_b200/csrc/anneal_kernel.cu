@@ -731,7 +731,7 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
     float4* save = pos + jd.pos_off + (int64_t)r * n;  // this replica's HBM slot: free while the slice runs
 
     const int sweep0 = S.jm.sweep;
-    const int sweep_end = min(jd.sweeps_total, sweep0 + slice_sweeps);
+    const int sweep_end = min(jd.sweeps_total, sweep0 + (jd.slice > 0 ? jd.slice : slice_sweeps));
     for (int sweep = sweep0; sweep < sweep_end; ++sweep) {
         if (active) {
             for (int kb = 0; kb < n; kb += 32) {

@@ -24,7 +24,18 @@ namespace ann {
 
 constexpr int kPT = 256;  // threads per polish CTA
 
-size_t polish_smem_bytes(int n) { return (size_t)n * (4 * 24 + 16) + 64; }
+// Neighbour lists of the polish: every partner within sqrt(2.000001) + 0.25
+// of a square when the list was built (at most kNbK, ascending), valid while
+// no square has moved more than 0.125 since -- then every pair inside the
+// pair cut-off is listed.  Energies over the list sum the same nonzero terms
+// in the same order as the all-pairs loop, so they are bit-identical to it.
+constexpr int kNbK = 24;
+constexpr double kNbR2 = 2.7697;       // (sqrt(2.000001) + 0.25)^2 = 2.76961, rounded up
+constexpr double kNbMove2 = 0.015625;  // 0.125^2
+
+// q0, q, g, sv (double3), cs (double2), the list's reference centres
+// (double2), partner indices (uint16) and counts (uint8)
+size_t polish_smem_bytes(int n) { return (size_t)n * (4 * 24 + 16 + 16 + 2 * kNbK + 1) + 64; }
 
 __device__ __forceinline__ double sgn_s(double x) { return fabs(x) > 1e-6 ? (x >= 0.0 ? 1.0 : -1.0) : 0.0; }
 
@@ -94,15 +105,25 @@ __device__ double block_max(double v, double* red) {
     return t;
 }
 
-// Energy (and gradient into g when g != nullptr) of the state q at side L.
-__device__ double energy(int n, const double3* q, const double2* cs, double L, double3* g, double* red) {
+struct NbrList {
+    double2* ref;   // centres at the build
+    uint16_t* idx;  // partners of square i: idx[i * kNbK + k], k < cnt[i]
+    uint8_t* cnt;
+};
+
+// Energy (and gradient into g when g != nullptr) of the state q at side L,
+// over the neighbour list when nb != nullptr, else over all pairs.
+__device__ double energy(int n, const double3* q, const double2* cs, double L, double3* g, double* red,
+                         const NbrList* nb = nullptr) {
     double e = 0.0;
     for (int i = threadIdx.x; i < n; i += kPT) {
         const double3 p = q[i];
         const double2 pc = cs[i];
         double gx = 0, gy = 0, ga = 0;
         e += wall_smooth(p.x, p.y, pc.x, pc.y, L, gx, gy, ga);
-        for (int j = 0; j < n; ++j) {
+        const int m = nb ? nb->cnt[i] : n;
+        for (int k = 0; k < m; ++k) {
+            const int j = nb ? (int)nb->idx[i * kNbK + k] : k;
             if (j == i) continue;
             const double3 o = q[j];
             const double2 oc = cs[j];
@@ -116,6 +137,38 @@ __device__ double energy(int n, const double3* q, const double2* cs, double L, d
         if (g) g[i] = make_double3(gx, gy, ga);
     }
     return block_sum(e, red);
+}
+
+// Build the list for state q; false when a square has more than kNbK
+// partners (the callers then use all pairs).
+__device__ bool build_nbr(int n, const NbrList& nb, const double3* q, double* red) {
+    double over = 0.0;
+    for (int i = threadIdx.x; i < n; i += kPT) {
+        const double3 p = q[i];
+        int c = 0;
+        for (int j = 0; j < n; ++j) {
+            if (j == i) continue;
+            const double dx = q[j].x - p.x, dy = q[j].y - p.y;
+            if (dx * dx + dy * dy < kNbR2) {
+                if (c < kNbK) nb.idx[i * kNbK + c] = (uint16_t)j;
+                ++c;
+            }
+        }
+        nb.cnt[i] = (uint8_t)min(c, kNbK);
+        nb.ref[i] = make_double2(p.x, p.y);
+        if (c > kNbK) over = 1.0;
+    }
+    return block_max(over, red) == 0.0;
+}
+
+// Largest squared centre displacement of q since the list was built.
+__device__ double moved2(int n, const NbrList& nb, const double3* q, double* red) {
+    double m = 0.0;
+    for (int i = threadIdx.x; i < n; i += kPT) {
+        const double dx = q[i].x - nb.ref[i].x, dy = q[i].y - nb.ref[i].y;
+        m = fmax(m, dx * dx + dy * dy);
+    }
+    return block_max(m, red);
 }
 
 // Certified side of q (dilation lambda, bounding box of the dilated state).
@@ -176,6 +229,7 @@ struct PolishBufs {
     double3* g;   // gradient at q0
     double3* sv;  // best so far (translated, dilated)
     double2* cs;  // cos/sin of the state being evaluated
+    NbrList nb;   // neighbour list of the descent
 };
 
 __device__ __forceinline__ PolishBufs polish_bufs(unsigned char* dyn, int n) {
@@ -185,6 +239,9 @@ __device__ __forceinline__ PolishBufs polish_bufs(unsigned char* dyn, int n) {
     b.g = b.q + n;
     b.sv = b.g + n;
     b.cs = reinterpret_cast<double2*>(b.sv + n);
+    b.nb.ref = b.cs + n;
+    b.nb.idx = reinterpret_cast<uint16_t*>(b.nb.ref + n);
+    b.nb.cnt = reinterpret_cast<uint8_t*>(b.nb.idx + (size_t)n * kNbK);
     return b;
 }
 
@@ -192,7 +249,8 @@ __device__ __forceinline__ PolishBufs polish_bufs(unsigned char* dyn, int n) {
 // *budget gradient steps, each with up to 8 backtracking trials).
 __device__ void descend(int n, const PolishBufs& B, double Lt, int* budget, double* red) {
     trig_of(n, B.q0, B.cs);
-    double E = energy(n, B.q0, B.cs, Lt, B.g, red);
+    bool listed = build_nbr(n, B.nb, B.q0, red);
+    double E = energy(n, B.q0, B.cs, Lt, B.g, red, listed ? &B.nb : nullptr);
     double alpha = 0.05;
     while (*budget > 0 && E > 1e-26) {
         --*budget;
@@ -204,19 +262,22 @@ __device__ void descend(int n, const PolishBufs& B, double Lt, int* budget, doub
             }
             __syncthreads();
             trig_of(n, B.q, B.cs);
-            const double En = energy(n, B.q, B.cs, Lt, nullptr, red);
+            const double d2 = listed ? moved2(n, B.nb, B.q, red) : 1e30;
+            const double En = energy(n, B.q, B.cs, Lt, nullptr, red, d2 <= kNbMove2 ? &B.nb : nullptr);
             if (En < E) {
                 E = En;
                 moved = true;
                 alpha = fmin(alpha * 1.5, 0.5);
                 for (int i = threadIdx.x; i < n; i += kPT) B.q0[i] = B.q[i];
                 __syncthreads();
+                // keep room for the next trials: rebuild once half the slack is used
+                if (d2 > 0.25 * kNbMove2) listed = build_nbr(n, B.nb, B.q0, red);
             } else {
                 alpha *= 0.3;
             }
         }
         if (!moved) break;
-        E = energy(n, B.q0, B.cs, Lt, B.g, red);  // cs holds the trig of q == q0
+        E = energy(n, B.q0, B.cs, Lt, B.g, red, listed ? &B.nb : nullptr);  // cs holds the trig of q == q0
     }
     trig_of(n, B.q0, B.cs);
 }

@@ -61,7 +61,7 @@ struct sqs_server {
     char* arena = nullptr;
     size_t arena_bytes = 0;
     std::map<size_t, size_t> free_blocks;  // offset -> bytes
-    int max_active = 0, slice = 0;
+    int max_active = 0, slice = 0;  // slice < 0: about -slice proposals per replica per step, per job
     JobDev* d_jd = nullptr;
     JobMut* d_jm = nullptr;
     int32_t* d_list = nullptr;
@@ -129,6 +129,11 @@ int admit(sqs_server* s) {
         j.jd.pos_off = (int64_t)(off / sizeof(float4));
         j.jd.scr_off = j.jd.pos_off + (int64_t)j.job.replicas * j.job.n;
         j.jd.best_off = (int64_t)((off + sizeof(float4) * (size_t)job_pos_elems(j.job)) / sizeof(double));
+        if (s->slice < 0) {  // this job's sweeps per step: about -slice proposals, whole exchange intervals
+            const int xe = j.jd.exchange_every;
+            const int64_t sw = std::max<int64_t>(1, (-(int64_t)s->slice + j.job.n - 1) / j.job.n);
+            j.jd.slice = (int)std::min<int64_t>((sw + xe - 1) / xe * xe, 1 << 30);
+        }
         std::vector<float4> init((size_t)job_pos_elems(j.job), make_float4(0.f, 0.f, 0.f, 0.f));
         init_replicas(j.job, init.data());
         SQS_CUDA(cudaMemcpyAsync(s->arena + off, init.data(), sizeof(float4) * init.size(), cudaMemcpyHostToDevice,
@@ -149,7 +154,7 @@ extern "C" int sqs_server_create(sqs_ctx* ctx, size_t hbm_bytes, int max_active,
     if (int r = enter(ctx)) return r;
     SQS_REQUIRE(out != nullptr, "null output pointer");
     SQS_REQUIRE(max_active >= 1 && max_active <= 4096, "max_active %d out of 1..4096", max_active);
-    SQS_REQUIRE(slice_sweeps >= 1, "slice_sweeps must be >= 1");
+    SQS_REQUIRE(slice_sweeps != 0, "slice_sweeps must be nonzero");
     SQS_REQUIRE(hbm_bytes >= (1u << 20), "hbm budget below 1 MiB");
     sqs_server* s = new sqs_server();
     s->ctx = ctx;
@@ -252,7 +257,8 @@ extern "C" int sqs_server_step(sqs_server* s, int* in_flight) {
                                    std::get<2>(g.first) != 0});
             ++gi;
         }
-        if (int r = launch_groups(s->ctx, launch, s->d_jd, s->d_jm, (float4*)s->arena, (double*)s->arena, s->slice))
+        if (int r = launch_groups(s->ctx, launch, s->d_jd, s->d_jm, (float4*)s->arena, (double*)s->arena,
+                                  std::max(1, s->slice)))
             return r;
         s->ctx->launches += (int64_t)launch.size();
         SQS_CUDA(cudaMemcpyAsync(s->h_jm.data(), s->d_jm, sizeof(JobMut) * (size_t)s->max_active,

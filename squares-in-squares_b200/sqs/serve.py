@@ -29,9 +29,15 @@ def _result_dict(job: AnnealJob, r: N.JobResult, q: np.ndarray) -> dict:
 
 
 class Server:
-    def __init__(self, ctx: N.Context, hbm_bytes: int = 4 << 30, max_active: int = 512, slice_sweeps: int = 100):
+    """sqs_server: slice_sweeps sweeps of every admitted job per step, or,
+    with slice_proposals, about that many proposals per replica of every job
+    per step (its own sweep count, whole exchange intervals)."""
+
+    def __init__(self, ctx: N.Context, hbm_bytes: int = 4 << 30, max_active: int = 512, slice_sweeps: int = 100,
+                 *, slice_proposals: int | None = None):
         h = N._vp()
-        N.check(N.lib().sqs_server_create(ctx.handle, hbm_bytes, max_active, slice_sweeps, C.byref(h)))
+        slice_arg = -int(slice_proposals) if slice_proposals else slice_sweeps
+        N.check(N.lib().sqs_server_create(ctx.handle, hbm_bytes, max_active, slice_arg, C.byref(h)))
         self.handle = h.value
         self.ctx = ctx
         self._jobs: dict[int, AnnealJob] = {}
@@ -121,17 +127,30 @@ def run_stream(server: Server, jobs: list[AnnealJob], arrivals, *, timeout: floa
     return results, _latency_stats(lat, span, sum(bool(r and r["certified"]) for r in results))
 
 
-def run_plain(ctx: N.Context, jobs: list[AnnealJob], arrivals):
-    """The comparator: every job alone in its own anneal/polish/certify
-    launches, in arrival order (FIFO).  Returns (results, stats)."""
+def plain_service(ctx: N.Context, jobs: list[AnnealJob]) -> tuple[list[dict], list[float]]:
+    """The comparator's service: every job alone in its own anneal, polish
+    and certify launches.  Returns (results, seconds per job)."""
     results, service = [], []
     for job in jobs:
         t = time.perf_counter()
         results.append(anneal_batch([job], ctx=ctx)[0])
         service.append(time.perf_counter() - t)
+    return results, service
+
+
+def plain_stats(results: list[dict], service: list[float], arrivals) -> dict:
+    """Latencies of the plain comparator serving jobs in arrival order (FIFO)
+    with the given per-job service times."""
     finish, lat = 0.0, []
     for a, s in zip(arrivals, service):
         finish = max(finish, float(a)) + s
         lat.append(finish - float(a))
-    span = finish - float(arrivals[0]) if jobs else 0.0
-    return results, _latency_stats(lat, span, sum(bool(r["certified"]) for r in results))
+    span = finish - float(arrivals[0]) if len(service) else 0.0
+    return _latency_stats(lat, span, sum(bool(r["certified"]) for r in results))
+
+
+def run_plain(ctx: N.Context, jobs: list[AnnealJob], arrivals):
+    """The comparator: every job alone in its own anneal/polish/certify
+    launches, in arrival order (FIFO).  Returns (results, stats)."""
+    results, service = plain_service(ctx, jobs)
+    return results, plain_stats(results, service, arrivals)

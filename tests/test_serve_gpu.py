@@ -83,3 +83,22 @@ def test_poisson_stream_reports_latency(ctx):
     assert stats["jobs"] == len(jobs)
     assert 0 < stats["p50_s"] <= stats["p99_s"]
     assert all(r is not None for r in results)
+
+
+def test_proposal_sliced_server_equals_alone(ctx):
+    """Per-job slices of about 300 proposals per replica (small jobs run many
+    sweeps per step, large ones few): every result equals the job alone."""
+    from sqs.anneal import anneal_batch
+    from sqs.serve import Server
+    jobs = [_job(6, 11, 400, replicas=4), _job(90, 12, 60, replicas=16), _job(25, 13, 200)]
+    alone = [anneal_batch([j], ctx=ctx)[0] for j in jobs]
+    with Server(ctx, hbm_bytes=64 << 20, max_active=3, slice_proposals=300) as srv:
+        ids = [srv.submit(j) for j in jobs]
+        steps = 0
+        while srv.step():
+            steps += 1
+        got = [srv.poll(i) for i in ids]
+    assert steps >= 3
+    for a, b in zip(alone, got):
+        for key in KEYS:
+            assert a[key] == b[key], key
