@@ -309,15 +309,31 @@ int sqs_server_create(sqs_ctx* ctx, size_t hbm_bytes, int max_active, int slice_
 int sqs_server_destroy(sqs_server* server);
 /* Queue a job (the job and its initial state are copied). */
 int sqs_server_submit(sqs_server* server, const sqs_job* job, int64_t* id);
-/* One admission + slice + retirement round; *in_flight = queued + running. */
+/* One round of the loop: admit queued jobs; collect the slices that have
+ * finished; start the next slice of every idle job (one launch per cluster
+ * shape, each on its own stream, so slices of different jobs start and end
+ * independently); polish, certify and retire the jobs whose budget is spent
+ * while the other slices run.  When there is nothing to do it waits up to
+ * 2 ms for a slice to finish.  *in_flight = queued + running. */
 int sqs_server_step(sqs_server* server, int* in_flight);
 /* 1 and the result (and n*3 packing into xya_out when certified) once the
  * job is done -- the job is then forgotten; 0 while it is queued or running;
  * SQS_ENOTFOUND for an unknown id. */
 int sqs_server_poll(sqs_server* server, int64_t id, sqs_job_result* out, double* xya_out);
-/* Withdraw a queued job now, or a running one at the end of the next step. */
+/* Withdraw a queued job now, or a running one when its slice in flight ends
+ * (it is retired uncertified by the step that collects that slice). */
 int sqs_server_cancel(sqs_server* server, int64_t id);
 int sqs_server_info(sqs_server* server, int* queued, int* active, size_t* hbm_used);
+/* Counters since the server's creation: steps, slice launches, jobs
+ * admitted and retired, and the host wall seconds of each phase of the steps
+ * -- admission (state upload), harvesting finished slices and launching new
+ * ones, retirement (polish, rescue, certification, while other slices run)
+ * and waiting for a slice to finish when there was nothing else to do. */
+typedef struct sqs_server_stats {
+    int64_t steps, slices, admitted, retired;
+    double admit_s, launch_s, retire_s, wait_s;
+} sqs_server_stats;
+int sqs_server_get_stats(sqs_server* server, sqs_server_stats* out);
 
 #ifdef __cplusplus
 }

@@ -5,13 +5,16 @@
 //   step     one round of the loop:
 //              admit queued jobs while a job slot is free and the job's state
 //              (R*n replica squares + quench scratch + FP64 best) fits the HBM
-//              arena (first fit, looking past a job that does not fit yet);
-//              one anneal slice for every admitted job in a single launch per
-//              cluster shape -- jobs admitted at different times, at different
-//              sweep counts, run side by side, their state resident in HBM
-//              between slices;
-//              the jobs whose budget ran out are polished, certified and
-//              retired, and their slot and arena space go to the next;
+//              arena (first fit, looking past up to 16 jobs that do not fit yet);
+//              collect the slices that have finished;
+//              start the next anneal slice of every idle job, one launch per
+//              cluster shape, each launch a cohort on its own stream -- jobs
+//              admitted at different times, at different sweep counts, run side
+//              by side, their state resident in HBM between slices, and no
+//              cohort waits for another (no barrier across the GPU per round);
+//              polish, certify and retire the jobs whose budget ran out, on a
+//              stream of the highest priority while the cohorts anneal, and
+//              give their slot and arena space to the next;
 //   poll     hands back a finished job's result and best packing.
 // A job's result is the same here as alone through sqs_anneal_batch: its
 // trajectory depends on its inputs and seed only.
@@ -23,9 +26,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <deque>
 #include <map>
+#include <thread>
 #include <tuple>
 #include <unordered_map>
 #include <vector>
@@ -49,6 +54,7 @@ struct SJob {
     JobDev jd{};
     JobMut jm{};
     Plan plan{};
+    int64_t left = 0;           // sweeps not yet launched
     size_t off = 0, bytes = 0;  // arena block
     sqs_job_result res{};
     std::vector<double> best;   // certified packing (n x 3) when done
@@ -56,8 +62,25 @@ struct SJob {
 
 }  // namespace
 
+namespace {
+// One in-flight slice: the jobs of one cluster shape, launched on the
+// cohort's own stream and finished independently of the other cohorts.
+struct Cohort {
+    cudaStream_t st = nullptr;
+    cudaEvent_t done = nullptr;
+    int32_t* d_list = nullptr;    // the cohort's job slots (device)
+    int32_t* d_status = nullptr;  // their status after the slice (device)
+    int32_t* h_status = nullptr;  // ... and its pinned host copy
+    std::vector<int32_t> slots;
+    bool busy = false;
+};
+constexpr int kCohorts = 8;
+constexpr double kWaitSeconds = 2e-3;
+}  // namespace
+
 struct sqs_server {
     sqs_ctx* ctx = nullptr;
+    sqs_ctx* rctx = nullptr;  // retirement: own buffers, a stream of the highest priority
     char* arena = nullptr;
     size_t arena_bytes = 0;
     std::map<size_t, size_t> free_blocks;  // offset -> bytes
@@ -70,7 +93,10 @@ struct sqs_server {
     std::unordered_map<int64_t, SJob> jobs;
     int64_t next_id = 1;
     std::vector<JobMut> h_jm;
+    std::vector<uint8_t> flying;           // per slot: in a cohort's slice now
+    std::vector<Cohort> cohorts;
     size_t used = 0;
+    sqs_server_stats st{};
 };
 
 namespace {
@@ -104,24 +130,31 @@ void arena_free(sqs_server* s, size_t off, size_t bytes) {
     s->free_blocks[off] = bytes;
 }
 
+double seconds_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
 size_t job_bytes(const sqs_job& J) {
     const size_t b = sizeof(float4) * (size_t)job_pos_elems(J) + sizeof(double) * 3 * (size_t)J.n;
     return (b + 255) & ~(size_t)255;
 }
 
 int admit(sqs_server* s) {
-    const size_t window = 16;  // look past jobs that do not fit yet
-    size_t looked = 0;
-    for (auto it = s->queue.begin(); it != s->queue.end() && looked < window;) {
-        ++looked;
+    const size_t window = 16;  // queued jobs that do not fit yet which admission looks past
+    size_t skipped = 0;
+    int slot = 0;
+    std::vector<std::vector<float4>> inits;  // host staging, alive until the copies are done
+    for (auto it = s->queue.begin(); it != s->queue.end() && skipped < window;) {
         SJob& j = s->jobs[*it];
-        int slot = -1;
-        for (int k = 0; k < s->max_active; ++k)
-            if (s->slot_job[(size_t)k] < 0) { slot = k; break; }
-        if (slot < 0) break;
+        while (slot < s->max_active && s->slot_job[(size_t)slot] >= 0) ++slot;
+        if (slot >= s->max_active) break;
         const size_t bytes = job_bytes(j.job);
         const size_t off = arena_alloc(s, bytes);
-        if (off == (size_t)-1) { ++it; continue; }
+        if (off == (size_t)-1) {
+            ++skipped;
+            ++it;
+            continue;
+        }
         j.off = off;
         j.bytes = bytes;
         j.slot = slot;
@@ -134,19 +167,41 @@ int admit(sqs_server* s) {
             const int64_t sw = std::max<int64_t>(1, (-(int64_t)s->slice + j.job.n - 1) / j.job.n);
             j.jd.slice = (int)std::min<int64_t>((sw + xe - 1) / xe * xe, 1 << 30);
         }
-        std::vector<float4> init((size_t)job_pos_elems(j.job), make_float4(0.f, 0.f, 0.f, 0.f));
+        inits.emplace_back((size_t)job_pos_elems(j.job), make_float4(0.f, 0.f, 0.f, 0.f));
+        std::vector<float4>& init = inits.back();
         init_replicas(j.job, init.data());
         SQS_CUDA(cudaMemcpyAsync(s->arena + off, init.data(), sizeof(float4) * init.size(), cudaMemcpyHostToDevice,
                                  s->ctx->stream));
         SQS_CUDA(cudaMemcpyAsync(s->d_jd + slot, &j.jd, sizeof(JobDev), cudaMemcpyHostToDevice, s->ctx->stream));
         SQS_CUDA(cudaMemcpyAsync(s->d_jm + slot, &j.jm, sizeof(JobMut), cudaMemcpyHostToDevice, s->ctx->stream));
-        SQS_CUDA(cudaStreamSynchronize(s->ctx->stream));  // `init` is a host temporary
         s->slot_job[(size_t)slot] = j.id;
+        ++s->st.admitted;
         it = s->queue.erase(it);
     }
+    if (!inits.empty()) SQS_CUDA(cudaStreamSynchronize(s->ctx->stream));  // the staging vectors end here
     return SQS_OK;
 }
 
+}  // namespace
+
+namespace {
+// Release everything a server holds (after its streams are idle).
+void free_server(sqs_server* s) {
+    for (Cohort& c : s->cohorts) {
+        if (c.st) cudaStreamSynchronize(c.st);
+        if (c.st) cudaStreamDestroy(c.st);
+        if (c.done) cudaEventDestroy(c.done);
+        cudaFree(c.d_list);
+        cudaFree(c.d_status);
+        if (c.h_status) cudaFreeHost(c.h_status);
+    }
+    cudaFree(s->arena);
+    cudaFree(s->d_jd);
+    cudaFree(s->d_jm);
+    cudaFree(s->d_list);
+    sqs_ctx_destroy(s->rctx);
+    delete s;
+}
 }  // namespace
 
 extern "C" int sqs_server_create(sqs_ctx* ctx, size_t hbm_bytes, int max_active, int slice_sweeps,
@@ -165,17 +220,35 @@ extern "C" int sqs_server_create(sqs_ctx* ctx, size_t hbm_bytes, int max_active,
     if (e == cudaSuccess) e = cudaMalloc(&s->d_jd, sizeof(JobDev) * (size_t)max_active);
     if (e == cudaSuccess) e = cudaMalloc(&s->d_jm, sizeof(JobMut) * (size_t)max_active);
     if (e == cudaSuccess) e = cudaMalloc(&s->d_list, sizeof(int32_t) * (size_t)max_active);
+    // Retirement (polish, certification) gets its own context on a stream of
+    // the highest priority: its blocks are dispatched ahead of pending anneal
+    // blocks as SMs free up, so a finished job does not queue behind slices.
+    if (e == cudaSuccess) {
+        if (int r = sqs_ctx_create(ctx->device, &s->rctx)) {
+            free_server(s);
+            return r;
+        }
+        int least = 0, greatest = 0;
+        e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        if (e == cudaSuccess) e = cudaStreamDestroy(s->rctx->stream);
+        if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&s->rctx->stream, cudaStreamNonBlocking, greatest);
+    }
+    s->cohorts.resize(kCohorts);
+    for (Cohort& c : s->cohorts) {
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c.st, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaMalloc(&c.d_list, sizeof(int32_t) * (size_t)max_active);
+        if (e == cudaSuccess) e = cudaMalloc(&c.d_status, sizeof(int32_t) * (size_t)max_active);
+        if (e == cudaSuccess) e = cudaMallocHost(&c.h_status, sizeof(int32_t) * (size_t)max_active);
+    }
     if (e != cudaSuccess) {
         set_error("server set-up: %s", cudaGetErrorString(e));
-        cudaFree(s->arena);
-        cudaFree(s->d_jd);
-        cudaFree(s->d_jm);
-        cudaFree(s->d_list);
-        delete s;
+        free_server(s);
         return e == cudaErrorMemoryAllocation ? SQS_ENOMEM : SQS_ECUDA;
     }
     s->free_blocks[0] = s->arena_bytes;
     s->slot_job.assign((size_t)max_active, -1);
+    s->flying.assign((size_t)max_active, 0);
     s->h_jm.resize((size_t)max_active);
     *out = s;
     return SQS_OK;
@@ -185,11 +258,7 @@ extern "C" int sqs_server_destroy(sqs_server* s) {
     if (!s) return SQS_OK;
     cudaSetDevice(s->ctx->device);
     cudaStreamSynchronize(s->ctx->stream);
-    cudaFree(s->arena);
-    cudaFree(s->d_jd);
-    cudaFree(s->d_jm);
-    cudaFree(s->d_list);
-    delete s;
+    free_server(s);
     return SQS_OK;
 }
 
@@ -208,6 +277,7 @@ extern "C" int sqs_server_submit(sqs_server* s, const sqs_job* job, int64_t* id)
         j.job.xya_rep = j.xya_rep.data();
     }
     if (int r = prepare_job(j.job, 0, j.jd, j.jm, j.plan, &shape)) return r;
+    j.left = j.job.sweeps;
     SQS_REQUIRE(job_bytes(j.job) <= s->arena_bytes, "job state (%zu bytes) exceeds the server's HBM budget",
                 job_bytes(j.job));
     *id = j.id;
@@ -226,109 +296,203 @@ extern "C" int sqs_server_submit(sqs_server* s, const sqs_job* job, int64_t* id)
     return SQS_OK;
 }
 
-extern "C" int sqs_server_step(sqs_server* s, int* in_flight) {
-    SQS_REQUIRE(s != nullptr, "null server");
-    if (int r = enter(s->ctx)) return r;
-    if (int r = admit(s)) return r;
-    // one slice for every admitted job, one launch per cluster shape
-    std::map<std::tuple<int, int, int>, std::vector<int32_t>> groups;
-    std::map<std::tuple<int, int, int>, int64_t> rb;
+namespace {
+
+__global__ void gather_status_kernel(const int32_t* list, int count, const JobMut* jm, int32_t* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) out[i] = jm[list[i]].status;
+}
+
+int launch_gather_status(cudaStream_t st, int count, const int32_t* list, const JobMut* jm, int32_t* out) {
+    gather_status_kernel<<<(count + 127) / 128, 128, 0, st>>>(list, count, jm, out);
+    SQS_CUDA(cudaGetLastError());
+    return SQS_OK;
+}
+
+// A job's sweeps per slice: its own count under proposal slicing, else the server's.
+int job_slice(const sqs_server* s, const SJob& j) { return j.jd.slice > 0 ? j.jd.slice : std::max(1, s->slice); }
+
+// Collect the cohorts whose slice has finished: their jobs become idle again,
+// or go to `fin` when their budget is spent (or they failed or were cancelled).
+int harvest(sqs_server* s, std::vector<int32_t>& fin, int& got) {
+    got = 0;
+    for (Cohort& c : s->cohorts) {
+        if (!c.busy) continue;
+        const cudaError_t e = cudaEventQuery(c.done);
+        if (e == cudaErrorNotReady) continue;
+        if (e != cudaSuccess) {
+            set_error("anneal slice: %s", cudaGetErrorString(e));
+            return SQS_ECUDA;
+        }
+        c.busy = false;
+        ++got;
+        for (size_t i = 0; i < c.slots.size(); ++i) {
+            const int32_t k = c.slots[i];
+            s->flying[(size_t)k] = 0;
+            if (c.h_status[i] != kRunning || s->jobs[s->slot_job[(size_t)k]].cancel) fin.push_back(k);
+        }
+        c.slots.clear();
+    }
+    return SQS_OK;
+}
+
+// Start one slice for every idle job: one launch per cluster shape, each on a
+// free cohort stream, the jobs with the most work left first (in the launch
+// order and in the grid).  Returns the number of launches in `launched`.
+int launch_idle(sqs_server* s, const std::vector<int32_t>& fin, int& launched) {
+    launched = 0;
+    using Key = std::tuple<int, int, int>;
+    std::map<Key, std::vector<int32_t>> groups;
+    std::map<Key, int64_t> rb;
+    std::vector<uint8_t> retiring((size_t)s->max_active, 0);
+    for (int32_t k : fin) retiring[(size_t)k] = 1;
     for (int k = 0; k < s->max_active; ++k) {
-        if (s->slot_job[(size_t)k] < 0) continue;
+        if (s->slot_job[(size_t)k] < 0 || s->flying[(size_t)k] || retiring[(size_t)k]) continue;
         const SJob& j = s->jobs[s->slot_job[(size_t)k]];
-        const auto key = std::make_tuple(j.plan.cs, j.plan.Rl, (int)(j.jd.flags != 0));
+        const Key key = std::make_tuple(j.plan.cs, j.plan.Rl, (int)(j.jd.flags != 0));
         groups[key].push_back(k);
         rb[key] = std::max(rb[key], j.plan.rb);
     }
-    std::vector<int32_t> lists;
-    std::vector<std::pair<size_t, size_t>> spans;
-    for (auto& g : groups) {
-        spans.push_back({lists.size(), g.second.size()});
-        lists.insert(lists.end(), g.second.begin(), g.second.end());
-    }
-    if (!lists.empty()) {
-        SQS_CUDA(cudaMemcpyAsync(s->d_list, lists.data(), sizeof(int32_t) * lists.size(), cudaMemcpyHostToDevice,
-                                 s->ctx->stream));
-        std::vector<Group> launch;
-        size_t gi = 0;
-        for (auto& g : groups) {
-            launch.push_back(Group{(int)spans[gi].second, std::get<0>(g.first), std::get<1>(g.first),
-                                   (size_t)(rb[g.first] * std::get<1>(g.first)), s->d_list + spans[gi].first,
-                                   std::get<2>(g.first) != 0});
-            ++gi;
-        }
-        if (int r = launch_groups(s->ctx, launch, s->d_jd, s->d_jm, (float4*)s->arena, (double*)s->arena,
-                                  std::max(1, s->slice)))
-            return r;
-        s->ctx->launches += (int64_t)launch.size();
-        SQS_CUDA(cudaMemcpyAsync(s->h_jm.data(), s->d_jm, sizeof(JobMut) * (size_t)s->max_active,
-                                 cudaMemcpyDeviceToHost, s->ctx->stream));
-        SQS_CUDA(cudaStreamSynchronize(s->ctx->stream));
-    }
-    // retire the jobs whose budget is spent (or that failed, or were cancelled)
-    std::vector<int32_t> fin;
-    for (int k = 0; k < s->max_active; ++k) {
-        if (s->slot_job[(size_t)k] < 0) continue;
+    auto work = [&](int32_t k) {
         const SJob& j = s->jobs[s->slot_job[(size_t)k]];
-        if (s->h_jm[(size_t)k].status != kRunning || j.cancel) fin.push_back(k);
+        return j.left * (int64_t)j.job.n;
+    };
+    std::vector<std::pair<int64_t, Key>> order;
+    for (auto& g : groups) {
+        std::stable_sort(g.second.begin(), g.second.end(), [&](int32_t a, int32_t b) { return work(a) > work(b); });
+        order.push_back({work(g.second.front()), g.first});
+    }
+    std::stable_sort(order.begin(), order.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+    for (const auto& o : order) {
+        Cohort* c = nullptr;
+        for (Cohort& x : s->cohorts)
+            if (!x.busy) { c = &x; break; }
+        if (!c) break;  // every stream busy: the rest wait for the next step
+        const std::vector<int32_t>& list = groups[o.second];
+        const int cnt = (int)list.size();
+        SQS_CUDA(cudaMemcpyAsync(c->d_list, list.data(), sizeof(int32_t) * (size_t)cnt, cudaMemcpyHostToDevice, c->st));
+        if (int r = launch_anneal(c->st, cnt, std::get<0>(o.second), std::get<1>(o.second),
+                                  (size_t)(rb[o.second] * std::get<1>(o.second)), std::get<2>(o.second) != 0, c->d_list,
+                                  s->d_jd, s->d_jm, (float4*)s->arena, (double*)s->arena, std::max(1, s->slice)))
+            return r;
+        if (int r = launch_gather_status(c->st, cnt, c->d_list, s->d_jm, c->d_status)) return r;
+        SQS_CUDA(cudaMemcpyAsync(c->h_status, c->d_status, sizeof(int32_t) * (size_t)cnt, cudaMemcpyDeviceToHost, c->st));
+        SQS_CUDA(cudaEventRecord(c->done, c->st));
+        c->slots = list;
+        c->busy = true;
+        for (int32_t k : list) {
+            s->flying[(size_t)k] = 1;
+            SJob& j = s->jobs[s->slot_job[(size_t)k]];
+            j.left = std::max<int64_t>(0, j.left - job_slice(s, j));
+        }
+        s->ctx->launches += 2;
+        ++s->st.slices;
+        ++launched;
+    }
+    return SQS_OK;
+}
+
+// Polish, rescue and certify the finished jobs and free their slots and
+// arena space.  Runs on the retirement context's stream while the cohorts
+// anneal.
+int retire(sqs_server* s, const std::vector<int32_t>& fin) {
+    size_t psmem = 0;
+    for (int k : fin) psmem = std::max(psmem, polish_smem_bytes(s->jobs[s->slot_job[(size_t)k]].job.n));
+    SQS_CUDA(cudaMemcpyAsync(s->d_list, fin.data(), sizeof(int32_t) * fin.size(), cudaMemcpyHostToDevice,
+                             s->rctx->stream));
+    if (int r = launch_polish(s->rctx->stream, (int)fin.size(), s->d_list, s->d_jd, s->d_jm, (double*)s->arena, psmem))
+        return r;
+    s->rctx->launches += 1;
+    std::vector<std::vector<double>> best(fin.size());
+    for (size_t q = 0; q < fin.size(); ++q) {
+        SJob& j = s->jobs[s->slot_job[(size_t)fin[q]]];
+        best[q].resize(3 * (size_t)j.job.n);
+        SQS_CUDA(cudaMemcpyAsync(best[q].data(), (double*)s->arena + j.jd.best_off, sizeof(double) * best[q].size(),
+                                 cudaMemcpyDeviceToHost, s->rctx->stream));
+        SQS_CUDA(cudaMemcpyAsync(&s->h_jm[(size_t)fin[q]], s->d_jm + fin[q], sizeof(JobMut), cudaMemcpyDeviceToHost,
+                                 s->rctx->stream));
+    }
+    SQS_CUDA(cudaStreamSynchronize(s->rctx->stream));
+    {
+        std::vector<Rescue> rs;
+        for (size_t q = 0; q < fin.size(); ++q) {
+            SJob& j = s->jobs[s->slot_job[(size_t)fin[q]]];
+            if (!j.cancel) add_rescue(rs, j.job, j.jd, s->h_jm[(size_t)fin[q]], (const float4*)s->arena, best[q].data());
+        }
+        if (int r = rescue_uncertified(s->rctx, rs)) return r;
+    }
+    std::vector<int> ns;
+    std::vector<const double*> bptr;
+    std::vector<sqs_job_result*> optr;
+    std::vector<double*> xptr;
+    for (size_t q = 0; q < fin.size(); ++q) {
+        SJob& j = s->jobs[s->slot_job[(size_t)fin[q]]];
+        j.res = sqs_job_result{};
+        fill_result(j.job, j.jd, s->h_jm[(size_t)fin[q]], 0.f, j.res);
+        if (j.cancel) {
+            j.res.status = SQS_ENOTFOUND;
+            put(j.res.reason, sizeof j.res.reason, "cancelled");
+        }
+        j.best.assign(3 * (size_t)j.job.n, 0.0);
+        const JobMut& m = s->h_jm[(size_t)fin[q]];
+        if (!j.cancel && m.status != kErrCells && m.best_L < 1e29) {
+            ns.push_back(j.job.n);
+            bptr.push_back(best[q].data());
+            optr.push_back(&j.res);
+            xptr.push_back(j.best.data());
+        }
+    }
+    if (int r = certify_states(s->rctx, ns, bptr, optr, xptr)) return r;
+    for (int k : fin) {
+        SJob& j = s->jobs[s->slot_job[(size_t)k]];
+        arena_free(s, j.off, j.bytes);
+        j.state = kDone;
+        j.slot = -1;
+        s->slot_job[(size_t)k] = -1;
+    }
+    s->st.retired += (int64_t)fin.size();
+    return SQS_OK;
+}
+
+}  // namespace
+
+extern "C" int sqs_server_step(sqs_server* s, int* in_flight) {
+    SQS_REQUIRE(s != nullptr, "null server");
+    if (int r = enter(s->ctx)) return r;
+    ++s->st.steps;
+    auto t0 = std::chrono::steady_clock::now();
+    if (int r = admit(s)) return r;
+    s->st.admit_s += seconds_since(t0);
+    std::vector<int32_t> fin;
+    for (int k = 0; k < s->max_active; ++k)  // cancelled jobs between slices
+        if (s->slot_job[(size_t)k] >= 0 && !s->flying[(size_t)k] && s->jobs[s->slot_job[(size_t)k]].cancel)
+            fin.push_back(k);
+    int got = 0, launched = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+        t0 = std::chrono::steady_clock::now();
+        if (int r = harvest(s, fin, got)) return r;
+        if (int r = launch_idle(s, fin, launched)) return r;
+        s->st.launch_s += seconds_since(t0);
+        bool busy = false;
+        for (const Cohort& c : s->cohorts) busy = busy || c.busy;
+        if (pass == 1 || got || launched || !fin.empty() || !busy) break;
+        // nothing to do but wait: block until a slice finishes, at most
+        // kWaitSeconds, so that the caller can keep submitting meanwhile
+        t0 = std::chrono::steady_clock::now();
+        bool ready = false;
+        while (!ready && seconds_since(t0) < kWaitSeconds) {
+            for (const Cohort& c : s->cohorts) ready = ready || (c.busy && cudaEventQuery(c.done) != cudaErrorNotReady);
+            if (!ready) std::this_thread::sleep_for(std::chrono::microseconds(50));
+        }
+        s->st.wait_s += seconds_since(t0);
     }
     if (!fin.empty()) {
-        size_t psmem = 0;
-        for (int k : fin) psmem = std::max(psmem, polish_smem_bytes(s->jobs[s->slot_job[(size_t)k]].job.n));
-        SQS_CUDA(cudaMemcpyAsync(s->d_list, fin.data(), sizeof(int32_t) * fin.size(), cudaMemcpyHostToDevice,
-                                 s->ctx->stream));
-        if (int r = launch_polish(s->ctx->stream, (int)fin.size(), s->d_list, s->d_jd, s->d_jm, (double*)s->arena,
-                                  psmem))
-            return r;
-        s->ctx->launches += 1;
-        std::vector<std::vector<double>> best(fin.size());
-        for (size_t q = 0; q < fin.size(); ++q) {
-            SJob& j = s->jobs[s->slot_job[(size_t)fin[q]]];
-            best[q].resize(3 * (size_t)j.job.n);
-            SQS_CUDA(cudaMemcpyAsync(best[q].data(), (double*)s->arena + j.jd.best_off, sizeof(double) * best[q].size(),
-                                     cudaMemcpyDeviceToHost, s->ctx->stream));
-        }
-        SQS_CUDA(cudaMemcpyAsync(s->h_jm.data(), s->d_jm, sizeof(JobMut) * (size_t)s->max_active,
-                                 cudaMemcpyDeviceToHost, s->ctx->stream));
-        SQS_CUDA(cudaStreamSynchronize(s->ctx->stream));
-        {
-            std::vector<Rescue> rs;
-            for (size_t q = 0; q < fin.size(); ++q) {
-                SJob& j = s->jobs[s->slot_job[(size_t)fin[q]]];
-                if (!j.cancel)
-                    add_rescue(rs, j.job, j.jd, s->h_jm[(size_t)fin[q]], (const float4*)s->arena, best[q].data());
-            }
-            if (int r = rescue_uncertified(s->ctx, rs)) return r;
-        }
-        std::vector<int> ns;
-        std::vector<const double*> bptr;
-        std::vector<sqs_job_result*> optr;
-        std::vector<double*> xptr;
-        for (size_t q = 0; q < fin.size(); ++q) {
-            SJob& j = s->jobs[s->slot_job[(size_t)fin[q]]];
-            j.res = sqs_job_result{};
-            fill_result(j.job, j.jd, s->h_jm[(size_t)fin[q]], 0.f, j.res);
-            if (j.cancel) {
-                j.res.status = SQS_ENOTFOUND;
-                put(j.res.reason, sizeof j.res.reason, "cancelled");
-            }
-            j.best.assign(3 * (size_t)j.job.n, 0.0);
-            const JobMut& m = s->h_jm[(size_t)fin[q]];
-            if (!j.cancel && m.status != kErrCells && m.best_L < 1e29) {
-                ns.push_back(j.job.n);
-                bptr.push_back(best[q].data());
-                optr.push_back(&j.res);
-                xptr.push_back(j.best.data());
-            }
-        }
-        if (int r = certify_states(s->ctx, ns, bptr, optr, xptr)) return r;
-        for (int k : fin) {
-            SJob& j = s->jobs[s->slot_job[(size_t)k]];
-            arena_free(s, j.off, j.bytes);
-            j.state = kDone;
-            j.slot = -1;
-            s->slot_job[(size_t)k] = -1;
-        }
+        t0 = std::chrono::steady_clock::now();
+        const int64_t l0 = s->rctx->launches;
+        const int r = retire(s, fin);
+        s->ctx->launches += s->rctx->launches - l0;
+        if (r) return r;
+        s->st.retire_s += seconds_since(t0);
     }
     if (in_flight) {
         int active = 0;
@@ -380,5 +544,11 @@ extern "C" int sqs_server_info(sqs_server* s, int* queued, int* active, size_t* 
     if (queued) *queued = (int)s->queue.size();
     if (active) *active = a;
     if (hbm_used) *hbm_used = s->used;
+    return SQS_OK;
+}
+
+extern "C" int sqs_server_get_stats(sqs_server* s, sqs_server_stats* out) {
+    SQS_REQUIRE(s && out, "null argument");
+    *out = s->st;
     return SQS_OK;
 }

@@ -67,6 +67,12 @@ class PolishResult(C.Structure):
     _fields_ = [("L_in", C.c_double), ("L_out", C.c_double), ("iterations", C.c_int32), ("improved", C.c_int32)]
 
 
+class ServerStats(C.Structure):
+    """sqs_server_stats (include/sqs.h)."""
+    _fields_ = [("steps", C.c_int64), ("slices", C.c_int64), ("admitted", C.c_int64), ("retired", C.c_int64),
+                ("admit_s", C.c_double), ("launch_s", C.c_double), ("retire_s", C.c_double), ("wait_s", C.c_double)]
+
+
 JOB_AUTOTUNE = 1
 JOB_ADAPT = 2
 JOB_COLLECTIVE = 4
@@ -114,6 +120,7 @@ SIGNATURES: dict[str, tuple] = {
                                    C.POINTER(C.c_double), C.POINTER(PolishResult)]),
     "sqs_autotune": (C.c_int, [_vp, C.POINTER(Job), C.c_int, C.POINTER(Tuning)]),
     "sqs_server_info": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_size_t)]),
+    "sqs_server_get_stats": (C.c_int, [_vp, C.POINTER(ServerStats)]),
 }
 
 _LIB = None

@@ -83,6 +83,12 @@ class Server:
         N.check(N.lib().sqs_server_info(self.handle, C.byref(q), C.byref(a), C.byref(u)))
         return q.value, a.value, u.value
 
+    def stats(self) -> dict:
+        """Steps, slice launches, jobs admitted and retired, host seconds per phase."""
+        st = N.ServerStats()
+        N.check(N.lib().sqs_server_get_stats(self.handle, C.byref(st)))
+        return {name: getattr(st, name) for name, _ in N.ServerStats._fields_}
+
 
 def poisson_arrivals(count: int, rate: float, seed: int = 0) -> np.ndarray:
     rng = np.random.default_rng(seed)

@@ -24,7 +24,7 @@ def test_served_results_equal_alone(ctx):
         srv.step()                       # the first two are running ...
         ids += [srv.submit(j) for j in jobs[2:]]  # ... when the others arrive
         got = {}
-        for _ in range(200):
+        for _ in range(100000):
             if srv.step() == 0:
                 break
         for k, jid in enumerate(ids):
@@ -64,8 +64,10 @@ def test_cancel_and_unknown_ids(ctx):
         b = srv.submit(_job(20, 6, 200))
         srv.step()                 # a runs, b waits for the only slot
         srv.cancel(b)
-        srv.cancel(a)
-        srv.step()
+        srv.cancel(a)              # a stops when its slice in flight ends
+        for _ in range(100000):
+            if srv.step() == 0:
+                break
         ra, rb = srv.poll(a), srv.poll(b)
         assert ra["reason"] == "cancelled" and rb["reason"] == "cancelled"
         with pytest.raises(SQSError):
