@@ -312,9 +312,11 @@ int sqs_server_submit(sqs_server* server, const sqs_job* job, int64_t* id);
 /* One round of the loop: admit queued jobs; collect the slices that have
  * finished; start the next slice of every idle job (one launch per cluster
  * shape, each on its own stream, so slices of different jobs start and end
- * independently); polish, certify and retire the jobs whose budget is spent
- * while the other slices run.  When there is nothing to do it waits up to
- * 2 ms for a slice to finish.  *in_flight = queued + running. */
+ * independently); hand the jobs whose budget is spent to the server's
+ * retirement thread, which polishes, certifies and retires them while the
+ * slices run.  When there is nothing to do it waits up to 2 ms for a slice
+ * or a retirement to finish.  *in_flight = queued + running + retiring.
+ * Server calls come from one thread at a time, as for a context. */
 int sqs_server_step(sqs_server* server, int* in_flight);
 /* 1 and the result (and n*3 packing into xya_out when certified) once the
  * job is done -- the job is then forgotten; 0 while it is queued or running;
@@ -325,10 +327,11 @@ int sqs_server_poll(sqs_server* server, int64_t id, sqs_job_result* out, double*
 int sqs_server_cancel(sqs_server* server, int64_t id);
 int sqs_server_info(sqs_server* server, int* queued, int* active, size_t* hbm_used);
 /* Counters since the server's creation: steps, slice launches, jobs
- * admitted and retired, and the host wall seconds of each phase of the steps
- * -- admission (state upload), harvesting finished slices and launching new
- * ones, retirement (polish, rescue, certification, while other slices run)
- * and waiting for a slice to finish when there was nothing else to do. */
+ * admitted and retired, and host wall seconds -- of the steps' admission
+ * (state upload), of harvesting finished slices and launching new ones, of
+ * waiting when there was nothing else to do, and of retirement (polish,
+ * rescue, certification), which runs on the server's own thread while the
+ * steps go on. */
 typedef struct sqs_server_stats {
     int64_t steps, slices, admitted, retired;
     double admit_s, launch_s, retire_s, wait_s;

@@ -12,9 +12,10 @@
 //              admitted at different times, at different sweep counts, run side
 //              by side, their state resident in HBM between slices, and no
 //              cohort waits for another (no barrier across the GPU per round);
-//              polish, certify and retire the jobs whose budget ran out, on a
-//              stream of the highest priority while the cohorts anneal, and
-//              give their slot and arena space to the next;
+//              hand the jobs whose budget ran out to the retirement thread,
+//              which polishes, certifies and retires them on a stream of the
+//              highest priority while the cohorts anneal, and gives their slot
+//              and arena space to the next;
 //   poll     hands back a finished job's result and best packing.
 // A job's result is the same here as alone through sqs_anneal_batch: its
 // trajectory depends on its inputs and seed only.
@@ -29,7 +30,10 @@
 #include <chrono>
 #include <cstring>
 #include <deque>
+#include <condition_variable>
 #include <map>
+#include <mutex>
+#include <string>
 #include <thread>
 #include <tuple>
 #include <unordered_map>
@@ -92,9 +96,19 @@ struct sqs_server {
     std::deque<int64_t> queue;
     std::unordered_map<int64_t, SJob> jobs;
     int64_t next_id = 1;
-    std::vector<JobMut> h_jm;
     std::vector<uint8_t> flying;           // per slot: in a cohort's slice now
+    std::vector<uint8_t> retiring;         // per slot: handed to the retirement thread
     std::vector<Cohort> cohorts;
+    // The retirement thread and what it shares with the caller's thread
+    // (jobs, slots, arena, counters), guarded by `mu`.
+    std::mutex mu;
+    std::condition_variable cv;
+    std::deque<std::vector<int32_t>> rq;   // batches of finished slots, in order
+    int64_t retire_pending = 0;            // batches queued or being retired
+    bool stop = false;
+    int werr = 0;
+    std::string werr_msg;
+    std::thread worker;
     size_t used = 0;
     sqs_server_stats st{};
 };
@@ -185,8 +199,18 @@ int admit(sqs_server* s) {
 }  // namespace
 
 namespace {
+void retire_loop(sqs_server* s);
+
 // Release everything a server holds (after its streams are idle).
 void free_server(sqs_server* s) {
+    if (s->worker.joinable()) {
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->stop = true;
+        }
+        s->cv.notify_all();
+        s->worker.join();
+    }
     for (Cohort& c : s->cohorts) {
         if (c.st) cudaStreamSynchronize(c.st);
         if (c.st) cudaStreamDestroy(c.st);
@@ -249,7 +273,8 @@ extern "C" int sqs_server_create(sqs_ctx* ctx, size_t hbm_bytes, int max_active,
     s->free_blocks[0] = s->arena_bytes;
     s->slot_job.assign((size_t)max_active, -1);
     s->flying.assign((size_t)max_active, 0);
-    s->h_jm.resize((size_t)max_active);
+    s->retiring.assign((size_t)max_active, 0);
+    s->worker = std::thread(retire_loop, s);
     *out = s;
     return SQS_OK;
 }
@@ -283,6 +308,7 @@ extern "C" int sqs_server_submit(sqs_server* s, const sqs_job* job, int64_t* id)
     *id = j.id;
     ++s->next_id;
     const int64_t key = j.id;
+    std::lock_guard<std::mutex> lk(s->mu);
     s->jobs.emplace(key, std::move(j));
     SJob& stored = s->jobs[key];
     stored.job.xya = stored.xya.data();  // the vectors moved with the record
@@ -347,7 +373,7 @@ int launch_idle(sqs_server* s, const std::vector<int32_t>& fin, int& launched) {
     std::vector<uint8_t> retiring((size_t)s->max_active, 0);
     for (int32_t k : fin) retiring[(size_t)k] = 1;
     for (int k = 0; k < s->max_active; ++k) {
-        if (s->slot_job[(size_t)k] < 0 || s->flying[(size_t)k] || retiring[(size_t)k]) continue;
+        if (s->slot_job[(size_t)k] < 0 || s->flying[(size_t)k] || retiring[(size_t)k] || s->retiring[(size_t)k]) continue;
         const SJob& j = s->jobs[s->slot_job[(size_t)k]];
         const Key key = std::make_tuple(j.plan.cs, j.plan.Rl, (int)(j.jd.flags != 0));
         groups[key].push_back(k);
@@ -393,65 +419,107 @@ int launch_idle(sqs_server* s, const std::vector<int32_t>& fin, int& launched) {
 }
 
 // Polish, rescue and certify the finished jobs and free their slots and
-// arena space.  Runs on the retirement context's stream while the cohorts
-// anneal.
+// arena space.  Runs on the retirement thread, on the retirement context's
+// stream, while the caller's thread keeps the cohorts going.  The lock is
+// taken only to look the jobs up and to publish the results; in between the
+// thread reads job fields that nothing changes while a job is active.
 int retire(sqs_server* s, const std::vector<int32_t>& fin) {
+    std::vector<SJob*> jobs;
+    std::vector<uint8_t> cancel;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (int32_t k : fin) {
+            SJob* j = &s->jobs[s->slot_job[(size_t)k]];
+            jobs.push_back(j);
+            cancel.push_back(j->cancel ? 1 : 0);
+        }
+    }
+    const int64_t l0 = s->rctx->launches;
     size_t psmem = 0;
-    for (int k : fin) psmem = std::max(psmem, polish_smem_bytes(s->jobs[s->slot_job[(size_t)k]].job.n));
+    for (const SJob* j : jobs) psmem = std::max(psmem, polish_smem_bytes(j->job.n));
     SQS_CUDA(cudaMemcpyAsync(s->d_list, fin.data(), sizeof(int32_t) * fin.size(), cudaMemcpyHostToDevice,
                              s->rctx->stream));
     if (int r = launch_polish(s->rctx->stream, (int)fin.size(), s->d_list, s->d_jd, s->d_jm, (double*)s->arena, psmem))
         return r;
     s->rctx->launches += 1;
-    std::vector<std::vector<double>> best(fin.size());
+    std::vector<std::vector<double>> best(fin.size()), out(fin.size());
+    std::vector<JobMut> jm(fin.size());
     for (size_t q = 0; q < fin.size(); ++q) {
-        SJob& j = s->jobs[s->slot_job[(size_t)fin[q]]];
-        best[q].resize(3 * (size_t)j.job.n);
-        SQS_CUDA(cudaMemcpyAsync(best[q].data(), (double*)s->arena + j.jd.best_off, sizeof(double) * best[q].size(),
-                                 cudaMemcpyDeviceToHost, s->rctx->stream));
-        SQS_CUDA(cudaMemcpyAsync(&s->h_jm[(size_t)fin[q]], s->d_jm + fin[q], sizeof(JobMut), cudaMemcpyDeviceToHost,
-                                 s->rctx->stream));
+        best[q].resize(3 * (size_t)jobs[q]->job.n);
+        SQS_CUDA(cudaMemcpyAsync(best[q].data(), (double*)s->arena + jobs[q]->jd.best_off,
+                                 sizeof(double) * best[q].size(), cudaMemcpyDeviceToHost, s->rctx->stream));
+        SQS_CUDA(cudaMemcpyAsync(&jm[q], s->d_jm + fin[q], sizeof(JobMut), cudaMemcpyDeviceToHost, s->rctx->stream));
     }
     SQS_CUDA(cudaStreamSynchronize(s->rctx->stream));
     {
         std::vector<Rescue> rs;
-        for (size_t q = 0; q < fin.size(); ++q) {
-            SJob& j = s->jobs[s->slot_job[(size_t)fin[q]]];
-            if (!j.cancel) add_rescue(rs, j.job, j.jd, s->h_jm[(size_t)fin[q]], (const float4*)s->arena, best[q].data());
-        }
+        for (size_t q = 0; q < fin.size(); ++q)
+            if (!cancel[q]) add_rescue(rs, jobs[q]->job, jobs[q]->jd, jm[q], (const float4*)s->arena, best[q].data());
         if (int r = rescue_uncertified(s->rctx, rs)) return r;
     }
+    std::vector<sqs_job_result> res(fin.size());
     std::vector<int> ns;
     std::vector<const double*> bptr;
     std::vector<sqs_job_result*> optr;
     std::vector<double*> xptr;
     for (size_t q = 0; q < fin.size(); ++q) {
-        SJob& j = s->jobs[s->slot_job[(size_t)fin[q]]];
-        j.res = sqs_job_result{};
-        fill_result(j.job, j.jd, s->h_jm[(size_t)fin[q]], 0.f, j.res);
-        if (j.cancel) {
-            j.res.status = SQS_ENOTFOUND;
-            put(j.res.reason, sizeof j.res.reason, "cancelled");
+        fill_result(jobs[q]->job, jobs[q]->jd, jm[q], 0.f, res[q]);
+        if (cancel[q]) {
+            res[q].status = SQS_ENOTFOUND;
+            put(res[q].reason, sizeof res[q].reason, "cancelled");
         }
-        j.best.assign(3 * (size_t)j.job.n, 0.0);
-        const JobMut& m = s->h_jm[(size_t)fin[q]];
-        if (!j.cancel && m.status != kErrCells && m.best_L < 1e29) {
-            ns.push_back(j.job.n);
+        out[q].assign(3 * (size_t)jobs[q]->job.n, 0.0);
+        if (!cancel[q] && jm[q].status != kErrCells && jm[q].best_L < 1e29) {
+            ns.push_back(jobs[q]->job.n);
             bptr.push_back(best[q].data());
-            optr.push_back(&j.res);
-            xptr.push_back(j.best.data());
+            optr.push_back(&res[q]);
+            xptr.push_back(out[q].data());
         }
     }
     if (int r = certify_states(s->rctx, ns, bptr, optr, xptr)) return r;
-    for (int k : fin) {
-        SJob& j = s->jobs[s->slot_job[(size_t)k]];
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (size_t q = 0; q < fin.size(); ++q) {
+        SJob& j = *jobs[q];
+        j.res = res[q];
+        j.best = std::move(out[q]);
         arena_free(s, j.off, j.bytes);
         j.state = kDone;
         j.slot = -1;
-        s->slot_job[(size_t)k] = -1;
+        s->slot_job[(size_t)fin[q]] = -1;
+        s->retiring[(size_t)fin[q]] = 0;
     }
     s->st.retired += (int64_t)fin.size();
+    s->ctx->launches += s->rctx->launches - l0;
     return SQS_OK;
+}
+
+// The retirement thread: retires every batch of finished jobs queued by the
+// time it looks, as one batch (jobs that finish while a retirement runs are
+// retired together next); an error is kept and reported by the caller's
+// next step.
+void retire_loop(sqs_server* s) {
+    cudaSetDevice(s->ctx->device);
+    for (;;) {
+        std::vector<int32_t> fin;
+        int64_t batches = 0;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv.wait(lk, [&] { return s->stop || !s->rq.empty(); });
+            if (s->rq.empty()) return;  // asked to stop, nothing left
+            for (auto& b : s->rq) fin.insert(fin.end(), b.begin(), b.end());
+            batches = (int64_t)s->rq.size();
+            s->rq.clear();
+        }
+        const auto t0 = std::chrono::steady_clock::now();
+        const int r = retire(s, fin);
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (r && !s->werr) {
+            s->werr = r;
+            s->werr_msg = sqs_last_error();
+        }
+        s->st.retire_s += seconds_since(t0);
+        s->retire_pending -= batches;
+    }
 }
 
 }  // namespace
@@ -459,40 +527,53 @@ int retire(sqs_server* s, const std::vector<int32_t>& fin) {
 extern "C" int sqs_server_step(sqs_server* s, int* in_flight) {
     SQS_REQUIRE(s != nullptr, "null server");
     if (int r = enter(s->ctx)) return r;
+    std::unique_lock<std::mutex> lk(s->mu);
+    if (s->werr) {
+        set_error("%s", s->werr_msg.c_str());
+        return s->werr;
+    }
     ++s->st.steps;
     auto t0 = std::chrono::steady_clock::now();
     if (int r = admit(s)) return r;
     s->st.admit_s += seconds_since(t0);
     std::vector<int32_t> fin;
     for (int k = 0; k < s->max_active; ++k)  // cancelled jobs between slices
-        if (s->slot_job[(size_t)k] >= 0 && !s->flying[(size_t)k] && s->jobs[s->slot_job[(size_t)k]].cancel)
+        if (s->slot_job[(size_t)k] >= 0 && !s->flying[(size_t)k] && !s->retiring[(size_t)k] &&
+            s->jobs[s->slot_job[(size_t)k]].cancel)
             fin.push_back(k);
-    int got = 0, launched = 0;
     for (int pass = 0; pass < 2; ++pass) {
+        int got = 0, launched = 0;
+        const int64_t pend0 = s->retire_pending;
         t0 = std::chrono::steady_clock::now();
         if (int r = harvest(s, fin, got)) return r;
         if (int r = launch_idle(s, fin, launched)) return r;
         s->st.launch_s += seconds_since(t0);
+        if (!fin.empty()) {  // hand the finished jobs to the retirement thread
+            for (int32_t k : fin) s->retiring[(size_t)k] = 1;
+            s->rq.push_back(std::move(fin));
+            fin.clear();
+            ++s->retire_pending;
+            s->cv.notify_one();
+            break;
+        }
         bool busy = false;
         for (const Cohort& c : s->cohorts) busy = busy || c.busy;
-        if (pass == 1 || got || launched || !fin.empty() || !busy) break;
-        // nothing to do but wait: block until a slice finishes, at most
-        // kWaitSeconds, so that the caller can keep submitting meanwhile
+        if (pass == 1 || got || launched || (!busy && !pend0)) break;
+        // nothing to do but wait: until a slice or a retirement finishes, at
+        // most kWaitSeconds, so that the caller can keep submitting meanwhile
+        lk.unlock();
         t0 = std::chrono::steady_clock::now();
         bool ready = false;
         while (!ready && seconds_since(t0) < kWaitSeconds) {
             for (const Cohort& c : s->cohorts) ready = ready || (c.busy && cudaEventQuery(c.done) != cudaErrorNotReady);
-            if (!ready) std::this_thread::sleep_for(std::chrono::microseconds(50));
+            if (!ready) {
+                std::this_thread::sleep_for(std::chrono::microseconds(50));
+                std::lock_guard<std::mutex> g(s->mu);
+                ready = s->retire_pending != pend0;
+            }
         }
+        lk.lock();
         s->st.wait_s += seconds_since(t0);
-    }
-    if (!fin.empty()) {
-        t0 = std::chrono::steady_clock::now();
-        const int64_t l0 = s->rctx->launches;
-        const int r = retire(s, fin);
-        s->ctx->launches += s->rctx->launches - l0;
-        if (r) return r;
-        s->st.retire_s += seconds_since(t0);
     }
     if (in_flight) {
         int active = 0;
@@ -504,6 +585,7 @@ extern "C" int sqs_server_step(sqs_server* s, int* in_flight) {
 
 extern "C" int sqs_server_poll(sqs_server* s, int64_t id, sqs_job_result* out, double* xya_out) {
     SQS_REQUIRE(s != nullptr && out != nullptr, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
     auto it = s->jobs.find(id);
     if (it == s->jobs.end()) {
         set_error("job %lld unknown (never submitted, or already collected)", (long long)id);
@@ -519,6 +601,7 @@ extern "C" int sqs_server_poll(sqs_server* s, int64_t id, sqs_job_result* out, d
 
 extern "C" int sqs_server_cancel(sqs_server* s, int64_t id) {
     SQS_REQUIRE(s != nullptr, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
     auto it = s->jobs.find(id);
     if (it == s->jobs.end() || it->second.state == kDone) {
         set_error("job %lld is not queued or running", (long long)id);
@@ -539,6 +622,7 @@ extern "C" int sqs_server_cancel(sqs_server* s, int64_t id) {
 
 extern "C" int sqs_server_info(sqs_server* s, int* queued, int* active, size_t* hbm_used) {
     SQS_REQUIRE(s != nullptr, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
     int a = 0;
     for (int64_t id : s->slot_job) a += id >= 0;
     if (queued) *queued = (int)s->queue.size();
@@ -549,6 +633,7 @@ extern "C" int sqs_server_info(sqs_server* s, int* queued, int* active, size_t* 
 
 extern "C" int sqs_server_get_stats(sqs_server* s, sqs_server_stats* out) {
     SQS_REQUIRE(s && out, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
     *out = s->st;
     return SQS_OK;
 }
