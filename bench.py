@@ -423,7 +423,7 @@ def served_jobs(count: int):
 
 def bench_served(ctx, jobs, plain, rate: float):
     """Served vs plain at one Poisson arrival rate: a stream of about four
-    seconds (at least 40 jobs, at most all of them) through the
+    seconds of arrivals (at least 40 jobs, at most all of them) through the
     continuous-batching server; the plain comparator serves the same jobs one
     launch per job in arrival order, its service times measured once
     (`plain`), its latencies from those times and the same arrivals.  The
@@ -437,11 +437,12 @@ def bench_served(ctx, jobs, plain, rate: float):
     arr = poisson_arrivals(count, rate, seed=3)
     with Server(ctx, hbm_bytes=4 << 30, max_active=count, slice_proposals=4000) as srv:
         served, s_stats = run_stream(srv, sub, arr, timeout=600)
+        counters = srv.stats()
     p_res, p_service = plain
     p_stats = plain_stats(p_res[:count], p_service[:count], arr)
     same_L = all((a or {}).get("L") == (b or {}).get("L") for a, b in zip(served, p_res[:count]))
     return dict(workload=f"{count} jobs, Poisson {rate:g}/s, n log-uniform [5, 1000], 16/32/64 replicas, "
-                         f"200 sweeps", served=s_stats, plain=p_stats, equal_final_L=same_L,
+                         f"200 sweeps", served=s_stats, plain=p_stats, equal_final_L=same_L, server_counters=counters,
                 served_over_plain=s_stats["certified_jobs_per_s"] / max(p_stats["certified_jobs_per_s"], 1e-12))
 
 
@@ -471,7 +472,7 @@ def bench_plain_pt(ctx):
     return res
 
 
-def bench_served_sweep(ctx, rates: str, count: int = 240):
+def bench_served_sweep(ctx, rates: str, count: int = 960):
     from sqs.serve import plain_service
 
     rs = [float(x) for x in rates.split(",") if x]
