@@ -189,6 +189,14 @@ typedef struct sqs_job {
 #define SQS_JOB_ADAPT 2
 #define SQS_JOB_COLLECTIVE 4
 #define SQS_JOB_KICK 8
+/* Evaluate proposals strictly one at a time.  Without move-set options a
+ * replica's warp evaluates two consecutive proposals at once, one per
+ * half-warp, against the same state, and evaluates the second again when the
+ * first was accepted and moved something the second read (the same square,
+ * or a square or cell list inside its 3 x 3 cell block).  Energies are exact
+ * integers, so the trajectory is the one-at-a-time trajectory bit for bit;
+ * this flag changes only the time taken, and lets a caller check that. */
+#define SQS_JOB_SERIAL 16
 /* Pin the launch shape instead: a cluster of `cs` CTAs (1..16; it must
  * divide the replica count and fit) and cell side index k (0: 1.59, 1: 1.75,
  * 2: 1.95, 3: 2.2).  Same trajectory as any other shape (see above). */

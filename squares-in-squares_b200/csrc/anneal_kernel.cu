@@ -110,8 +110,9 @@ __device__ bool build_cells(const Rep& R, int n, const Grid& g, int lane) {
 }
 
 // Visit the squares of the 3x3 cell block around (cx, cy): returns through
-// `fn(j)` for every candidate t = lane, lane + 32, ...
-template <typename Fn>
+// `fn(j)` for every candidate t = lane, lane + kStride, ... (kStride lanes
+// share the block: the whole warp, or one half of it).
+template <int kStride = 32, typename Fn>
 __device__ __forceinline__ void for_block(const Rep& R, const Grid& g, int cx, int cy, int lane, Fn&& fn) {
     // Every lane reads the nine cell counts (broadcast shared loads) and
     // forms their running sum; slot t of the block belongs to the first cell
@@ -127,7 +128,7 @@ __device__ __forceinline__ void for_block(const Rep& R, const Grid& g, int cx, i
         run += in ? (int)R.cnt[y * g.G + x] : 0;
         ends[c] = run;
     }
-    for (int t = lane; t < run; t += 32) {
+    for (int t = lane; t < run; t += kStride) {
         int c = 0, start = 0;
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
@@ -758,7 +759,25 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                     if (MOVES && (jd.flags & kMoveCollective)) di |= (int)(rb.z % 7u) << 16;  // move mode
                 }
                 const int kn = min(32, n - kb);
-                for (int q = 0; q < kn; ++q) {
+                // one lane moves square i to its new state and cell
+                auto apply_move = [&](int i, float nx, float ny, float nc, float ns, float na, int oc, int ncell) {
+                    rep.sq[i] = make_float4(nx, ny, nc, ns);
+                    rep.ang[i] = na;
+                    if (oc != ncell) {
+                        const int m = rep.cnt[oc];
+                        for (int t = 0; t < m; ++t) {
+                            if (rep.slot[oc * kCellK + t] == (uint16_t)i) {
+                                rep.slot[oc * kCellK + t] = rep.slot[oc * kCellK + m - 1];
+                                break;
+                            }
+                        }
+                        rep.cnt[oc] = (uint8_t)(m - 1);
+                        rep.slot[ncell * kCellK + rep.cnt[ncell]] = (uint16_t)i;
+                        rep.cnt[ncell] = (uint8_t)(rep.cnt[ncell] + 1);
+                    }
+                };
+                // proposal q of this batch, evaluated by the whole warp
+                auto single = [&](int q) {
                     const int dpk = __shfl_sync(0xffffffffu, di, q);
                     const int i = dpk & 0xffff, mode = dpk >> 16;
                     const float sdx = __shfl_sync(0xffffffffu, ddx, q), sdy = __shfl_sync(0xffffffffu, ddy, q);
@@ -813,22 +832,7 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                     if (acc) {
                         ++accs;
                         E += dq;
-                        if (lane == 0) {
-                            rep.sq[i] = make_float4(nx, ny, nc, ns);
-                            rep.ang[i] = na;
-                            if (oc != ncell) {
-                                const int m = rep.cnt[oc];
-                                for (int q = 0; q < m; ++q) {
-                                    if (rep.slot[oc * kCellK + q] == (uint16_t)i) {
-                                        rep.slot[oc * kCellK + q] = rep.slot[oc * kCellK + m - 1];
-                                        break;
-                                    }
-                                }
-                                rep.cnt[oc] = (uint8_t)(m - 1);
-                                rep.slot[ncell * kCellK + rep.cnt[ncell]] = (uint16_t)i;
-                                rep.cnt[ncell] = (uint8_t)(rep.cnt[ncell] + 1);
-                            }
-                        }
+                        if (lane == 0) apply_move(i, nx, ny, nc, ns, na, oc, ncell);
                     }
                     }
                     if (adaptive) {  // every 16 proposals: steer toward 25% acceptance
@@ -839,6 +843,94 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                         }
                     }
                     __syncwarp();
+                };
+                // Proposals q and q + 1 evaluated at once, one per half-warp,
+                // both against the current state.  Proposal q is decided as
+                // usual.  Proposal q + 1's result stands unless q was accepted
+                // and its move touched what q + 1 read: the same square, or an
+                // old or new cell of q inside q + 1's 3x3 block (cells are wider
+                // than a step, so a move changes a square's cell by at most one;
+                // every other read -- counts and slots of the block, squares in
+                // it, the count of q + 1's target cell -- lies in that block).
+                // Then it is evaluated again by the whole warp after q's move.
+                // Energies are exact and order-free, so the trajectory is the
+                // one-at-a-time trajectory, bit for bit.
+                auto paired = [&](int q) {
+                    const int half = lane >> 4, hl = lane & 15;
+                    const int qs = q + half;
+                    const int i = __shfl_sync(0xffffffffu, di, qs) & 0xffff;
+                    const float sdx = __shfl_sync(0xffffffffu, ddx, qs), sdy = __shfl_sync(0xffffffffu, ddy, qs);
+                    const float sda = __shfl_sync(0xffffffffu, dda, qs), u_acc = __shfl_sync(0xffffffffu, du, qs);
+                    const float dx = fminf(kMaxStep, fmaxf(-kMaxStep, sdx));
+                    const float dy = fminf(kMaxStep, fmaxf(-kMaxStep, sdy));
+                    const float4 P = rep.sq[i];
+                    const float nx = fminf(fmaxf(P.x, L - 0.5f), fmaxf(fminf(P.x, 0.5f), P.x + dx));
+                    const float ny = fminf(fmaxf(P.y, L - 0.5f), fmaxf(fminf(P.y, 0.5f), P.y + dy));
+                    float na = rep.ang[i] + sda;
+                    na = na - kHalfPiF * floorf(na * (1.0f / kHalfPiF));
+                    if (!(na >= 0.f && na < kHalfPiF)) na = 0.f;
+                    float ns, nc;
+                    state_trig(na, &ns, &nc);
+                    const int ocx = g.cx(P.x), ocy = g.cx(P.y);
+                    long long dq = 0;
+                    if (hl == 0) dq = qe(wall_e(nx, ny, nc, ns, L)) - qe(wall_e(P.x, P.y, P.z, P.w, L));
+                    for_block<16>(rep, g, ocx, ocy, hl, [&](int j) {
+                        if (j == i) return;
+                        const float4 Q = rep.sq[j];
+                        const float ex = Q.x - nx, ey = Q.y - ny;
+                        if (ex * ex + ey * ey < kPairCut2) dq += qe(sat_pair_energy(ex, ey, nc, ns, Q.z, Q.w));
+                        const float fx = Q.x - P.x, fy = Q.y - P.y;
+                        if (fx * fx + fy * fy < kPairCut2) dq -= qe(sat_pair_energy(fx, fy, P.z, P.w, Q.z, Q.w));
+                    });
+                    const long long dA = warp_sum_dq(half == 0 ? dq : 0);
+                    const long long dB = warp_sum_dq(half == 0 ? 0 : dq);
+                    const long long mine = half == 0 ? dA : dB;
+                    const float de = (float)mine * (1.0f / kEScale);
+                    const int ncx = g.cx(nx), ncy = g.cx(ny);
+                    const int oc = ocy * g.G + ocx, ncell = ncy * g.G + ncx;
+                    int acc = mine <= 0 || u_acc < __expf(-de * invT);
+                    int ov = 0;
+                    if (acc && oc != ncell && rep.cnt[ncell] >= kCellK) {
+                        acc = 0;
+                        ov = 1;
+                    }
+                    const int accA = __shfl_sync(0xffffffffu, acc, 0), ovA = __shfl_sync(0xffffffffu, ov, 0);
+                    const int accB = __shfl_sync(0xffffffffu, acc, 16), ovB = __shfl_sync(0xffffffffu, ov, 16);
+                    const int iA = __shfl_sync(0xffffffffu, i, 0), iB = __shfl_sync(0xffffffffu, i, 16);
+                    const int axo = __shfl_sync(0xffffffffu, ocx, 0), ayo = __shfl_sync(0xffffffffu, ocy, 0);
+                    const int axn = __shfl_sync(0xffffffffu, ncx, 0), ayn = __shfl_sync(0xffffffffu, ncy, 0);
+                    const int bx = __shfl_sync(0xffffffffu, ocx, 16), by = __shfl_sync(0xffffffffu, ocy, 16);
+                    ++props;
+                    accs += accA;
+                    ovf += ovA;
+                    if (accA) E += dA;
+                    if (accA && lane == 0) apply_move(i, nx, ny, nc, ns, na, oc, ncell);
+                    const bool redo = accA && (iA == iB || (abs(axo - bx) <= 1 && abs(ayo - by) <= 1) ||
+                                               (abs(axn - bx) <= 1 && abs(ayn - by) <= 1));
+                    __syncwarp();
+                    if (redo) {
+                        single(q + 1);
+                    } else {
+                        ++props;
+                        accs += accB;
+                        ovf += ovB;
+                        if (accB) E += dB;
+                        if (accB && lane == 16) apply_move(i, nx, ny, nc, ns, na, oc, ncell);
+                        __syncwarp();
+                    }
+                };
+                // pairs need room: on grids below 4 x 4 almost every pair would
+                // be evaluated twice; the move-set instance keeps one at a time
+                // (its step scale follows the acceptance of the previous move)
+                const bool pairs = !MOVES && g.G >= 4;
+                for (int q = 0; q < kn;) {
+                    if (pairs && q + 1 < kn) {
+                        paired(q);
+                        q += 2;
+                    } else {
+                        single(q);
+                        ++q;
+                    }
                 }
             }
         }

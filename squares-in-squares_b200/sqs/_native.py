@@ -77,6 +77,7 @@ JOB_AUTOTUNE = 1
 JOB_ADAPT = 2
 JOB_COLLECTIVE = 4
 JOB_KICK = 8
+JOB_SERIAL = 16
 TUNE_LATENCY = 1
 
 

@@ -121,3 +121,27 @@ def test_job_without_a_certified_state_is_rescued(ctx, oracle):
         served = srv.poll(jid)
     for k in KEYS:
         assert mixed[k] == r[k] and served[k] == r[k], k
+
+
+def test_paired_proposals_equal_one_at_a_time(ctx):
+    """Plain jobs evaluate two proposals at once (one per half-warp) and
+    evaluate the second again when the first's accepted move touched what it
+    read.  The trajectory must be the one-at-a-time trajectory (SQS_JOB_SERIAL)
+    bit for bit, on grids from 4 x 4 cells up, alone and batched, in every
+    launch shape."""
+    from sqs.anneal import anneal_batch
+    cases = [dict(n=20, replicas=8, sweeps=300), dict(n=60, replicas=16, sweeps=200),
+             dict(n=200, replicas=32, sweeps=60), dict(n=500, replicas=16, sweeps=20),
+             dict(n=976, replicas=16, sweeps=10), dict(n=130, replicas=64, sweeps=40, cluster=8)]
+    jobs = [plain_job(seed=50 + k, polish_iters=20, **c) for k, c in enumerate(cases)]
+    serial = [plain_job(seed=50 + k, polish_iters=20, serial=True, **c) for k, c in enumerate(cases)]
+    batched = anneal_batch(jobs, ctx=ctx)
+    alone_serial = [anneal_batch([j], ctx=ctx)[0] for j in serial]
+    for k, (a, b) in enumerate(zip(batched, alone_serial)):
+        assert a["accepted"] > 0, k
+        for key in KEYS:
+            assert a[key] == b[key], (cases[k], key)
+    # another shape of the 200-square job, paired, still the same
+    other = anneal_batch([plain_job(seed=52, polish_iters=20, cluster=4, **cases[2])], ctx=ctx)[0]
+    for key in KEYS:
+        assert other[key] == alone_serial[2][key], key
