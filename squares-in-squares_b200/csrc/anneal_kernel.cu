@@ -656,6 +656,27 @@ struct CtaShared {
 
 // MOVES: whether the move-set options (adaptation, collective moves, kicks)
 // are compiled in; jobs without them run the leaner instance.
+template <int V>
+struct IntTag {
+    static constexpr int value = V;
+};
+
+// A proposal's move: the square (-1: nothing moved) and its old and new
+// cells, one byte per coordinate (grids are at most 64 / 1.59 < 256 wide).
+struct Moved {
+    int i, cells;
+};
+__device__ __forceinline__ int pack_cells(int ox, int oy, int nx, int ny) {
+    return ox | (oy << 8) | (nx << 16) | (ny << 24);
+}
+// Did move (mi, mc) change what a proposal of square ik from cells ck read?
+__device__ __forceinline__ bool touches(int mi, int mc, int ik, int ck) {
+    if (mi < 0) return false;
+    const int bx = ck & 0xff, by = (ck >> 8) & 0xff;
+    const int ox = mc & 0xff, oy = (mc >> 8) & 0xff, nx = (mc >> 16) & 0xff, ny = (int)((unsigned)mc >> 24);
+    return mi == ik || (abs(ox - bx) <= 1 && abs(oy - by) <= 1) || (abs(nx - bx) <= 1 && abs(ny - by) <= 1);
+}
+
 template <bool MOVES>
 __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __restrict__ job_list,
                                                       const JobDev* __restrict__ jdev, JobMut* __restrict__ jmut,
@@ -776,8 +797,10 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                         rep.cnt[ncell] = (uint8_t)(rep.cnt[ncell] + 1);
                     }
                 };
-                // proposal q of this batch, evaluated by the whole warp
-                auto single = [&](int q) {
+                // proposal q of this batch, evaluated by the whole warp; returns
+                // the square it moved (-1: none) and its old and new cells
+                auto single = [&](int q) -> Moved {
+                    Moved mv{-1, 0};
                     const int dpk = __shfl_sync(0xffffffffu, di, q);
                     const int i = dpk & 0xffff, mode = dpk >> 16;
                     const float sdx = __shfl_sync(0xffffffffu, ddx, q), sdy = __shfl_sync(0xffffffffu, ddy, q);
@@ -833,6 +856,7 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                         ++accs;
                         E += dq;
                         if (lane == 0) apply_move(i, nx, ny, nc, ns, na, oc, ncell);
+                        mv = Moved{i, pack_cells(ocx, ocy, ncx, ncy)};
                     }
                     }
                     if (adaptive) {  // every 16 proposals: steer toward 25% acceptance
@@ -843,21 +867,24 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                         }
                     }
                     __syncwarp();
+                    return mv;
                 };
-                // Proposals q and q + 1 evaluated at once, one per half-warp,
-                // both against the current state.  Proposal q is decided as
-                // usual.  Proposal q + 1's result stands unless q was accepted
-                // and its move touched what q + 1 read: the same square, or an
-                // old or new cell of q inside q + 1's 3x3 block (cells are wider
-                // than a step, so a move changes a square's cell by at most one;
-                // every other read -- counts and slots of the block, squares in
-                // it, the count of q + 1's target cell -- lies in that block).
-                // Then it is evaluated again by the whole warp after q's move.
-                // Energies are exact and order-free, so the trajectory is the
-                // one-at-a-time trajectory, bit for bit.
-                auto paired = [&](int q) {
-                    const int half = lane >> 4, hl = lane & 15;
-                    const int qs = q + half;
+                // Proposals q .. q + M - 1 evaluated at once, one per group of
+                // 32 / M lanes, all against the current state, then decided in
+                // order.  A proposal's result stands unless an earlier move of
+                // the group that was accepted touched what it read: the same
+                // square, or an old or new cell of that move inside its 3x3
+                // block (cells are wider than a step, so a move changes a
+                // square's cell by at most one; every other read -- counts and
+                // slots of the block, squares in it, the count of its target
+                // cell -- lies in that block).  Then the whole warp evaluates it
+                // again on the current state.  Energies are exact and
+                // order-free, so the trajectory is the one-at-a-time trajectory,
+                // bit for bit.
+                auto group = [&](int q, auto mtag) {
+                    constexpr int M = decltype(mtag)::value, W = 32 / M;
+                    const int grp = lane / W, gl = lane % W;
+                    const int qs = q + grp;
                     const int i = __shfl_sync(0xffffffffu, di, qs) & 0xffff;
                     const float sdx = __shfl_sync(0xffffffffu, ddx, qs), sdy = __shfl_sync(0xffffffffu, ddy, qs);
                     const float sda = __shfl_sync(0xffffffffu, dda, qs), u_acc = __shfl_sync(0xffffffffu, du, qs);
@@ -873,8 +900,8 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                     state_trig(na, &ns, &nc);
                     const int ocx = g.cx(P.x), ocy = g.cx(P.y);
                     long long dq = 0;
-                    if (hl == 0) dq = qe(wall_e(nx, ny, nc, ns, L)) - qe(wall_e(P.x, P.y, P.z, P.w, L));
-                    for_block<16>(rep, g, ocx, ocy, hl, [&](int j) {
+                    if (gl == 0) dq = qe(wall_e(nx, ny, nc, ns, L)) - qe(wall_e(P.x, P.y, P.z, P.w, L));
+                    for_block<W>(rep, g, ocx, ocy, gl, [&](int j) {
                         if (j == i) return;
                         const float4 Q = rep.sq[j];
                         const float ex = Q.x - nx, ey = Q.y - ny;
@@ -882,9 +909,16 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                         const float fx = Q.x - P.x, fy = Q.y - P.y;
                         if (fx * fx + fy * fy < kPairCut2) dq -= qe(sat_pair_energy(fx, fy, P.z, P.w, Q.z, Q.w));
                     });
-                    const long long dA = warp_sum_dq(half == 0 ? dq : 0);
-                    const long long dB = warp_sum_dq(half == 0 ? 0 : dq);
-                    const long long mine = half == 0 ? dA : dB;
+                    // exact sum over the group's lanes: hi * 2^20 + lo parts
+                    // (a lane's term is below 2^46, so both parts stay in 32 bits)
+                    int hi = (int)(dq >> 20);
+                    unsigned lo = (unsigned)(dq & 0xFFFFF);
+#pragma unroll
+                    for (int off = W / 2; off > 0; off >>= 1) {
+                        hi += __shfl_xor_sync(0xffffffffu, hi, off);
+                        lo += __shfl_xor_sync(0xffffffffu, lo, off);
+                    }
+                    const long long mine = (long long)hi * 1048576ll + (long long)lo;
                     const float de = (float)mine * (1.0f / kEScale);
                     const int ncx = g.cx(nx), ncy = g.cx(ny);
                     const int oc = ocy * g.G + ocx, ncell = ncy * g.G + ncx;
@@ -894,38 +928,44 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                         acc = 0;
                         ov = 1;
                     }
-                    const int accA = __shfl_sync(0xffffffffu, acc, 0), ovA = __shfl_sync(0xffffffffu, ov, 0);
-                    const int accB = __shfl_sync(0xffffffffu, acc, 16), ovB = __shfl_sync(0xffffffffu, ov, 16);
-                    const int iA = __shfl_sync(0xffffffffu, i, 0), iB = __shfl_sync(0xffffffffu, i, 16);
-                    const int axo = __shfl_sync(0xffffffffu, ocx, 0), ayo = __shfl_sync(0xffffffffu, ocy, 0);
-                    const int axn = __shfl_sync(0xffffffffu, ncx, 0), ayn = __shfl_sync(0xffffffffu, ncy, 0);
-                    const int bx = __shfl_sync(0xffffffffu, ocx, 16), by = __shfl_sync(0xffffffffu, ocy, 16);
-                    ++props;
-                    accs += accA;
-                    ovf += ovA;
-                    if (accA) E += dA;
-                    if (accA && lane == 0) apply_move(i, nx, ny, nc, ns, na, oc, ncell);
-                    const bool redo = accA && (iA == iB || (abs(axo - bx) <= 1 && abs(ayo - by) <= 1) ||
-                                               (abs(axn - bx) <= 1 && abs(ayn - by) <= 1));
-                    __syncwarp();
-                    if (redo) {
-                        single(q + 1);
-                    } else {
-                        ++props;
-                        accs += accB;
-                        ovf += ovB;
-                        if (accB) E += dB;
-                        if (accB && lane == 16) apply_move(i, nx, ny, nc, ns, na, oc, ncell);
-                        __syncwarp();
+                    const int cells = pack_cells(ocx, ocy, ncx, ncy);
+                    int mi[M], mc[M];  // the group's moves so far: square (-1: none), cells
+#pragma unroll
+                    for (int k = 0; k < M; ++k) {
+                        const int src = k * W;
+                        const int ik = __shfl_sync(0xffffffffu, i, src), ck = __shfl_sync(0xffffffffu, cells, src);
+                        bool redo = false;
+#pragma unroll
+                        for (int m = 0; m < k; ++m) redo |= touches(mi[m], mc[m], ik, ck);
+                        if (redo) {
+                            const Moved mv = single(q + k);
+                            mi[k] = mv.i;
+                            mc[k] = mv.cells;
+                        } else {
+                            const int ak = __shfl_sync(0xffffffffu, acc, src), ovk = __shfl_sync(0xffffffffu, ov, src);
+                            const unsigned dlo = __shfl_sync(0xffffffffu, (unsigned)(unsigned long long)mine, src);
+                            const int dhi = __shfl_sync(0xffffffffu, (int)(mine >> 32), src);
+                            ++props;
+                            accs += ak;
+                            ovf += ovk;
+                            if (ak) E += (long long)(((unsigned long long)(unsigned)dhi << 32) | dlo);
+                            if (ak && lane == src) apply_move(i, nx, ny, nc, ns, na, oc, ncell);
+                            __syncwarp();
+                            mi[k] = ak ? ik : -1;
+                            mc[k] = ck;
+                        }
                     }
                 };
-                // pairs need room: on grids below 4 x 4 almost every pair would
-                // be evaluated twice; the move-set instance keeps one at a time
+                // groups need room: on small grids most proposals would be
+                // evaluated twice; the move-set instance keeps one at a time
                 // (its step scale follows the acceptance of the previous move)
-                const bool pairs = !MOVES && g.G >= 4;
+                const bool fours = !MOVES && g.G >= 8, twos = !MOVES && g.G >= 4;
                 for (int q = 0; q < kn;) {
-                    if (pairs && q + 1 < kn) {
-                        paired(q);
+                    if (fours && q + 3 < kn) {
+                        group(q, IntTag<4>{});
+                        q += 4;
+                    } else if (twos && q + 1 < kn) {
+                        group(q, IntTag<2>{});
                         q += 2;
                     } else {
                         single(q);
