@@ -157,6 +157,17 @@ __device__ __forceinline__ long long warp_sum_dq(long long v) {
 
 __device__ __forceinline__ long long qe(float e) { return __float2ll_rn(e * kEScale); }
 
+// Change of square Q's pair term when a square moves from P to (nx, ny) with
+// (cos, sin) = (nc, ns), in kEScale units.  Both terms are evaluated and each
+// is kept only inside the cut-off: the same values as testing first, without
+// a branch around them (a warp's lanes almost always disagree on the test).
+__device__ __forceinline__ long long pair_delta(float4 Q, float nx, float ny, float nc, float ns, float4 P) {
+    const float ex = Q.x - nx, ey = Q.y - ny, fx = Q.x - P.x, fy = Q.y - P.y;
+    const long long en = qe(sat_pair_energy(ex, ey, nc, ns, Q.z, Q.w));
+    const long long eo = qe(sat_pair_energy(fx, fy, P.z, P.w, Q.z, Q.w));
+    return (ex * ex + ey * ey < kPairCut2 ? en : 0) - (fx * fx + fy * fy < kPairCut2 ? eo : 0);
+}
+
 __device__ __forceinline__ long long warp_sum_ll(long long v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -835,12 +846,8 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                     long long dq = 0;
                     if (lane == 0) dq = qe(wall_e(nx, ny, nc, ns, L)) - qe(wall_e(P.x, P.y, P.z, P.w, L));
                     for_block(rep, g, ocx, ocy, lane, [&](int j) {
-                        if (j == i) return;
-                        const float4 Q = rep.sq[j];
-                        const float ex = Q.x - nx, ey = Q.y - ny;
-                        if (ex * ex + ey * ey < kPairCut2) dq += qe(sat_pair_energy(ex, ey, nc, ns, Q.z, Q.w));
-                        const float fx = Q.x - P.x, fy = Q.y - P.y;
-                        if (fx * fx + fy * fy < kPairCut2) dq -= qe(sat_pair_energy(fx, fy, P.z, P.w, Q.z, Q.w));
+                        const long long d = pair_delta(rep.sq[j], nx, ny, nc, ns, P);
+                        dq += j != i ? d : 0;
                     });
                     dq = warp_sum_dq(dq);
                     const float de = (float)dq * (1.0f / kEScale);
@@ -902,12 +909,8 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                     long long dq = 0;
                     if (gl == 0) dq = qe(wall_e(nx, ny, nc, ns, L)) - qe(wall_e(P.x, P.y, P.z, P.w, L));
                     for_block<W>(rep, g, ocx, ocy, gl, [&](int j) {
-                        if (j == i) return;
-                        const float4 Q = rep.sq[j];
-                        const float ex = Q.x - nx, ey = Q.y - ny;
-                        if (ex * ex + ey * ey < kPairCut2) dq += qe(sat_pair_energy(ex, ey, nc, ns, Q.z, Q.w));
-                        const float fx = Q.x - P.x, fy = Q.y - P.y;
-                        if (fx * fx + fy * fy < kPairCut2) dq -= qe(sat_pair_energy(fx, fy, P.z, P.w, Q.z, Q.w));
+                        const long long d = pair_delta(rep.sq[j], nx, ny, nc, ns, P);
+                        dq += j != i ? d : 0;
                     });
                     // exact sum over the group's lanes: hi * 2^20 + lo parts
                     // (a lane's term is below 2^46, so both parts stay in 32 bits)
