@@ -341,7 +341,7 @@ def run_sqs(args, D: Dist):
         line["cpu_baseline"] = dict(value=val, unit=UNIT, cores=cores, kind=kind, sample=sample)
     if D.rank == 0 and D.world == 1 and not args.no_extras:
         line["certify"] = bench_certify(ctx, args.cpu_seconds)
-        line["served"] = bench_served_sweep(ctx, args.served_rates)
+        line["served"] = bench_served_sweep(ctx, args.served_rates, args.served_jobs, args.served_sweeps)
         line["plain_pt"] = bench_plain_pt(ctx)
         line["batched"] = bench_batched(ctx)
     for d in (d_x, d_s, d_e, d_g, d_c):
@@ -399,11 +399,11 @@ def bench_certify(ctx, cpu_seconds: float, count: int = 10000):
     return res
 
 
-def served_jobs(count: int):
+def served_jobs(count: int, sweeps: int = 200):
     """Anneal-and-certify jobs of the served stream: n log-uniform in
-    [5, 1000], 16, 32 or 64 replicas, a 200-sweep budget each (a bounded
-    stand-in for the 50,000 sweeps a production job would run, so the bench
-    ends in minutes), seeded."""
+    [5, 1000], 16, 32 or 64 replicas, a `sweeps` budget each (200 by default:
+    a bounded stand-in for the 50,000 sweeps a production job would run, so
+    the bench ends in minutes), seeded."""
     import math
 
     import numpy as np
@@ -416,7 +416,7 @@ def served_jobs(count: int):
         n = int(round(math.exp(rng.uniform(math.log(5), math.log(1000)))))
         replicas = int(rng.choice([16, 32, 64]))
         xya, L0 = jittered_grid(n, seed=100 + k)
-        jobs.append(AnnealJob(xya, L0=L0, replicas=replicas, sweeps=200, exchange_every=10, tmin=1e-3, tmax=1e-1,
+        jobs.append(AnnealJob(xya, L0=L0, replicas=replicas, sweeps=sweeps, exchange_every=10, tmin=1e-3, tmax=1e-1,
                               seed=1000 + k, polish_iters=100))
     return jobs
 
@@ -442,7 +442,7 @@ def bench_served(ctx, jobs, plain, rate: float):
     p_stats = plain_stats(p_res[:count], p_service[:count], arr)
     same_L = all((a or {}).get("L") == (b or {}).get("L") for a, b in zip(served, p_res[:count]))
     return dict(workload=f"{count} jobs, Poisson {rate:g}/s, n log-uniform [5, 1000], 16/32/64 replicas, "
-                         f"200 sweeps", served=s_stats, plain=p_stats, equal_final_L=same_L, server_counters=counters,
+                         f"{jobs[0].sweeps} sweeps", served=s_stats, plain=p_stats, equal_final_L=same_L, server_counters=counters,
                 served_over_plain=s_stats["certified_jobs_per_s"] / max(p_stats["certified_jobs_per_s"], 1e-12))
 
 
@@ -472,11 +472,11 @@ def bench_plain_pt(ctx):
     return res
 
 
-def bench_served_sweep(ctx, rates: str, count: int = 960):
+def bench_served_sweep(ctx, rates: str, count: int = 960, sweeps: int = 200):
     from sqs.serve import plain_service
 
     rs = [float(x) for x in rates.split(",") if x]
-    jobs = served_jobs(count)
+    jobs = served_jobs(count, sweeps)
     need = min(count, max(40, max(int(4 * r + 1) for r in rs)))
     plain = plain_service(ctx, jobs[:need])
     return {f"{r:g}/s": bench_served(ctx, jobs, plain, r) for r in rs}
@@ -646,13 +646,16 @@ def main():
     ap.add_argument("--batched-instances", type=int, default=512)
     ap.add_argument("--batched-sweeps", type=int, default=50)
     ap.add_argument("--served-rates", default="10,50,200,1000")
+    ap.add_argument("--served-jobs", type=int, default=960, help="most jobs in one served stream")
+    ap.add_argument("--served-sweeps", type=int, default=200, help="sweep budget of every served job")
     args = ap.parse_args()
     if args.section:
         from sqs import Context
 
         with Context(int(os.environ.get("LOCAL_RANK", 0))) as ctx:
             fn = dict(certify=lambda: bench_certify(ctx, args.cpu_seconds),
-                      served=lambda: bench_served_sweep(ctx, args.served_rates),
+                      served=lambda: bench_served_sweep(ctx, args.served_rates, args.served_jobs,
+                                                        args.served_sweeps),
                       plain_pt=lambda: bench_plain_pt(ctx),
                       batched=lambda: bench_batched(ctx, args.batched_sweeps, args.batched_instances),
                       batched_fixed=lambda: bench_batched_fixed(ctx, args.batched_sweeps, args.batched_instances),
