@@ -341,7 +341,8 @@ def run_sqs(args, D: Dist):
         line["cpu_baseline"] = dict(value=val, unit=UNIT, cores=cores, kind=kind, sample=sample)
     if D.rank == 0 and D.world == 1 and not args.no_extras:
         line["certify"] = bench_certify(ctx, args.cpu_seconds)
-        line["served"] = bench_served_sweep(ctx, args.served_rates, args.served_jobs, args.served_sweeps)
+        line["served"] = bench_served_sweep(ctx, args.served_rates, args.served_jobs, args.served_sweeps,
+                                            args.served_slice)
         line["plain_pt"] = bench_plain_pt(ctx)
         line["batched"] = bench_batched(ctx)
     for d in (d_x, d_s, d_e, d_g, d_c):
@@ -421,7 +422,7 @@ def served_jobs(count: int, sweeps: int = 200):
     return jobs
 
 
-def bench_served(ctx, jobs, plain, rate: float):
+def bench_served(ctx, jobs, plain, rate: float, slice_proposals: int = 4000):
     """Served vs plain at one Poisson arrival rate: a stream of about four
     seconds of arrivals (at least 40 jobs, at most all of them) through the
     continuous-batching server; the plain comparator serves the same jobs one
@@ -435,7 +436,7 @@ def bench_served(ctx, jobs, plain, rate: float):
     count = min(len(jobs), max(40, int(math.ceil(4 * rate))))
     sub = jobs[:count]
     arr = poisson_arrivals(count, rate, seed=3)
-    with Server(ctx, hbm_bytes=4 << 30, max_active=count, slice_proposals=4000) as srv:
+    with Server(ctx, hbm_bytes=4 << 30, max_active=count, slice_proposals=slice_proposals) as srv:
         served, s_stats = run_stream(srv, sub, arr, timeout=600)
         counters = srv.stats()
     p_res, p_service = plain
@@ -472,14 +473,14 @@ def bench_plain_pt(ctx):
     return res
 
 
-def bench_served_sweep(ctx, rates: str, count: int = 960, sweeps: int = 200):
+def bench_served_sweep(ctx, rates: str, count: int = 960, sweeps: int = 200, slice_proposals: int = 4000):
     from sqs.serve import plain_service
 
     rs = [float(x) for x in rates.split(",") if x]
     jobs = served_jobs(count, sweeps)
     need = min(count, max(40, max(int(4 * r + 1) for r in rs)))
     plain = plain_service(ctx, jobs[:need])
-    return {f"{r:g}/s": bench_served(ctx, jobs, plain, r) for r in rs}
+    return {f"{r:g}/s": bench_served(ctx, jobs, plain, r, slice_proposals) for r in rs}
 
 
 # Algorithmic FP32 work of one proposal, the cost unit 2 k * 35 + 2 * 10 flop
@@ -648,6 +649,7 @@ def main():
     ap.add_argument("--served-rates", default="10,50,200,1000")
     ap.add_argument("--served-jobs", type=int, default=960, help="most jobs in one served stream")
     ap.add_argument("--served-sweeps", type=int, default=200, help="sweep budget of every served job")
+    ap.add_argument("--served-slice", type=int, default=4000, help="proposals per replica per server slice")
     args = ap.parse_args()
     if args.section:
         from sqs import Context
@@ -655,7 +657,7 @@ def main():
         with Context(int(os.environ.get("LOCAL_RANK", 0))) as ctx:
             fn = dict(certify=lambda: bench_certify(ctx, args.cpu_seconds),
                       served=lambda: bench_served_sweep(ctx, args.served_rates, args.served_jobs,
-                                                        args.served_sweeps),
+                                                        args.served_sweeps, args.served_slice),
                       plain_pt=lambda: bench_plain_pt(ctx),
                       batched=lambda: bench_batched(ctx, args.batched_sweeps, args.batched_instances),
                       batched_fixed=lambda: bench_batched_fixed(ctx, args.batched_sweeps, args.batched_instances),

@@ -339,10 +339,11 @@ int sqs_server_info(sqs_server* server, int* queued, int* active, size_t* hbm_us
  * (state upload), of harvesting finished slices and launching new ones, of
  * waiting when there was nothing else to do, and of retirement (polish,
  * rescue, certification), which runs on the server's own thread while the
- * steps go on. */
+ * steps go on; polish_s and certify_s are the polish (launch to results on
+ * the host) and the certification ladder within retire_s. */
 typedef struct sqs_server_stats {
     int64_t steps, slices, admitted, retired;
-    double admit_s, launch_s, retire_s, wait_s;
+    double admit_s, launch_s, retire_s, wait_s, polish_s, certify_s;
 } sqs_server_stats;
 int sqs_server_get_stats(sqs_server* server, sqs_server_stats* out);
 

@@ -20,8 +20,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -717,7 +719,10 @@ static int host_lit(const char* s, Lit& L) {
 }
 
 static int upload_consts(int device) {
-    static bool done[64] = {false};
+    static std::atomic<bool> done[64];
+    static std::mutex mu;  // several host threads may certify at once
+    if (done[device & 63]) return SQS_OK;
+    std::lock_guard<std::mutex> lk(mu);
     if (done[device & 63]) return SQS_OK;
     Consts c;
     Lit hp, tp, h;
@@ -791,7 +796,7 @@ static int launch_packing(sqs_ctx* ctx, int count, const int32_t* bucket, const 
                           uint32_t cap) {
     if (count == 0) return SQS_OK;
     const size_t smem = (size_t)NMAX * (sizeof(FSq) + 5 * sizeof(double) + sizeof(int16_t));
-    static bool attr[64] = {false};
+    static std::atomic<bool> attr[64];  // set-up once per device (idempotent if repeated)
     if (!attr[ctx->device & 63]) {
         SQS_CUDA(cudaFuncSetAttribute(cert_packing_kernel<T, NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));

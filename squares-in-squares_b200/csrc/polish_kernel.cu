@@ -14,6 +14,7 @@
 // order (the result is deterministic).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 
 #include "anneal.cuh"
@@ -410,7 +411,7 @@ __global__ void __launch_bounds__(kPT) polish_states_kernel(const int32_t* __res
 
 int launch_polish_states(cudaStream_t stream, int count, const int32_t* n_of, const int64_t* row0, int iters,
                          double* xya, double* res, size_t smem) {
-    static bool attr_done[64] = {false};
+    static std::atomic<bool> attr_done[64];  // set-up once per device (idempotent if repeated)
     int dev = 0;
     SQS_CUDA(cudaGetDevice(&dev));
     if (!attr_done[dev & 63]) {
@@ -425,7 +426,7 @@ int launch_polish_states(cudaStream_t stream, int count, const int32_t* n_of, co
 
 int launch_polish(cudaStream_t stream, int njobs, const int32_t* job_list, const JobDev* jdev, JobMut* jmut,
                   double* best, size_t smem) {
-    static bool attr_done[64] = {false};
+    static std::atomic<bool> attr_done[64];  // set-up once per device (idempotent if repeated)
     int dev = 0;
     cudaGetDevice(&dev);
     if (!attr_done[dev & 63]) {

@@ -80,18 +80,34 @@ struct Cohort {
 };
 constexpr int kCohorts = 8;
 constexpr double kWaitSeconds = 2e-3;
+// Retirement threads.  One: several threads issuing CUDA calls at once
+// slowed every phase (measured: a stream of 480 jobs at 1,000/s took 2.2 s
+// with three against 0.77 s with one).
+constexpr int kRetirers = 1;
+// Device buffers of a retirement thread's context, reserved up front (about
+// 420 bytes per square of a retired batch for the certifier's staging, the
+// interval cache of its undecided squares, the rescue polish's state).
+constexpr size_t kRetireStaging = (size_t)64 << 20;
+constexpr size_t kRetireCache = (size_t)32 << 20;
+constexpr size_t kRetirePolish = (size_t)8 << 20;
+
+// A retirement thread's own context (buffers, a stream of the highest
+// priority) and device list of job slots.
+struct Retirer {
+    sqs_ctx* ctx = nullptr;
+    int32_t* d_list = nullptr;
+    std::thread th;
+};
 }  // namespace
 
 struct sqs_server {
     sqs_ctx* ctx = nullptr;
-    sqs_ctx* rctx = nullptr;  // retirement: own buffers, a stream of the highest priority
     char* arena = nullptr;
     size_t arena_bytes = 0;
     std::map<size_t, size_t> free_blocks;  // offset -> bytes
     int max_active = 0, slice = 0;  // slice < 0: about -slice proposals per replica per step, per job
     JobDev* d_jd = nullptr;
     JobMut* d_jm = nullptr;
-    int32_t* d_list = nullptr;
     std::vector<int64_t> slot_job;         // job id per slot, -1 free
     std::deque<int64_t> queue;
     std::unordered_map<int64_t, SJob> jobs;
@@ -108,7 +124,7 @@ struct sqs_server {
     bool stop = false;
     int werr = 0;
     std::string werr_msg;
-    std::thread worker;
+    std::vector<Retirer> retirers;
     size_t used = 0;
     sqs_server_stats st{};
 };
@@ -199,18 +215,17 @@ int admit(sqs_server* s) {
 }  // namespace
 
 namespace {
-void retire_loop(sqs_server* s);
+void retire_loop(sqs_server* s, Retirer* me);
 
 // Release everything a server holds (after its streams are idle).
 void free_server(sqs_server* s) {
-    if (s->worker.joinable()) {
-        {
-            std::lock_guard<std::mutex> lk(s->mu);
-            s->stop = true;
-        }
-        s->cv.notify_all();
-        s->worker.join();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
     }
+    s->cv.notify_all();
+    for (Retirer& w : s->retirers)
+        if (w.th.joinable()) w.th.join();
     for (Cohort& c : s->cohorts) {
         if (c.st) cudaStreamSynchronize(c.st);
         if (c.st) cudaStreamDestroy(c.st);
@@ -222,8 +237,10 @@ void free_server(sqs_server* s) {
     cudaFree(s->arena);
     cudaFree(s->d_jd);
     cudaFree(s->d_jm);
-    cudaFree(s->d_list);
-    sqs_ctx_destroy(s->rctx);
+    for (Retirer& w : s->retirers) {
+        cudaFree(w.d_list);
+        sqs_ctx_destroy(w.ctx);
+    }
     delete s;
 }
 }  // namespace
@@ -243,19 +260,29 @@ extern "C" int sqs_server_create(sqs_ctx* ctx, size_t hbm_bytes, int max_active,
     cudaError_t e = cudaMalloc(&s->arena, s->arena_bytes);
     if (e == cudaSuccess) e = cudaMalloc(&s->d_jd, sizeof(JobDev) * (size_t)max_active);
     if (e == cudaSuccess) e = cudaMalloc(&s->d_jm, sizeof(JobMut) * (size_t)max_active);
-    if (e == cudaSuccess) e = cudaMalloc(&s->d_list, sizeof(int32_t) * (size_t)max_active);
-    // Retirement (polish, certification) gets its own context on a stream of
-    // the highest priority: its blocks are dispatched ahead of pending anneal
-    // blocks as SMs free up, so a finished job does not queue behind slices.
-    if (e == cudaSuccess) {
-        if (int r = sqs_ctx_create(ctx->device, &s->rctx)) {
+    // Each retirement thread (polish, certification) gets its own context on
+    // a stream of the highest priority: its blocks are dispatched ahead of
+    // pending anneal blocks as SMs free up, so a finished job does not queue
+    // behind slices, and batches retire side by side.
+    s->retirers.resize(kRetirers);
+    for (Retirer& w : s->retirers) {
+        if (e != cudaSuccess) break;
+        if (int r = sqs_ctx_create(ctx->device, &w.ctx)) {
             free_server(s);
             return r;
         }
         int least = 0, greatest = 0;
         e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
-        if (e == cudaSuccess) e = cudaStreamDestroy(s->rctx->stream);
-        if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&s->rctx->stream, cudaStreamNonBlocking, greatest);
+        if (e == cudaSuccess) e = cudaStreamDestroy(w.ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&w.ctx->stream, cudaStreamNonBlocking, greatest);
+        if (e == cudaSuccess) e = cudaMalloc(&w.d_list, sizeof(int32_t) * (size_t)max_active);
+        // Staging of the certifier, its interval cache and the rescue polish,
+        // sized now: growing a buffer later frees the old one, which waits for
+        // every slice on the GPU and holds up the caller's thread meanwhile.
+        if (e == cudaSuccess && (w.ctx->d_misc.reserve(kRetireStaging) != SQS_OK ||
+                                 w.ctx->d_cert.reserve(kRetireCache) != SQS_OK ||
+                                 w.ctx->d_polish.reserve(kRetirePolish) != SQS_OK))
+            e = cudaErrorMemoryAllocation;
     }
     s->cohorts.resize(kCohorts);
     for (Cohort& c : s->cohorts) {
@@ -274,7 +301,7 @@ extern "C" int sqs_server_create(sqs_ctx* ctx, size_t hbm_bytes, int max_active,
     s->slot_job.assign((size_t)max_active, -1);
     s->flying.assign((size_t)max_active, 0);
     s->retiring.assign((size_t)max_active, 0);
-    s->worker = std::thread(retire_loop, s);
+    for (Retirer& w : s->retirers) w.th = std::thread(retire_loop, s, &w);
     *out = s;
     return SQS_OK;
 }
@@ -423,7 +450,7 @@ int launch_idle(sqs_server* s, const std::vector<int32_t>& fin, int& launched) {
 // stream, while the caller's thread keeps the cohorts going.  The lock is
 // taken only to look the jobs up and to publish the results; in between the
 // thread reads job fields that nothing changes while a job is active.
-int retire(sqs_server* s, const std::vector<int32_t>& fin) {
+int retire(sqs_server* s, Retirer* me, const std::vector<int32_t>& fin) {
     std::vector<SJob*> jobs;
     std::vector<uint8_t> cancel;
     {
@@ -434,28 +461,30 @@ int retire(sqs_server* s, const std::vector<int32_t>& fin) {
             cancel.push_back(j->cancel ? 1 : 0);
         }
     }
-    const int64_t l0 = s->rctx->launches;
+    const int64_t l0 = me->ctx->launches;
+    const auto t0 = std::chrono::steady_clock::now();
     size_t psmem = 0;
     for (const SJob* j : jobs) psmem = std::max(psmem, polish_smem_bytes(j->job.n));
-    SQS_CUDA(cudaMemcpyAsync(s->d_list, fin.data(), sizeof(int32_t) * fin.size(), cudaMemcpyHostToDevice,
-                             s->rctx->stream));
-    if (int r = launch_polish(s->rctx->stream, (int)fin.size(), s->d_list, s->d_jd, s->d_jm, (double*)s->arena, psmem))
+    SQS_CUDA(cudaMemcpyAsync(me->d_list, fin.data(), sizeof(int32_t) * fin.size(), cudaMemcpyHostToDevice,
+                             me->ctx->stream));
+    if (int r = launch_polish(me->ctx->stream, (int)fin.size(), me->d_list, s->d_jd, s->d_jm, (double*)s->arena, psmem))
         return r;
-    s->rctx->launches += 1;
+    me->ctx->launches += 1;
     std::vector<std::vector<double>> best(fin.size()), out(fin.size());
     std::vector<JobMut> jm(fin.size());
     for (size_t q = 0; q < fin.size(); ++q) {
         best[q].resize(3 * (size_t)jobs[q]->job.n);
         SQS_CUDA(cudaMemcpyAsync(best[q].data(), (double*)s->arena + jobs[q]->jd.best_off,
-                                 sizeof(double) * best[q].size(), cudaMemcpyDeviceToHost, s->rctx->stream));
-        SQS_CUDA(cudaMemcpyAsync(&jm[q], s->d_jm + fin[q], sizeof(JobMut), cudaMemcpyDeviceToHost, s->rctx->stream));
+                                 sizeof(double) * best[q].size(), cudaMemcpyDeviceToHost, me->ctx->stream));
+        SQS_CUDA(cudaMemcpyAsync(&jm[q], s->d_jm + fin[q], sizeof(JobMut), cudaMemcpyDeviceToHost, me->ctx->stream));
     }
-    SQS_CUDA(cudaStreamSynchronize(s->rctx->stream));
+    SQS_CUDA(cudaStreamSynchronize(me->ctx->stream));
+    const double polish_s = seconds_since(t0);
     {
         std::vector<Rescue> rs;
         for (size_t q = 0; q < fin.size(); ++q)
             if (!cancel[q]) add_rescue(rs, jobs[q]->job, jobs[q]->jd, jm[q], (const float4*)s->arena, best[q].data());
-        if (int r = rescue_uncertified(s->rctx, rs)) return r;
+        if (int r = rescue_uncertified(me->ctx, rs)) return r;
     }
     std::vector<sqs_job_result> res(fin.size());
     std::vector<int> ns;
@@ -476,8 +505,12 @@ int retire(sqs_server* s, const std::vector<int32_t>& fin) {
             xptr.push_back(out[q].data());
         }
     }
-    if (int r = certify_states(s->rctx, ns, bptr, optr, xptr)) return r;
+    const auto t1 = std::chrono::steady_clock::now();
+    if (int r = certify_states(me->ctx, ns, bptr, optr, xptr)) return r;
+    const double certify_s = seconds_since(t1);
     std::lock_guard<std::mutex> lk(s->mu);
+    s->st.polish_s += polish_s;
+    s->st.certify_s += certify_s;
     for (size_t q = 0; q < fin.size(); ++q) {
         SJob& j = *jobs[q];
         j.res = res[q];
@@ -489,7 +522,7 @@ int retire(sqs_server* s, const std::vector<int32_t>& fin) {
         s->retiring[(size_t)fin[q]] = 0;
     }
     s->st.retired += (int64_t)fin.size();
-    s->ctx->launches += s->rctx->launches - l0;
+    s->ctx->launches += me->ctx->launches - l0;
     return SQS_OK;
 }
 
@@ -497,7 +530,7 @@ int retire(sqs_server* s, const std::vector<int32_t>& fin) {
 // time it looks, as one batch (jobs that finish while a retirement runs are
 // retired together next); an error is kept and reported by the caller's
 // next step.
-void retire_loop(sqs_server* s) {
+void retire_loop(sqs_server* s, Retirer* me) {
     cudaSetDevice(s->ctx->device);
     for (;;) {
         std::vector<int32_t> fin;
@@ -511,7 +544,7 @@ void retire_loop(sqs_server* s) {
             s->rq.clear();
         }
         const auto t0 = std::chrono::steady_clock::now();
-        const int r = retire(s, fin);
+        const int r = retire(s, me, fin);
         std::lock_guard<std::mutex> lk(s->mu);
         if (r && !s->werr) {
             s->werr = r;

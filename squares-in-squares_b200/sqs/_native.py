@@ -70,7 +70,8 @@ class PolishResult(C.Structure):
 class ServerStats(C.Structure):
     """sqs_server_stats (include/sqs.h)."""
     _fields_ = [("steps", C.c_int64), ("slices", C.c_int64), ("admitted", C.c_int64), ("retired", C.c_int64),
-                ("admit_s", C.c_double), ("launch_s", C.c_double), ("retire_s", C.c_double), ("wait_s", C.c_double)]
+                ("admit_s", C.c_double), ("launch_s", C.c_double), ("retire_s", C.c_double), ("wait_s", C.c_double),
+                ("polish_s", C.c_double), ("certify_s", C.c_double)]
 
 
 JOB_AUTOTUNE = 1

@@ -104,3 +104,25 @@ def test_proposal_sliced_server_equals_alone(ctx):
     for a, b in zip(alone, got):
         for key in KEYS:
             assert a[key] == b[key], key
+
+
+def test_server_counters_and_retirement_thread(ctx):
+    """Every admitted job is retired exactly once by the retirement thread;
+    slices and host phase times are counted; jobs of several cluster shapes
+    (separate cohorts) all come back equal to their results alone."""
+    from sqs.anneal import anneal_batch
+    from sqs.serve import Server, poisson_arrivals, run_stream
+    jobs = [_job(n, 30 + k, 80, replicas=r) for k, (n, r) in
+            enumerate([(12, 4), (40, 16), (90, 32), (25, 8), (150, 64), (8, 2), (60, 16), (33, 32)])]
+    alone = [anneal_batch([j], ctx=ctx)[0] for j in jobs]
+    arr = poisson_arrivals(len(jobs), rate=500.0, seed=4)
+    with Server(ctx, hbm_bytes=64 << 20, max_active=8, slice_proposals=500) as srv:
+        results, stats = run_stream(srv, jobs, arr, timeout=120)
+        st = srv.stats()
+    assert stats["jobs"] == len(jobs)
+    assert st["admitted"] == st["retired"] == len(jobs)
+    assert st["slices"] >= len(jobs) and st["steps"] >= 1
+    assert min(st["admit_s"], st["launch_s"], st["retire_s"], st["wait_s"]) >= 0.0
+    for a, b in zip(alone, results):
+        for key in KEYS:
+            assert a[key] == b[key], key
