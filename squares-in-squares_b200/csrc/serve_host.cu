@@ -115,6 +115,11 @@ struct sqs_server {
     std::vector<uint8_t> flying;           // per slot: in a cohort's slice now
     std::vector<uint8_t> retiring;         // per slot: handed to the retirement thread
     std::vector<Cohort> cohorts;
+    // Admission uploads and builds job state on its own stream of the
+    // highest priority; every slice launch waits for its last event on the
+    // device, so admission needs no host synchronisation.
+    cudaStream_t ast = nullptr;
+    cudaEvent_t admitted = nullptr;
     // The retirement thread and what it shares with the caller's thread
     // (jobs, slots, arena, counters), guarded by `mu`.
     std::mutex mu;
@@ -164,6 +169,25 @@ double seconds_since(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
+// Every replica of a job starts from its state xya (n x 3 doubles, staged in
+// the job's best-packing slot): centres as floats, angles reduced to
+// [0, pi/2) in double first -- the host's init_replicas, bit for bit (fmod is
+// exact, the conversions round to nearest) -- and the quench scratch zeroed.
+__global__ void init_replicas_kernel(const double* __restrict__ xya, int n, int R, float4* __restrict__ dst) {
+    const int64_t total = (int64_t)R * n + 2 * (int64_t)n;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
+        if (k >= (int64_t)R * n) {
+            dst[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+            continue;
+        }
+        const int i = (int)(k % n);
+        const double q = 1.57079632679489661923;
+        double a = fmod(xya[3 * i + 2], q);
+        if (a < 0.0) a += q;
+        dst[k] = make_float4((float)xya[3 * i], (float)xya[3 * i + 1], (float)a, 0.f);
+    }
+}
+
 size_t job_bytes(const sqs_job& J) {
     const size_t b = sizeof(float4) * (size_t)job_pos_elems(J) + sizeof(double) * 3 * (size_t)J.n;
     return (b + 255) & ~(size_t)255;
@@ -173,7 +197,8 @@ int admit(sqs_server* s) {
     const size_t window = 16;  // queued jobs that do not fit yet which admission looks past
     size_t skipped = 0;
     int slot = 0;
-    std::vector<std::vector<float4>> inits;  // host staging, alive until the copies are done
+    std::vector<std::vector<float4>> inits;  // host staging of jobs with one start per replica
+    bool admitted_any = false;
     for (auto it = s->queue.begin(); it != s->queue.end() && skipped < window;) {
         SJob& j = s->jobs[*it];
         while (slot < s->max_active && s->slot_job[(size_t)slot] >= 0) ++slot;
@@ -197,18 +222,33 @@ int admit(sqs_server* s) {
             const int64_t sw = std::max<int64_t>(1, (-(int64_t)s->slice + j.job.n - 1) / j.job.n);
             j.jd.slice = (int)std::min<int64_t>((sw + xe - 1) / xe * xe, 1 << 30);
         }
-        inits.emplace_back((size_t)job_pos_elems(j.job), make_float4(0.f, 0.f, 0.f, 0.f));
-        std::vector<float4>& init = inits.back();
-        init_replicas(j.job, init.data());
-        SQS_CUDA(cudaMemcpyAsync(s->arena + off, init.data(), sizeof(float4) * init.size(), cudaMemcpyHostToDevice,
-                                 s->ctx->stream));
-        SQS_CUDA(cudaMemcpyAsync(s->d_jd + slot, &j.jd, sizeof(JobDev), cudaMemcpyHostToDevice, s->ctx->stream));
-        SQS_CUDA(cudaMemcpyAsync(s->d_jm + slot, &j.jm, sizeof(JobMut), cudaMemcpyHostToDevice, s->ctx->stream));
+        if (j.job.xya_rep) {  // one start per replica: built on the host
+            inits.emplace_back((size_t)job_pos_elems(j.job), make_float4(0.f, 0.f, 0.f, 0.f));
+            std::vector<float4>& init = inits.back();
+            init_replicas(j.job, init.data());
+            SQS_CUDA(cudaMemcpyAsync(s->arena + off, init.data(), sizeof(float4) * init.size(),
+                                     cudaMemcpyHostToDevice, s->ast));
+        } else {  // one start for all: n x 3 doubles up, replicas built on the device
+            double* stage = (double*)s->arena + j.jd.best_off;
+            SQS_CUDA(cudaMemcpyAsync(stage, j.xya.data(), sizeof(double) * 3 * (size_t)j.job.n,
+                                     cudaMemcpyHostToDevice, s->ast));
+            const int64_t total = job_pos_elems(j.job);
+            const int blocks = (int)std::min<int64_t>(1024, (total + 255) / 256);
+            init_replicas_kernel<<<blocks, 256, 0, s->ast>>>(stage, j.job.n, j.job.replicas,
+                                                                     (float4*)(s->arena + off));
+            SQS_CUDA(cudaGetLastError());
+            s->ctx->launches += 1;
+        }
+        SQS_CUDA(cudaMemcpyAsync(s->d_jd + slot, &j.jd, sizeof(JobDev), cudaMemcpyHostToDevice, s->ast));
+        SQS_CUDA(cudaMemcpyAsync(s->d_jm + slot, &j.jm, sizeof(JobMut), cudaMemcpyHostToDevice, s->ast));
         s->slot_job[(size_t)slot] = j.id;
+        admitted_any = true;
         ++s->st.admitted;
         it = s->queue.erase(it);
     }
-    if (!inits.empty()) SQS_CUDA(cudaStreamSynchronize(s->ctx->stream));  // the staging vectors end here
+    // (copies from pageable memory have consumed their host source on return,
+    // so the staging vectors may end here)
+    if (admitted_any) SQS_CUDA(cudaEventRecord(s->admitted, s->ast));
     return SQS_OK;
 }
 
@@ -226,6 +266,7 @@ void free_server(sqs_server* s) {
     s->cv.notify_all();
     for (Retirer& w : s->retirers)
         if (w.th.joinable()) w.th.join();
+    if (s->ast) cudaStreamSynchronize(s->ast);
     for (Cohort& c : s->cohorts) {
         if (c.st) cudaStreamSynchronize(c.st);
         if (c.st) cudaStreamDestroy(c.st);
@@ -241,6 +282,8 @@ void free_server(sqs_server* s) {
         cudaFree(w.d_list);
         sqs_ctx_destroy(w.ctx);
     }
+    if (s->ast) cudaStreamDestroy(s->ast);
+    if (s->admitted) cudaEventDestroy(s->admitted);
     delete s;
 }
 }  // namespace
@@ -283,6 +326,13 @@ extern "C" int sqs_server_create(sqs_ctx* ctx, size_t hbm_bytes, int max_active,
                                  w.ctx->d_cert.reserve(kRetireCache) != SQS_OK ||
                                  w.ctx->d_polish.reserve(kRetirePolish) != SQS_OK))
             e = cudaErrorMemoryAllocation;
+    }
+    if (e == cudaSuccess) {
+        int least = 0, greatest = 0;
+        e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&s->ast, cudaStreamNonBlocking, greatest);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->admitted, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(s->admitted, s->ast);  // waited on before any admission
     }
     s->cohorts.resize(kCohorts);
     for (Cohort& c : s->cohorts) {
@@ -423,6 +473,7 @@ int launch_idle(sqs_server* s, const std::vector<int32_t>& fin, int& launched) {
         if (!c) break;  // every stream busy: the rest wait for the next step
         const std::vector<int32_t>& list = groups[o.second];
         const int cnt = (int)list.size();
+        SQS_CUDA(cudaStreamWaitEvent(c->st, s->admitted, 0));  // the jobs' uploads are done first
         SQS_CUDA(cudaMemcpyAsync(c->d_list, list.data(), sizeof(int32_t) * (size_t)cnt, cudaMemcpyHostToDevice, c->st));
         if (int r = launch_anneal(c->st, cnt, std::get<0>(o.second), std::get<1>(o.second),
                                   (size_t)(rb[o.second] * std::get<1>(o.second)), std::get<2>(o.second) != 0, c->d_list,
