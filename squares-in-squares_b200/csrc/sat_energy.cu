@@ -514,8 +514,8 @@ __global__ void __launch_bounds__(W * 32) sat_energy_warp_kernel(int configs, in
 }
 
 template <int W>
-static int launch_warp(sqs_ctx* ctx, int configs, int n, const float* xya, const float* side, float* energy,
-                       float* grad, uint32_t* cand) {
+static int launch_warp(sqs_ctx* ctx, cudaStream_t st, int configs, int n, const float* xya, const float* side,
+                       float* energy, float* grad, uint32_t* cand) {
     const size_t smem = warp_smem_bytes(n) * W;
     static bool attr_set[64] = {false};
     const int dev = ctx->device & 63;
@@ -528,10 +528,10 @@ static int launch_warp(sqs_ctx* ctx, int configs, int n, const float* xya, const
     }
     const unsigned blocks = (unsigned)((configs + W - 1) / W);
     if (cand)
-        sat_energy_warp_kernel<W, true><<<blocks, W * 32, smem, ctx->stream>>>(configs, n, xya, side, energy, grad,
+        sat_energy_warp_kernel<W, true><<<blocks, W * 32, smem, st>>>(configs, n, xya, side, energy, grad,
                                                                                cand);
     else
-        sat_energy_warp_kernel<W, false><<<blocks, W * 32, smem, ctx->stream>>>(configs, n, xya, side, energy, grad,
+        sat_energy_warp_kernel<W, false><<<blocks, W * 32, smem, st>>>(configs, n, xya, side, energy, grad,
                                                                                 nullptr);
     SQS_CUDA(cudaGetLastError());
     ctx->launches += 1;
@@ -539,7 +539,7 @@ static int launch_warp(sqs_ctx* ctx, int configs, int n, const float* xya, const
 }
 
 template <int T>
-static int launch(sqs_ctx* ctx, int configs, int n, const float* xya, const float* side,
+static int launch(sqs_ctx* ctx, cudaStream_t st, int configs, int n, const float* xya, const float* side,
                   float* energy, float* grad, uint32_t* cand) {
     const size_t smem = sat_smem_bytes(n, T);
     static bool attr_set[64] = {false};
@@ -549,14 +549,14 @@ static int launch(sqs_ctx* ctx, int configs, int n, const float* xya, const floa
                                       96 * 1024));
         attr_set[dev] = true;
     }
-    sat_energy_kernel<T><<<configs, T, smem, ctx->stream>>>(n, xya, side, energy, grad, cand);
+    sat_energy_kernel<T><<<configs, T, smem, st>>>(n, xya, side, energy, grad, cand);
     SQS_CUDA(cudaGetLastError());
     ctx->launches += 1;
     return SQS_OK;
 }
 
-int sat_energy_launch(sqs_ctx* ctx, int configs, int n, const float* xya, const float* side,
-                      float* energy, float* grad, uint32_t* cand, int threads) {
+static int sat_energy_launch_on(sqs_ctx* ctx, cudaStream_t st, int configs, int n, const float* xya,
+                                const float* side, float* energy, float* grad, uint32_t* cand, int threads) {
     SQS_REQUIRE(configs >= 0 && configs <= (1 << 30), "configs %d out of range", configs);
     SQS_REQUIRE(n >= 1 && n <= kSatMaxN, "n %d out of 1..%d", n, kSatMaxN);
     SQS_REQUIRE(xya && side && energy, "null device pointer");
@@ -565,21 +565,26 @@ int sat_energy_launch(sqs_ctx* ctx, int configs, int n, const float* xya, const 
     if (threads < 0) {  // warp-per-configuration kernel, -threads warps per CTA
         SQS_REQUIRE(n <= kWarpMaxN, "the warp-per-configuration kernel takes n <= %d", kWarpMaxN);
         switch (-threads) {
-            case 2: return launch_warp<2>(ctx, configs, n, xya, side, energy, grad, cand);
-            case 4: return launch_warp<4>(ctx, configs, n, xya, side, energy, grad, cand);
-            case 8: return launch_warp<8>(ctx, configs, n, xya, side, energy, grad, cand);
+            case 2: return launch_warp<2>(ctx, st, configs, n, xya, side, energy, grad, cand);
+            case 4: return launch_warp<4>(ctx, st, configs, n, xya, side, energy, grad, cand);
+            case 8: return launch_warp<8>(ctx, st, configs, n, xya, side, energy, grad, cand);
             default: break;
         }
         SQS_REQUIRE(false, "threads %d: warps per CTA must be 2, 4 or 8", threads);
     }
     switch (threads) {
-        case 32: return launch<32>(ctx, configs, n, xya, side, energy, grad, cand);
-        case 64: return launch<64>(ctx, configs, n, xya, side, energy, grad, cand);
-        case 128: return launch<128>(ctx, configs, n, xya, side, energy, grad, cand);
-        case 256: return launch<256>(ctx, configs, n, xya, side, energy, grad, cand);
+        case 32: return launch<32>(ctx, st, configs, n, xya, side, energy, grad, cand);
+        case 64: return launch<64>(ctx, st, configs, n, xya, side, energy, grad, cand);
+        case 128: return launch<128>(ctx, st, configs, n, xya, side, energy, grad, cand);
+        case 256: return launch<256>(ctx, st, configs, n, xya, side, energy, grad, cand);
         default: break;
     }
     SQS_REQUIRE(false, "threads %d not in {32, 64, 128, 256}", threads);
+}
+
+int sat_energy_launch(sqs_ctx* ctx, int configs, int n, const float* xya, const float* side,
+                      float* energy, float* grad, uint32_t* cand, int threads) {
+    return sat_energy_launch_on(ctx, ctx->stream, configs, n, xya, side, energy, grad, cand, threads);
 }
 
 }  // namespace sqs
@@ -604,20 +609,44 @@ extern "C" int sqs_sat_energy_host(sqs_ctx* ctx, int configs, int n, const float
         if (int r = ctx->d_grad.reserve(sb)) return r;
     if (cand)
         if (int r = ctx->d_cand.reserve((size_t)configs * sizeof(uint32_t))) return r;
-    SQS_CUDA(cudaMemcpyAsync(ctx->d_in.p, xya, sb, cudaMemcpyHostToDevice, ctx->stream));
-    SQS_CUDA(cudaMemcpyAsync(ctx->d_side.p, side, (size_t)configs * sizeof(float),
-                             cudaMemcpyHostToDevice, ctx->stream));
-    int r = sqs::sat_energy_launch(ctx, configs, n, (const float*)ctx->d_in.p, (const float*)ctx->d_side.p,
-                                   (float*)ctx->d_out.p, grad ? (float*)ctx->d_grad.p : nullptr,
-                                   cand ? (uint32_t*)ctx->d_cand.p : nullptr, 0);
-    if (r) return r;
-    SQS_CUDA(cudaMemcpyAsync(energy, ctx->d_out.p, (size_t)configs * sizeof(float),
-                             cudaMemcpyDeviceToHost, ctx->stream));
-    if (grad)
-        SQS_CUDA(cudaMemcpyAsync(grad, ctx->d_grad.p, sb, cudaMemcpyDeviceToHost, ctx->stream));
-    if (cand)
-        SQS_CUDA(cudaMemcpyAsync(cand, ctx->d_cand.p, (size_t)configs * sizeof(uint32_t),
-                                 cudaMemcpyDeviceToHost, ctx->stream));
+    // Chunks of the batch on the context's side streams: the upload of one
+    // chunk, the kernel of the one before and the download of the one before
+    // that overlap.  Four chunks measured best for 4,096 x 200 squares
+    // (0.38 ms per call against 0.44 ms in one piece; 8 and 16 chunks cost
+    // more in calls than they gain: the host link carried about 51 GB/s in
+    // both directions together, so the transfers overlap only in part).
+    const int chunks = configs >= 1024 ? std::min(4, configs / 256) : 1;
+    float* d_in = (float*)ctx->d_in.p;
+    float* d_side = (float*)ctx->d_side.p;
+    float* d_out = (float*)ctx->d_out.p;
+    float* d_grad = grad ? (float*)ctx->d_grad.p : nullptr;
+    uint32_t* d_cand = cand ? (uint32_t*)ctx->d_cand.p : nullptr;
+    const int na = chunks == 1 ? 0 : std::min(chunks, sqs_ctx::kAux);
+    SQS_CUDA(cudaEventRecord(ctx->fork, ctx->stream));
+    for (int a = 0; a < na; ++a) SQS_CUDA(cudaStreamWaitEvent(ctx->aux[a], ctx->fork, 0));
+    int rc = SQS_OK;
+    for (int c = 0; c < chunks && rc == SQS_OK; ++c) {
+        cudaStream_t st = chunks == 1 ? ctx->stream : ctx->aux[c % sqs_ctx::kAux];
+        const int64_t lo = (int64_t)configs * c / chunks, hi = (int64_t)configs * (c + 1) / chunks;
+        const int cnt = (int)(hi - lo);
+        const size_t e0 = (size_t)lo * n * 3, eb = (size_t)cnt * n * 3 * sizeof(float);
+        SQS_CUDA(cudaMemcpyAsync(d_in + e0, xya + e0, eb, cudaMemcpyHostToDevice, st));
+        SQS_CUDA(cudaMemcpyAsync(d_side + lo, side + lo, (size_t)cnt * sizeof(float), cudaMemcpyHostToDevice, st));
+        rc = sqs::sat_energy_launch_on(ctx, st, cnt, n, d_in + e0, d_side + lo, d_out + lo,
+                                       d_grad ? d_grad + e0 : nullptr, d_cand ? d_cand + lo : nullptr, 0);
+        if (rc) break;
+        SQS_CUDA(cudaMemcpyAsync(energy + lo, d_out + lo, (size_t)cnt * sizeof(float), cudaMemcpyDeviceToHost, st));
+        if (grad) SQS_CUDA(cudaMemcpyAsync(grad + e0, d_grad + e0, eb, cudaMemcpyDeviceToHost, st));
+        if (cand)
+            SQS_CUDA(cudaMemcpyAsync(cand + lo, d_cand + lo, (size_t)cnt * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                     st));
+    }
+    // join every side stream, also after a failure
+    for (int a = 0; a < na; ++a) {
+        SQS_CUDA(cudaEventRecord(ctx->join[a], ctx->aux[a]));
+        SQS_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->join[a], 0));
+    }
+    if (rc) return rc;
     SQS_CUDA(cudaStreamSynchronize(ctx->stream));
     return SQS_OK;
 }
