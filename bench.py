@@ -29,6 +29,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 from pathlib import Path
 
@@ -95,7 +96,7 @@ class Clocks:
         ids = [s for s in cvd.split(",") if s.strip()]
         self.sel = ids[local_rank] if local_rank < len(ids) else str(local_rank)
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f".clocks_{os.getpid()}.csv"
+        self.path = Path(tempfile.gettempdir()) / f"sqs_clocks_{os.getpid()}_{local_rank}.csv"
 
     def start(self):
         try:
