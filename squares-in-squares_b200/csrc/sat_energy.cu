@@ -275,7 +275,8 @@ __global__ void __launch_bounds__(T) sat_energy_kernel(int n, const float* __res
 
 // ---------------------------------------------------------------------------
 // Warp-per-configuration form for n <= 256: the same phases as above run by
-// one warp without block barriers, several configurations per CTA.  A lane
+// one warp without block barriers, several configurations per CTA, except that
+// energies are summed exactly as integers, so a cell's entries need no ordering.  A lane
 // keeps its (up to 8) squares in registers from the load to the scatter, all
 // loads are issued before any is used, and the cell grid is sized from n, so
 // ~7.7 KB of shared memory per configuration lets a whole 4,096-configuration
@@ -304,6 +305,15 @@ __host__ __device__ inline size_t warp_smem_bytes(int n) {
 // sum is exact and order-free.
 constexpr float kGScale = 524288.0f;
 
+// Energies of the warp kernel are summed as 64-bit integers in units of
+// 2^-40: every wall and pair term is rounded once (error below 5e-13), the
+// sum is exact, and so it does not depend on the order in which the pairs are
+// found -- cell lists built with atomics need no sorting for a deterministic
+// result.  A configuration's energy is far below 2^23, so the sum stays
+// below 2^63 units.
+constexpr double kEUnit = 1099511627776.0;  // 2^40
+__device__ __forceinline__ long long e_units(float e) { return __float2ll_rn(e * 1099511627776.0f); }
+
 // round(v * kGScale) to the nearest integer (ties to even) on the FMA pipe:
 // for |v * kGScale| < 2^22 the fused v * 2^19 + 1.5 * 2^23 lands in
 // [2^23, 2^24), where one float ulp is 1, so its bit pattern minus that of
@@ -312,8 +322,10 @@ __device__ __forceinline__ int gq_units(float v) {
     return __float_as_int(fmaf(v, kGScale, 12582912.0f)) - 0x4B400000;
 }
 
+// 28 / W CTAs of W warps per SM (72 registers a thread at W = 4): with the
+// shared memory of n = 200 that keeps 4,096 configurations in one wave.
 template <int W, bool COUNT>
-__global__ void __launch_bounds__(W * 32) sat_energy_warp_kernel(int configs, int n, const float* __restrict__ xya,
+__global__ void __launch_bounds__(W * 32, 28 / W) sat_energy_warp_kernel(int configs, int n, const float* __restrict__ xya,
                                                                  const float* __restrict__ side,
                                                                  float* __restrict__ energy, float* __restrict__ grad,
                                                                  uint32_t* __restrict__ cand) {
@@ -352,7 +364,7 @@ __global__ void __launch_bounds__(W * 32) sat_energy_warp_kernel(int configs, in
         }
     }
     __syncwarp();
-    float e_loc = 0.f;
+    long long e_loc = 0;  // kEUnit units: exact, so the sum does not depend on the order of the pairs
     float pc[kWarpNpl], ps[kWarpNpl];
     int cr[kWarpNpl];  // cell << 16 | rank
 #pragma unroll
@@ -361,7 +373,7 @@ __global__ void __launch_bounds__(W * 32) sat_energy_warp_kernel(int configs, in
         if (i < n) {
             sincosf(pa[k], &ps[k], &pc[k]);
             float gx = 0.f, gy = 0.f, ga = 0.f;
-            e_loc += wall_energy_grad(px[k], py[k], pc[k], ps[k], L, gx, gy, ga);
+            e_loc += e_units(wall_energy_grad(px[k], py[k], pc[k], ps[k], L, gx, gy, ga));
             if (gdst) {  // the wall term goes straight out; pair terms are added at the end
                 gdst[3 * i] = gx;
                 gdst[3 * i + 1] = gy;
@@ -411,24 +423,6 @@ __global__ void __launch_bounds__(W * 32) sat_energy_warp_kernel(int configs, in
         }
     }
     __syncwarp();
-    for (int c = lane; c < ncell; c += 32) {  // each cell's entries by original index
-        const int a = cells[c], b = cells[c + 1];
-        for (int u = a + 1; u < b; ++u) {
-            const float2 kxy = sxy[u], kcs = scs[u];
-            const uint8_t km = orig[u];
-            int w = u - 1;
-            while (w >= a && orig[w] > km) {
-                sxy[w + 1] = sxy[w];
-                scs[w + 1] = scs[w];
-                orig[w + 1] = orig[w];
-                --w;
-            }
-            sxy[w + 1] = kxy;
-            scs[w + 1] = kcs;
-            orig[w + 1] = km;
-        }
-    }
-    __syncwarp();
 
     // 3. broad phase into the warp queue, narrow phase 32 pairs at a time
     uint32_t cand_loc = 0;
@@ -438,7 +432,7 @@ __global__ void __launch_bounds__(W * 32) sat_energy_warp_kernel(int configs, in
         const float2 P = sxy[p], Q = sxy[q], Pc = scs[p], Qc = scs[q];
         PairGrad g;
         if (sat_pair_grad(Q.x - P.x, Q.y - P.y, Pc.x, Pc.y, Qc.x, Qc.y, g)) {
-            e_loc += g.e;
+            e_loc += e_units(g.e);
             const int i = orig[p], j = orig[q];
             atomicAdd(gq + 3 * i, gq_units(g.px));
             atomicAdd(gq + 3 * i + 1, gq_units(g.py));
@@ -505,7 +499,7 @@ __global__ void __launch_bounds__(W * 32) sat_energy_warp_kernel(int configs, in
         cand_loc += __shfl_xor_sync(0xffffffffu, cand_loc, o);
     }
     if (lane == 0) {
-        energy[cfg] = e_loc;
+        energy[cfg] = (float)((double)e_loc * (1.0 / kEUnit));
         if (COUNT) cand[cfg] = cand_loc;
     }
     if (gdst) {
