@@ -287,8 +287,10 @@ def run_sqs(args, D: Dist):
     clk = clocks.stop()
     D.barrier()
     total_ms = D.max(sum(kernel_ms))
-    all_pairs = D.sum(pairs_per_step * K)
-    value = all_pairs / (total_ms / 1e3)
+    cand_pairs = D.sum(pairs_per_step * K)
+    value = cand_pairs / (total_ms / 1e3)
+    # the same time counted as all-pairs tests (n (n - 1) / 2 per configuration)
+    all_pairs_per_s = D.sum(configs * n * (n - 1) // 2 * K) / (total_ms / 1e3)
     ms_per_step = total_ms / K
     mean_ms = sum(kernel_ms) / len(kernel_ms)
 
@@ -325,7 +327,10 @@ def run_sqs(args, D: Dist):
         data="synthetic",
         config=dict(workload=f"SAT energy+gradient, {configs} configs x n={n}, FP32 cell list",
                     configs=configs, n=n, seed=SEED, side=float(s32[0]), l2="flushed before every launch",
-                    cta_threads=threads or 64, parallelism=f"replicas x{D.world}", device=name, sm_count=sms),
+                    cta_threads=threads if threads > 0 else 32 * (-threads or 4),
+                    kernel_shape=(f"one warp per configuration, {-threads or 4} per CTA" if threads <= 0 and n <= 256
+                                  else "one CTA per configuration"),
+                    parallelism=f"replicas x{D.world}", device=name, sm_count=sms),
         e2e=dict(value=e2e_val, unit=UNIT, h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h,
                  steps=e2e_steps, call="sqs_sat_energy_host (pinned host buffers)"),
         roofline=dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
@@ -333,6 +338,7 @@ def run_sqs(args, D: Dist):
                       algorithmic_bytes_per_launch=algo, kernel=kernel_name),
         gpu_launches=launches,
         pairs_per_step=pairs_per_step,
+        all_pairs_equivalent_per_s=all_pairs_per_s,
         clocks=clk,
     )
     if D.rank == 0:
