@@ -449,8 +449,14 @@ def bench_served(ctx, jobs, plain, rate: float, slice_proposals: int = 4000):
     p_res, p_service = plain
     p_stats = plain_stats(p_res[:count], p_service[:count], arr)
     same_L = all((a or {}).get("L") == (b or {}).get("L") for a, b in zip(served, p_res[:count]))
+    # annealing work done per second of the stream: against the batched
+    # launch's rate it says how busy the stream kept the GPU
+    props = sum(int((r or {}).get("proposals", 0)) for r in served)
+    s_stats["proposals_per_s"] = props / s_stats["seconds"] if s_stats["seconds"] > 0 else 0.0
+    p_stats["proposals_per_s"] = props / p_stats["seconds"] if p_stats["seconds"] > 0 else 0.0
     return dict(workload=f"{count} jobs, Poisson {rate:g}/s, n log-uniform [5, 1000], 16/32/64 replicas, "
-                         f"{jobs[0].sweeps} sweeps", served=s_stats, plain=p_stats, equal_final_L=same_L, server_counters=counters,
+                         f"{jobs[0].sweeps} sweeps", served=s_stats, plain=p_stats, equal_final_L=same_L,
+                server_counters=counters,
                 served_over_plain=s_stats["certified_jobs_per_s"] / max(p_stats["certified_jobs_per_s"], 1e-12))
 
 
