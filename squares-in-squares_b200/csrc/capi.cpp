@@ -127,6 +127,7 @@ int sqs_ctx_destroy(sqs_ctx* ctx) {
     ctx->d_cert.release();
     ctx->d_tune.release();
     ctx->d_polish.release();
+    ctx->h_cert.release();
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SQS_OK;

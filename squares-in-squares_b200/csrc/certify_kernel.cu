@@ -909,8 +909,14 @@ extern "C" int sqs_certify_batch(sqs_ctx* ctx, int count, const int32_t* n_of, c
     SQS_REQUIRE(S < (1ll << 30), "%lld squares in one call (limit 2^30)", (long long)S);
     // 2. square ids and literal slices (round-tripped when asked), host
     //    threads over contiguous ranges of packings with equal square counts
-    std::vector<int64_t> raw_off((size_t)(3 * S));
-    std::vector<int32_t> raw_len((size_t)(3 * S));
+    // Literal slice tables, written straight into the context's pinned
+    // staging: no zero fill, no page faults after the first call, and an
+    // upload at the full host-link rate.  Every slot of a live packing is
+    // written below; slots of packings found invalid are never read.
+    const size_t n3 = (size_t)(3 * S);
+    if (int r = ctx->h_cert.reserve(n3 * (sizeof(int64_t) + sizeof(int32_t)) + 16)) return r;
+    int64_t* const raw_off = (int64_t*)ctx->h_cert.p;
+    int32_t* const raw_len = (int32_t*)(raw_off + n3);
     const int nt = count >= 64 ? (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency())) : 1;
     std::vector<int> p_lo((size_t)nt + 1, count);
     {
@@ -1002,7 +1008,7 @@ extern "C" int sqs_certify_batch(sqs_ctx* ctx, int count, const int32_t* n_of, c
     struct Seg { size_t off, bytes; };
     size_t tot = 0;
     auto seg = [&](size_t bytes) { Seg s{tot, bytes}; tot += (bytes + 255) & ~(size_t)255; return s; };
-    const Seg g_text = seg(blob_bytes), g_off = seg(raw_off.size() * 8 + 8), g_len = seg(raw_len.size() * 4 + 4);
+    const Seg g_text = seg(blob_bytes), g_off = seg(n3 * 8 + 8), g_len = seg(n3 * 4 + 4);
     const Seg g_n = seg((size_t)count * 4), g_s0 = seg((size_t)count * 8);
     const Seg g_b0 = seg(bk[0].size() * 4 + 4), g_b1 = seg(bk[1].size() * 4 + 4), g_b2 = seg(bk[2].size() * 4 + 4);
     const Seg g_lits = seg((size_t)(3 * S + 3) * sizeof(Lit)), g_out = seg((size_t)count * sizeof(PkOut));
@@ -1015,8 +1021,8 @@ extern "C" int sqs_certify_batch(sqs_ctx* ctx, int count, const int32_t* n_of, c
         return SQS_OK;
     };
     if (int r = up(g_text, blob, do_rt ? rt_text.size() : (size_t)lit_off[3 * row_start[count]])) return r;
-    if (int r = up(g_off, raw_off.data(), raw_off.size() * 8)) return r;
-    if (int r = up(g_len, raw_len.data(), raw_len.size() * 4)) return r;
+    if (int r = up(g_off, raw_off, n3 * 8)) return r;
+    if (int r = up(g_len, raw_len, n3 * 4)) return r;
     if (int r = up(g_n, pk_n.data(), (size_t)count * 4)) return r;
     if (int r = up(g_s0, pk_sq0.data(), (size_t)count * 8)) return r;
     if (int r = up(g_b0, bk[0].data(), bk[0].size() * 4)) return r;

@@ -73,6 +73,7 @@ struct sqs_ctx {
     sqs::DevBuf d_cert;  // the certifier's per-square interval cache
     sqs::DevBuf d_tune;  // the annealer autotuner's trial state
     sqs::DevBuf d_polish;  // standalone polish batches
+    sqs::HostBuf h_cert;   // the certifier's literal slice tables (pinned)
 };
 
 namespace sqs {

@@ -90,6 +90,7 @@ constexpr int kRetirers = 1;
 constexpr size_t kRetireStaging = (size_t)64 << 20;
 constexpr size_t kRetireCache = (size_t)32 << 20;
 constexpr size_t kRetirePolish = (size_t)8 << 20;
+constexpr size_t kRetireHost = (size_t)8 << 20;  // pinned literal slice tables
 
 // A retirement thread's own context (buffers, a stream of the highest
 // priority) and device list of job slots.
@@ -324,7 +325,8 @@ extern "C" int sqs_server_create(sqs_ctx* ctx, size_t hbm_bytes, int max_active,
         // every slice on the GPU and holds up the caller's thread meanwhile.
         if (e == cudaSuccess && (w.ctx->d_misc.reserve(kRetireStaging) != SQS_OK ||
                                  w.ctx->d_cert.reserve(kRetireCache) != SQS_OK ||
-                                 w.ctx->d_polish.reserve(kRetirePolish) != SQS_OK))
+                                 w.ctx->d_polish.reserve(kRetirePolish) != SQS_OK ||
+                                 w.ctx->h_cert.reserve(kRetireHost) != SQS_OK))
             e = cudaErrorMemoryAllocation;
     }
     if (e == cudaSuccess) {
