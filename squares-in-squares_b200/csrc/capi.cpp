@@ -128,6 +128,7 @@ int sqs_ctx_destroy(sqs_ctx* ctx) {
     ctx->d_tune.release();
     ctx->d_polish.release();
     ctx->h_cert.release();
+    ctx->h_text.release();
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SQS_OK;

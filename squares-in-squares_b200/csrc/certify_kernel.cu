@@ -718,6 +718,12 @@ static int host_lit(const char* s, Lit& L) {
     return SQS_OK;
 }
 
+// Literal texts of this size range are staged in pinned memory for the
+// upload (larger ones are uploaded from the caller's memory, rather than
+// pinning gigabytes of host memory).
+constexpr size_t kPinnedTextMin = (size_t)4 << 20;
+constexpr size_t kPinnedTextMax = (size_t)1 << 30;
+
 static int upload_consts(int device) {
     static std::atomic<bool> done[64];
     static std::mutex mu;  // several host threads may certify at once
@@ -928,7 +934,21 @@ extern "C" int sqs_certify_batch(sqs_ctx* ctx, int count, const int32_t* n_of, c
     }
     std::vector<std::string> rt((size_t)nt);  // round-tripped text of each thread's packings
     std::vector<int64_t> bad_row((size_t)nt, -1);
+    // A large literal text is staged in pinned memory too, each thread copying
+    // the span of its own packings (the first from offset 0), so that it
+    // uploads at the full host-link rate.
+    const size_t text_bytes = (size_t)lit_off[3 * row_start[count]];
+    char* h_text = nullptr;
+    if (!do_rt && text_bytes >= kPinnedTextMin && text_bytes <= kPinnedTextMax) {
+        if (int r = ctx->h_text.reserve(text_bytes)) return r;
+        h_text = (char*)ctx->h_text.p;
+    }
     auto slice = [&](int t) {
+        if (h_text) {
+            const int64_t a = t == 0 ? 0 : lit_off[3 * row_start[p_lo[(size_t)t]]];
+            const int64_t b = t + 1 == nt ? (int64_t)text_bytes : lit_off[3 * row_start[p_lo[(size_t)t + 1]]];
+            if (b > a && a >= 0 && (size_t)b <= text_bytes) std::memcpy(h_text + a, text + a, (size_t)(b - a));
+        }
         std::vector<int64_t> row_of;
         for (int p = p_lo[(size_t)t]; p < p_lo[(size_t)t + 1]; ++p) {
             if (!live[(size_t)p]) continue;
@@ -993,7 +1013,7 @@ extern "C" int sqs_certify_batch(sqs_ctx* ctx, int count, const int32_t* n_of, c
         rt_text.reserve(base);
         for (int t = 0; t < nt; ++t) rt_text += rt[(size_t)t];
     }
-    const char* blob = do_rt ? rt_text.data() : text;
+    const char* blob = do_rt ? rt_text.data() : (h_text ? h_text : text);
     size_t blob_bytes = do_rt ? rt_text.size() : (size_t)lit_off[3 * row_start[count]];
     if (blob_bytes == 0) blob_bytes = 1;
     // buckets by n

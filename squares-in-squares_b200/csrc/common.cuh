@@ -74,6 +74,7 @@ struct sqs_ctx {
     sqs::DevBuf d_tune;  // the annealer autotuner's trial state
     sqs::DevBuf d_polish;  // standalone polish batches
     sqs::HostBuf h_cert;   // the certifier's literal slice tables (pinned)
+    sqs::HostBuf h_text;   // the certifier's literal text, when large (pinned)
 };
 
 namespace sqs {
