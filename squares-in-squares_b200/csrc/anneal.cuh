@@ -57,6 +57,9 @@ constexpr float kEScale = 1099511627776.0f;  // 2^40
 
 enum : int32_t { kRunning = 0, kFinished = 1, kErrCells = -2, kErrInput = -3 };
 
+// Dynamic shared memory a CTA of the annealer may ask for (the static part reserved).
+constexpr size_t kAnnealSmemLimit = 232448 - 4096;
+
 // Shared-memory bytes one replica needs: (x, y, cos, sin), angle, cell counts, cell slots.
 __host__ __device__ inline int64_t replica_smem_bytes(int n, int Gmax) {
     int64_t b = (int64_t)n * 16 + (int64_t)n * 4;

@@ -25,7 +25,7 @@
 namespace sqs {
 namespace ann {
 
-constexpr size_t kSmemLimit = 232448 - 4096;  // dynamic shared memory per CTA (static part reserved)
+constexpr size_t kSmemLimit = kAnnealSmemLimit;
 
 // Smallest cluster (CTAs per job), from cs_min up, whose per-CTA replica
 // share fits, with cells of side at least `cell`.
@@ -252,7 +252,8 @@ static int trial_ms(sqs_ctx* ctx, const sqs_job& J0, const Plan& p, int copies, 
             SQS_CUDA(cudaMemcpyAsync(D + o_pos + sizeof(float4) * (size_t)pe * c, pos.data(), sizeof(float4) * pos.size(),
                                      cudaMemcpyHostToDevice, ctx->stream));
         SQS_CUDA(cudaEventRecord(ctx->ev[60], ctx->stream));
-        if (int r = launch_anneal(ctx->stream, copies, p.cs, p.Rl, (size_t)(p.rb * p.Rl), d.flags != 0, (const int32_t*)(D + o_list),
+        if (int r = launch_anneal(ctx->stream, copies, p.cs, p.Rl, anneal_smem(p.cs, p.Rl, p.rb, J.n, d.flags != 0),
+                                  d.flags != 0, (const int32_t*)(D + o_list),
                                   (const JobDev*)(D + o_jd), (JobMut*)(D + o_jm), (float4*)(D + o_pos),
                                   (double*)(D + o_best), sweeps))
             return r;
@@ -271,7 +272,8 @@ static int copies_for(const sqs_job& J, const Plan& p, int mode, int* copies) {
     *copies = 1;
     if (mode & SQS_TUNE_LATENCY) return SQS_OK;
     int waves = 1;
-    if (int r = anneal_max_clusters(p.cs, p.Rl, (size_t)(p.rb * p.Rl), (J.flags & (SQS_JOB_ADAPT | SQS_JOB_COLLECTIVE | SQS_JOB_KICK | SQS_JOB_SERIAL)) != 0, &waves)) return r;
+    const bool moves = (J.flags & (SQS_JOB_ADAPT | SQS_JOB_COLLECTIVE | SQS_JOB_KICK | SQS_JOB_SERIAL)) != 0;
+    if (int r = anneal_max_clusters(p.cs, p.Rl, anneal_smem(p.cs, p.Rl, p.rb, J.n, moves), moves, &waves)) return r;
     const size_t per = sizeof(float4) * (size_t)job_pos_elems(J) + sizeof(double) * 3 * (size_t)J.n + 1024;
     *copies = (int)std::max<int64_t>(1, std::min<int64_t>(waves, (int64_t)(kTuneBytes / per)));
     return SQS_OK;
@@ -593,10 +595,14 @@ extern "C" int sqs_anneal_batch(sqs_ctx* ctx, const sqs_job* jobs, int njobs, in
     std::vector<std::tuple<int, int, int>> keys;
     for (auto& kv : groups) {
         int64_t rb = 0;
-        for (int j : kv.second) rb = std::max(rb, plan[(size_t)j].rb);
+        int nmax = 1;
+        for (int j : kv.second) {
+            rb = std::max(rb, plan[(size_t)j].rb);
+            nmax = std::max(nmax, jobs[j].n);
+        }
         spans.push_back({lists.size(), kv.second.size()});
         lists.insert(lists.end(), kv.second.begin(), kv.second.end());
-        smems.push_back((size_t)(rb * std::get<1>(kv.first)));
+        smems.push_back(anneal_smem(std::get<0>(kv.first), std::get<1>(kv.first), rb, nmax, std::get<2>(kv.first) != 0));
         keys.push_back(kv.first);
     }
     SQS_CUDA(cudaMemcpyAsync(d_list, lists.data(), sizeof(int32_t) * lists.size(), cudaMemcpyHostToDevice,

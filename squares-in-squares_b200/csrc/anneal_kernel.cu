@@ -22,6 +22,9 @@
 //     (no per-epoch device-to-host round trip).
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
+#include <tuple>
+#include <mutex>
+#include <map>
 
 #include <cmath>
 
@@ -692,7 +695,7 @@ template <bool MOVES>
 __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __restrict__ job_list,
                                                       const JobDev* __restrict__ jdev, JobMut* __restrict__ jmut,
                                                       float4* __restrict__ pos, double* __restrict__ best,
-                                                      int slice_sweeps) {
+                                                      int slice_sweeps, int dyn_bytes) {
     cg::cluster_group cluster = cg::this_cluster();
     __shared__ CtaShared S;
     extern __shared__ __align__(16) unsigned char dyn[];
@@ -992,8 +995,12 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                 if (w == cold % Rl && lane == 0) S.qE = E;
                 __syncthreads();
                 const Rep cr = rep_view(dyn + (cold % Rl) * rb, n, jd.Gmax);
-                const long long qe_out = quench_cta(cr, n, g, L, jd.quench_iters, pos + jd.scr_off,
-                                                    pos + jd.scr_off + n, S.qE, S.red);
+                // the quench's gradient sums and saved state: in shared memory
+                // after the replicas when the launch left room, else in HBM
+                float4* qs = (int64_t)dyn_bytes >= (int64_t)Rl * rb + 32 * (int64_t)n
+                                 ? reinterpret_cast<float4*>(dyn + (int64_t)Rl * rb)
+                                 : pos + jd.scr_off;
+                const long long qe_out = quench_cta(cr, n, g, L, jd.quench_iters, qs, qs + n, S.qE, S.red);
                 if (w == cold % Rl) E = qe_out;
                 __syncthreads();
             }
@@ -1198,9 +1205,36 @@ int launch_anneal(cudaStream_t stream, int njobs, int cs, int Rl, size_t smem, b
     if (int r = prime_anneal()) return r;
     cudaLaunchAttribute attr[1];
     const cudaLaunchConfig_t cfg = anneal_config(njobs, cs, Rl, smem, stream, attr);
-    if (moves) SQS_CUDA(cudaLaunchKernelEx(&cfg, anneal_kernel<true>, job_list, jdev, jmut, pos, best, slice));
-    else SQS_CUDA(cudaLaunchKernelEx(&cfg, anneal_kernel<false>, job_list, jdev, jmut, pos, best, slice));
+    if (moves) SQS_CUDA(cudaLaunchKernelEx(&cfg, anneal_kernel<true>, job_list, jdev, jmut, pos, best, slice, (int)smem));
+    else SQS_CUDA(cudaLaunchKernelEx(&cfg, anneal_kernel<false>, job_list, jdev, jmut, pos, best, slice, (int)smem));
     return SQS_OK;
+}
+
+// Shared memory of a launch whose largest job needs rb bytes a replica and
+// has n_max squares: the replicas, plus room for the checkpoint quench's
+// scratch (2 n float4) when that fits and keeps as many clusters resident --
+// the quench then runs on shared instead of global memory (same results).
+size_t anneal_smem(int cs, int Rl, int64_t rb, int n_max, bool moves) {
+    const size_t base = (size_t)(rb * Rl), with = base + 32 * (size_t)n_max;
+    if (with > kAnnealSmemLimit) return base;
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int, size_t, size_t, bool>, size_t> memo;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return base;
+    const auto key = std::make_tuple(dev, cs, Rl, base, with, moves);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = memo.find(key);
+        if (it != memo.end()) return it->second;
+    }
+    int a = 0, b = 0;
+    size_t pick = base;
+    if (anneal_max_clusters(cs, Rl, base, moves, &a) == SQS_OK && anneal_max_clusters(cs, Rl, with, moves, &b) == SQS_OK &&
+        b >= a)
+        pick = with;
+    std::lock_guard<std::mutex> lk(mu);
+    memo[key] = pick;
+    return pick;
 }
 
 }  // namespace ann

@@ -449,6 +449,7 @@ int launch_idle(sqs_server* s, const std::vector<int32_t>& fin, int& launched) {
     using Key = std::tuple<int, int, int>;
     std::map<Key, std::vector<int32_t>> groups;
     std::map<Key, int64_t> rb;
+    std::map<Key, int> nmax;
     std::vector<uint8_t> retiring((size_t)s->max_active, 0);
     for (int32_t k : fin) retiring[(size_t)k] = 1;
     for (int k = 0; k < s->max_active; ++k) {
@@ -457,6 +458,7 @@ int launch_idle(sqs_server* s, const std::vector<int32_t>& fin, int& launched) {
         const Key key = std::make_tuple(j.plan.cs, j.plan.Rl, (int)(j.jd.flags != 0));
         groups[key].push_back(k);
         rb[key] = std::max(rb[key], j.plan.rb);
+        nmax[key] = std::max(nmax[key], j.job.n);
     }
     auto work = [&](int32_t k) {
         const SJob& j = s->jobs[s->slot_job[(size_t)k]];
@@ -478,7 +480,9 @@ int launch_idle(sqs_server* s, const std::vector<int32_t>& fin, int& launched) {
         SQS_CUDA(cudaStreamWaitEvent(c->st, s->admitted, 0));  // the jobs' uploads are done first
         SQS_CUDA(cudaMemcpyAsync(c->d_list, list.data(), sizeof(int32_t) * (size_t)cnt, cudaMemcpyHostToDevice, c->st));
         if (int r = launch_anneal(c->st, cnt, std::get<0>(o.second), std::get<1>(o.second),
-                                  (size_t)(rb[o.second] * std::get<1>(o.second)), std::get<2>(o.second) != 0, c->d_list,
+                                  anneal_smem(std::get<0>(o.second), std::get<1>(o.second), rb[o.second],
+                                              nmax[o.second], std::get<2>(o.second) != 0),
+                                  std::get<2>(o.second) != 0, c->d_list,
                                   s->d_jd, s->d_jm, (float4*)s->arena, (double*)s->arena, std::max(1, s->slice)))
             return r;
         if (int r = launch_gather_status(c->st, cnt, c->d_list, s->d_jm, c->d_status)) return r;
