@@ -301,14 +301,15 @@ int sqs_autotune(sqs_ctx* ctx, const sqs_job* job, int mode, sqs_tuning* out);
 /* ------------------------------------------------------------- serving */
 /* Continuous-batching request loop for anneal-and-certify jobs on one GPU.
  * Jobs are admitted while a job slot is free and their state (replicas,
- * scratch, best packing) fits an HBM arena of `hbm_bytes`; every step runs
- * one slice of `slice_sweeps` sweeps for all admitted jobs side by side in
- * one launch per cluster shape (slice_sweeps < 0: every job runs about
- * -slice_sweeps proposals per replica per step -- ceil(-slice_sweeps / n)
- * sweeps rounded up to whole exchange intervals -- so a step takes about
- * the same time for small and large jobs), their state resident between slices, then
- * polishes, certifies and retires the finished ones so queued jobs take
- * their place.  Each job's result equals its sqs_anneal_batch result.
+ * scratch, best packing) fits an HBM arena of `hbm_bytes`.  Each job runs in
+ * slices of `slice_sweeps` sweeps (slice_sweeps < 0: about -slice_sweeps
+ * proposals per replica -- ceil(-slice_sweeps / n) sweeps rounded up to
+ * whole exchange intervals -- so a slice takes about the same time for small
+ * and large jobs), launched together with the other idle jobs of its cluster
+ * shape as soon as its previous slice ends, its state resident between
+ * slices.  Finished jobs are polished, certified and retired by the server's
+ * own thread, and queued jobs take their place.  Each job's result equals
+ * its sqs_anneal_batch result.
  * Replaces one-search-process-per-job campaigns (scheduler.run_gpu,
  * cuda/scheduler.py:80-89) and their VRAM-budgeted worker admission
  * (cpp_loop.concurrency, cuda/cpp_loop.py:41-45). */

@@ -338,7 +338,8 @@ __device__ long long full_energy_cta(const Rep& R, int n, const Grid& g, float L
 constexpr float kQScale = 1048576.0f;
 __device__ __forceinline__ int qg(float v) { return __float2int_rn(v * kQScale); }
 
-// The quench of the coldest replica by the whole CTA, one thread per square:
+// The quench of the coldest replica by the whole CTA, one thread per (square,
+// neighbouring cell) work item for the gradient and the energies:
 // Jacobi gradient descent on the overlap energy with a backtracking step
 // (up to 6 trials per iteration), at most `iters` iterations, ending early at
 // zero energy, when no trial improves, or after three accepted steps in a
