@@ -531,10 +531,13 @@ __device__ __noinline__ void make_ivsq(const char* text, const Lit* L3, const Iv
     e.px[3] = fx::isub(x, vx); e.py[3] = fx::isub(y, vy);
 }
 
+// The interval SAT test runs for nearly every undecided pair: its comparisons,
+// additions and subtractions are inlined at 7 limbs (fx::kInlineLimbs), the
+// products stay out of line.
 template <int F>
-__device__ __forceinline__ Fix<F> fmin_(const Fix<F>& a, const Fix<F>& b) { return fx::cmp(a, b) < 0 ? a : b; }
+__device__ __forceinline__ Fix<F> fmin_(const Fix<F>& a, const Fix<F>& b) { return fx::cmp<F, true>(a, b) < 0 ? a : b; }
 template <int F>
-__device__ __forceinline__ Fix<F> fmax_(const Fix<F>& a, const Fix<F>& b) { return fx::cmp(a, b) > 0 ? a : b; }
+__device__ __forceinline__ Fix<F> fmax_(const Fix<F>& a, const Fix<F>& b) { return fx::cmp<F, true>(a, b) > 0 ? a : b; }
 
 // sat_check_interval_cached (certifier.cpp:638-703)
 template <int F>
@@ -542,13 +545,13 @@ __device__ __noinline__ int iv_sat(const IvSq<F>& p, const IvSq<F>& q) {
     Fix<F> z;
     fx::set_zero(z);
     if (p.flat && q.flat) {
-        const Iv<F> ox = fx::isub(Iv<F>{fmin_(p.x1.lo, q.x1.lo), fmin_(p.x1.hi, q.x1.hi)},
+        const Iv<F> ox = fx::isub<F, true>(Iv<F>{fmin_(p.x1.lo, q.x1.lo), fmin_(p.x1.hi, q.x1.hi)},
                                   Iv<F>{fmax_(p.x0.lo, q.x0.lo), fmax_(p.x0.hi, q.x0.hi)});
-        if (fx::cmp(ox.hi, z) <= 0) return 1;
-        const Iv<F> oy = fx::isub(Iv<F>{fmin_(p.y1.lo, q.y1.lo), fmin_(p.y1.hi, q.y1.hi)},
+        if (fx::cmp<F, true>(ox.hi, z) <= 0) return 1;
+        const Iv<F> oy = fx::isub<F, true>(Iv<F>{fmin_(p.y1.lo, q.y1.lo), fmin_(p.y1.hi, q.y1.hi)},
                                   Iv<F>{fmax_(p.y0.lo, q.y0.lo), fmax_(p.y0.hi, q.y0.hi)});
-        if (fx::cmp(oy.hi, z) <= 0) return 1;
-        if (fx::cmp(ox.lo, z) <= 0 || fx::cmp(oy.lo, z) <= 0) return 0;
+        if (fx::cmp<F, true>(oy.hi, z) <= 0) return 1;
+        if (fx::cmp<F, true>(ox.lo, z) <= 0 || fx::cmp<F, true>(oy.lo, z) <= 0) return 0;
         return -1;
     }
     bool open = false;
@@ -558,8 +561,8 @@ __device__ __noinline__ int iv_sat(const IvSq<F>& p, const IvSq<F>& q) {
         const Iv<F>& ay = (a & 1) ? o.c : o.s;
         Iv<F> mn1, mx1, mn2, mx2;
         for (int k = 0; k < 4; ++k) {
-            const Iv<F> u = fx::iadd(fx::imul(ax, p.px[k]), fx::imul(ay, p.py[k]));
-            const Iv<F> v = fx::iadd(fx::imul(ax, q.px[k]), fx::imul(ay, q.py[k]));
+            const Iv<F> u = fx::iadd<F, true>(fx::imul(ax, p.px[k]), fx::imul(ay, p.py[k]));
+            const Iv<F> v = fx::iadd<F, true>(fx::imul(ax, q.px[k]), fx::imul(ay, q.py[k]));
             if (k == 0) {
                 mn1 = mx1 = u;
                 mn2 = mx2 = v;
@@ -570,10 +573,10 @@ __device__ __noinline__ int iv_sat(const IvSq<F>& p, const IvSq<F>& q) {
             mn2.lo = fmin_(v.lo, mn2.lo); mn2.hi = fmin_(v.hi, mn2.hi);
             mx2.lo = fmax_(v.lo, mx2.lo); mx2.hi = fmax_(v.hi, mx2.hi);
         }
-        const Iv<F> ov = fx::isub(Iv<F>{fmin_(mx1.lo, mx2.lo), fmin_(mx1.hi, mx2.hi)},
+        const Iv<F> ov = fx::isub<F, true>(Iv<F>{fmin_(mx1.lo, mx2.lo), fmin_(mx1.hi, mx2.hi)},
                                   Iv<F>{fmax_(mn1.lo, mn2.lo), fmax_(mn1.hi, mn2.hi)});
-        if (fx::cmp(ov.hi, z) <= 0) return 1;
-        if (fx::cmp(ov.lo, z) <= 0) open = true;
+        if (fx::cmp<F, true>(ov.hi, z) <= 0) return 1;
+        if (fx::cmp<F, true>(ov.lo, z) <= 0) open = true;
     }
     return open ? 0 : -1;
 }

@@ -30,6 +30,9 @@ namespace sqs {
 namespace fx {
 
 constexpr uint32_t B9 = 1000000000u;
+// Widest fraction whose comparison and addition a caller may ask to have
+// inlined (the hot 7-limb interval SAT test: values stay in registers).
+constexpr int kInlineLimbs = 7;
 
 template <int F>
 struct Fix {
@@ -77,24 +80,42 @@ FX_HD double approx(const Fix<F>& a) {
     return a.neg ? -v : v;
 }
 
-template <int F>
-FX_HEAVY int mag_cmp(const Fix<F>& a, const Fix<F>& b) {
+template <int F, bool IN>
+FX_HD int mag_cmp_body(const Fix<F>& a, const Fix<F>& b) {
     for (int i = 0; i <= F; ++i)
         if (a.d[i] != b.d[i]) return a.d[i] < b.d[i] ? -1 : 1;
     return 0;
 }
-
 template <int F>
-FX_HEAVY int cmp(const Fix<F>& a, const Fix<F>& b) {
+FX_HEAVY int mag_cmp_out(const Fix<F>& a, const Fix<F>& b) { return mag_cmp_body<F, false>(a, b); }
+// IN: inline at up to kInlineLimbs limbs (for the interval SAT test);
+// otherwise the out-of-line routine
+template <int F, bool IN = false>
+FX_HD int mag_cmp(const Fix<F>& a, const Fix<F>& b) {
+    if constexpr (IN && F <= kInlineLimbs) return mag_cmp_body<F, true>(a, b);
+    else return mag_cmp_out<F>(a, b);
+}
+
+template <int F, bool IN>
+FX_HD int cmp_body(const Fix<F>& a, const Fix<F>& b) {
     const bool za = is_zero(a), zb = is_zero(b);
     if (za && zb) return 0;
     if (a.neg != b.neg) return a.neg ? -1 : 1;
-    const int c = mag_cmp(a, b);
+    const int c = mag_cmp<F, IN>(a, b);
     return a.neg ? -c : c;
 }
-
 template <int F>
-FX_HEAVY Fix<F> mag_add(const Fix<F>& a, const Fix<F>& b, uint32_t neg) {
+FX_HEAVY int cmp_out(const Fix<F>& a, const Fix<F>& b) { return cmp_body<F, false>(a, b); }
+// IN: inline at up to kInlineLimbs limbs (for the interval SAT test);
+// otherwise the out-of-line routine
+template <int F, bool IN = false>
+FX_HD int cmp(const Fix<F>& a, const Fix<F>& b) {
+    if constexpr (IN && F <= kInlineLimbs) return cmp_body<F, true>(a, b);
+    else return cmp_out<F>(a, b);
+}
+
+template <int F, bool IN>
+FX_HD Fix<F> mag_add_body(const Fix<F>& a, const Fix<F>& b, uint32_t neg) {
     Fix<F> r;
     uint32_t c = 0;
     for (int i = F; i >= 1; --i) {
@@ -107,9 +128,18 @@ FX_HEAVY Fix<F> mag_add(const Fix<F>& a, const Fix<F>& b, uint32_t neg) {
     fix_zero(r);
     return r;
 }
-
 template <int F>
-FX_HEAVY Fix<F> mag_sub(const Fix<F>& a, const Fix<F>& b, uint32_t neg) {  // |a| >= |b|
+FX_HEAVY Fix<F> mag_add_out(const Fix<F>& a, const Fix<F>& b, uint32_t neg) { return mag_add_body<F, false>(a, b, neg); }
+// IN: inline at up to kInlineLimbs limbs (for the interval SAT test);
+// otherwise the out-of-line routine
+template <int F, bool IN = false>
+FX_HD Fix<F> mag_add(const Fix<F>& a, const Fix<F>& b, uint32_t neg) {
+    if constexpr (IN && F <= kInlineLimbs) return mag_add_body<F, true>(a, b, neg);
+    else return mag_add_out<F>(a, b, neg);
+}
+
+template <int F, bool IN>
+FX_HD Fix<F> mag_sub_body(const Fix<F>& a, const Fix<F>& b, uint32_t neg) {  // |a| >= |b|
     Fix<F> r;
     uint32_t br = 0;
     for (int i = F; i >= 1; --i) {
@@ -122,17 +152,35 @@ FX_HEAVY Fix<F> mag_sub(const Fix<F>& a, const Fix<F>& b, uint32_t neg) {  // |a
     fix_zero(r);
     return r;
 }
-
 template <int F>
-FX_HEAVY Fix<F> add(const Fix<F>& a, const Fix<F>& b) {
-    if (a.neg == b.neg) return mag_add(a, b, a.neg);
-    const int c = mag_cmp(a, b);
+FX_HEAVY Fix<F> mag_sub_out(const Fix<F>& a, const Fix<F>& b, uint32_t neg) { return mag_sub_body<F, false>(a, b, neg); }
+// IN: inline at up to kInlineLimbs limbs (for the interval SAT test);
+// otherwise the out-of-line routine
+template <int F, bool IN = false>
+FX_HD Fix<F> mag_sub(const Fix<F>& a, const Fix<F>& b, uint32_t neg) {
+    if constexpr (IN && F <= kInlineLimbs) return mag_sub_body<F, true>(a, b, neg);
+    else return mag_sub_out<F>(a, b, neg);
+}
+
+template <int F, bool IN>
+FX_HD Fix<F> add_body(const Fix<F>& a, const Fix<F>& b) {
+    if (a.neg == b.neg) return mag_add<F, IN>(a, b, a.neg);
+    const int c = mag_cmp<F, IN>(a, b);
     if (c == 0) {
         Fix<F> z;
         set_zero(z);
         return z;
     }
-    return c > 0 ? mag_sub(a, b, a.neg) : mag_sub(b, a, b.neg);
+    return c > 0 ? mag_sub<F, IN>(a, b, a.neg) : mag_sub<F, IN>(b, a, b.neg);
+}
+template <int F>
+FX_HEAVY Fix<F> add_out(const Fix<F>& a, const Fix<F>& b) { return add_body<F, false>(a, b); }
+// IN: inline at up to kInlineLimbs limbs (for the interval SAT test);
+// otherwise the out-of-line routine
+template <int F, bool IN = false>
+FX_HD Fix<F> add(const Fix<F>& a, const Fix<F>& b) {
+    if constexpr (IN && F <= kInlineLimbs) return add_body<F, true>(a, b);
+    else return add_out<F>(a, b);
 }
 
 template <int F>
@@ -142,8 +190,8 @@ FX_HD Fix<F> neg(Fix<F> a) {
     return a;
 }
 
-template <int F>
-FX_HD Fix<F> sub(const Fix<F>& a, const Fix<F>& b) { return add(a, neg(b)); }
+template <int F, bool IN = false>
+FX_HD Fix<F> sub(const Fix<F>& a, const Fix<F>& b) { return add<F, IN>(a, neg(b)); }
 
 template <int F>
 FX_HD void bump(Fix<F>& a) {  // |a| += 1 unit of the last limb
@@ -248,10 +296,10 @@ struct Iv {
     Fix<F> lo, hi;
 };
 
-template <int F>
-FX_HD Iv<F> iadd(const Iv<F>& a, const Iv<F>& b) { return {add(a.lo, b.lo), add(a.hi, b.hi)}; }
-template <int F>
-FX_HD Iv<F> isub(const Iv<F>& a, const Iv<F>& b) { return {sub(a.lo, b.hi), sub(a.hi, b.lo)}; }
+template <int F, bool IN = false>
+FX_HD Iv<F> iadd(const Iv<F>& a, const Iv<F>& b) { return {add<F, IN>(a.lo, b.lo), add<F, IN>(a.hi, b.hi)}; }
+template <int F, bool IN = false>
+FX_HD Iv<F> isub(const Iv<F>& a, const Iv<F>& b) { return {sub<F, IN>(a.lo, b.hi), sub<F, IN>(a.hi, b.lo)}; }
 template <int F>
 FX_HD Iv<F> ineg(const Iv<F>& a) { return {neg(a.hi), neg(a.lo)}; }
 // 1: the interval is >= 0; -1: it is <= 0; 0: it straddles zero.
