@@ -331,7 +331,8 @@ __global__ void __launch_bounds__(T) cert_packing_kernel(
     }
     __syncthreads();
 
-    // 2. Fix<9> corners (side) and float geometry, per square
+    // 2. Fix<9> corners (side) and float geometry, per square (the additions
+    // and comparisons inlined; products, parsing and sin/cos out of line)
     Fix<9> mnx, mxx, mny, mxy;
     fx::set_zero(mnx);
     fx::set_zero(mxx);
@@ -341,13 +342,13 @@ __global__ void __launch_bounds__(T) cert_packing_kernel(
     const Consts& C = c_consts;
     for (int i = tid; i < n; i += T) {
         const Lit lx = lits[3 * (s0 + i)], ly = lits[3 * (s0 + i) + 1], la = lits[3 * (s0 + i) + 2];
-        const Fix<9> X = fx::sub(fx::parse<9>(text, lx, 0), org[0]);
-        const Fix<9> Y = fx::sub(fx::parse<9>(text, ly, 0), org[1]);
+        const Fix<9> X = fx::sub<9, true>(fx::parse<9>(text, lx, 0), org[0]);
+        const Fix<9> Y = fx::sub<9, true>(fx::parse<9>(text, ly, 0), org[1]);
         const Fix<9> A = fx::parse<9>(text, la, 0);
         const long long turns = (long long)floor(fx::approx(A) / 6.283185307179586476925);
-        Fix<9> red = fx::sub(A, fx::mul(fx::of_int<9>(turns), C.two_pi9, 0));
-        if (red.neg && !fx::is_zero(red)) red = fx::add(red, C.two_pi9);
-        if (fx::cmp(red, C.two_pi9) >= 0) red = fx::sub(red, C.two_pi9);
+        Fix<9> red = fx::sub<9, true>(A, fx::mul(fx::of_int<9>(turns), C.two_pi9, 0));
+        if (red.neg && !fx::is_zero(red)) red = fx::add<9, true>(red, C.two_pi9);
+        if (fx::cmp<9, true>(red, C.two_pi9) >= 0) red = fx::sub<9, true>(red, C.two_pi9);
         FSq q;
         q.x = fx::approx(X);
         q.y = fx::approx(Y);
@@ -372,12 +373,12 @@ __global__ void __launch_bounds__(T) cert_packing_kernel(
             fx::sincos_point(A, C.half_pi9, sn, cs);
         }
         const Fix<9> hc = fx::mul(C.half9, cs, 0), hs = fx::mul(C.half9, sn, 0);
-        const Fix<9> ux = fx::sub(hc, hs), uy = fx::add(hs, hc);
+        const Fix<9> ux = fx::sub<9, true>(hc, hs), uy = fx::add<9, true>(hs, hc);
         Fix<9> zero;
         fx::set_zero(zero);
-        const Fix<9> vx = fx::sub(zero, fx::add(hc, hs)), vy = fx::sub(hc, hs);
-        const Fix<9> px[4] = {fx::add(X, ux), fx::add(X, vx), fx::sub(X, ux), fx::sub(X, vx)};
-        const Fix<9> py[4] = {fx::add(Y, uy), fx::add(Y, vy), fx::sub(Y, uy), fx::sub(Y, vy)};
+        const Fix<9> vx = fx::sub<9, true>(zero, fx::add<9, true>(hc, hs)), vy = fx::sub<9, true>(hc, hs);
+        const Fix<9> px[4] = {fx::add<9, true>(X, ux), fx::add<9, true>(X, vx), fx::sub<9, true>(X, ux), fx::sub<9, true>(X, vx)};
+        const Fix<9> py[4] = {fx::add<9, true>(Y, uy), fx::add<9, true>(Y, vy), fx::sub<9, true>(Y, uy), fx::sub<9, true>(Y, vy)};
         for (int k = 0; k < 4; ++k) {
             if (!have) {
                 mnx = mxx = px[k];
@@ -385,10 +386,10 @@ __global__ void __launch_bounds__(T) cert_packing_kernel(
                 have = true;
                 continue;
             }
-            if (fx::cmp(px[k], mnx) < 0) mnx = px[k];
-            if (fx::cmp(px[k], mxx) > 0) mxx = px[k];
-            if (fx::cmp(py[k], mny) < 0) mny = py[k];
-            if (fx::cmp(py[k], mxy) > 0) mxy = py[k];
+            if (fx::cmp<9, true>(px[k], mnx) < 0) mnx = px[k];
+            if (fx::cmp<9, true>(px[k], mxx) > 0) mxx = px[k];
+            if (fx::cmp<9, true>(py[k], mny) < 0) mny = py[k];
+            if (fx::cmp<9, true>(py[k], mxy) > 0) mxy = py[k];
         }
     }
     {

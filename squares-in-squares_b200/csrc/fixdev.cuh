@@ -31,8 +31,9 @@ namespace fx {
 
 constexpr uint32_t B9 = 1000000000u;
 // Widest fraction whose comparison and addition a caller may ask to have
-// inlined (the hot 7-limb interval SAT test: values stay in registers).
-constexpr int kInlineLimbs = 7;
+// inlined (the 7-limb interval SAT test and the 9-limb side measurement:
+// values stay in registers).
+constexpr int kInlineLimbs = 9;
 
 template <int F>
 struct Fix {
