@@ -197,6 +197,10 @@ typedef struct sqs_job {
  * integers, so the trajectory is the one-at-a-time trajectory bit for bit;
  * this flag changes only the time taken, and lets a caller check that. */
 #define SQS_JOB_SERIAL 16
+/* Quench every replica, not only the coldest, at each exchange round: the
+ * counterpart of the reference search's per-epoch gradient polish of every
+ * chain (seeded.cu:621-713).  Costs one quench per replica per round. */
+#define SQS_JOB_QUENCH_ALL 32
 /* Pin the launch shape instead: a cluster of `cs` CTAs (1..16; it must
  * divide the replica count and fit) and cell side index k (0: 1.59, 1: 1.75,
  * 2: 1.95, 3: 2.2).  Same trajectory as any other shape (see above). */

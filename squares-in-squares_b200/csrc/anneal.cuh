@@ -31,7 +31,7 @@ struct JobDev {
 
 // Move-set options of a job (the same bits as SQS_JOB_ADAPT, _COLLECTIVE, _KICK).
 // kMoveSerial selects the one-at-a-time kernel instance and changes nothing else
-enum : int32_t { kMoveAdapt = 2, kMoveCollective = 4, kMoveKick = 8, kMoveSerial = 16 };
+enum : int32_t { kMoveAdapt = 2, kMoveCollective = 4, kMoveKick = 8, kMoveSerial = 16, kMoveQuenchAll = 32 };
 
 // Per job, advanced by every slice.
 struct JobMut {

@@ -109,7 +109,7 @@ int prepare_job(const sqs_job& J, int j, JobDev& d, JobMut& m, Plan& p, const Sh
     d.cell = p.cell;
     d.seed = J.seed;
     d.quench_iters = 64;
-    d.flags = J.flags & (kMoveAdapt | kMoveCollective | kMoveKick | kMoveSerial);
+    d.flags = J.flags & (kMoveAdapt | kMoveCollective | kMoveKick | kMoveSerial | kMoveQuenchAll);
     std::memset(&m, 0, sizeof m);
     m.L = (float)J.L0;
     m.best_L = 1e30;
@@ -272,7 +272,7 @@ static int copies_for(const sqs_job& J, const Plan& p, int mode, int* copies) {
     *copies = 1;
     if (mode & SQS_TUNE_LATENCY) return SQS_OK;
     int waves = 1;
-    const bool moves = (J.flags & (SQS_JOB_ADAPT | SQS_JOB_COLLECTIVE | SQS_JOB_KICK | SQS_JOB_SERIAL)) != 0;
+    const bool moves = (J.flags & (SQS_JOB_ADAPT | SQS_JOB_COLLECTIVE | SQS_JOB_KICK | SQS_JOB_SERIAL | SQS_JOB_QUENCH_ALL)) != 0;
     if (int r = anneal_max_clusters(p.cs, p.Rl, anneal_smem(p.cs, p.Rl, p.rb, J.n, moves), moves, &waves)) return r;
     const size_t per = sizeof(float4) * (size_t)job_pos_elems(J) + sizeof(double) * 3 * (size_t)J.n + 1024;
     *copies = (int)std::max<int64_t>(1, std::min<int64_t>(waves, (int64_t)(kTuneBytes / per)));
@@ -403,7 +403,7 @@ static int autotune(sqs_ctx* ctx, const sqs_job& job, int mode, sqs_tuning& out)
 int resolve_job(sqs_ctx* ctx, const sqs_job& job, int mode, sqs_job& eff, Shape& shape) {
     eff = job;
     shape = Shape{};
-    SQS_REQUIRE((job.flags & ~0xfff1f) == 0, "unknown job flags 0x%x", (unsigned)job.flags);
+    SQS_REQUIRE((job.flags & ~0xfff3f) == 0, "unknown job flags 0x%x", (unsigned)job.flags);
     const int pin_cs = (job.flags >> 8) & 0xff, pin_cell = (job.flags >> 16) & 0xf;
     if (pin_cs || pin_cell) {
         SQS_REQUIRE(!(job.flags & SQS_JOB_AUTOTUNE), "SQS_JOB_AUTOTUNE and a pinned shape exclude each other");

@@ -986,9 +986,23 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
         // job's trajectory does not depend on how it is sliced.
         const bool xpoint = (sweep + 1) % jd.exchange_every == 0;
         if (!xpoint && sweep + 1 != jd.sweeps_total) continue;
-        // the replica on the coldest rung is quenched toward zero overlap by
-        // every thread of the CTA that holds it
-        {
+        // the replica on the coldest rung (every replica under
+        // SQS_JOB_QUENCH_ALL) is quenched toward zero overlap by every thread
+        // of the CTA that holds it
+        if (MOVES && (jd.flags & kMoveQuenchAll) && jd.quench_iters > 0) {
+            // every replica of the CTA, one after another, by every thread
+            for (int lr = 0; lr < Rl; ++lr) {
+                if (w == lr && lane == 0) S.qE = E;
+                __syncthreads();
+                const Rep cr = rep_view(dyn + lr * rb, n, jd.Gmax);
+                float4* qs = (int64_t)dyn_bytes >= (int64_t)Rl * rb + 32 * (int64_t)n
+                                 ? reinterpret_cast<float4*>(dyn + (int64_t)Rl * rb)
+                                 : pos + jd.scr_off;
+                const long long qe_out = quench_cta(cr, n, g, L, jd.quench_iters, qs, qs + n, S.qE, S.red);
+                if (w == lr) E = qe_out;
+                __syncthreads();
+            }
+        } else {
             int cold = 0;
             for (int q = 0; q < R; ++q)
                 if (S.jm.perm[q] == 0) cold = q;

@@ -79,6 +79,7 @@ JOB_ADAPT = 2
 JOB_COLLECTIVE = 4
 JOB_KICK = 8
 JOB_SERIAL = 16
+JOB_QUENCH_ALL = 32
 TUNE_LATENCY = 1
 
 

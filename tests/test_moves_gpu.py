@@ -1,6 +1,7 @@
 """The reference's richer move set on the GPU annealer: step adaptation with
-the cooling cycle (SQS_JOB_ADAPT), collective set moves (SQS_JOB_COLLECTIVE)
-and kicks of overlapped replicas (SQS_JOB_KICK).  Each option runs to a
+the cooling cycle (SQS_JOB_ADAPT), collective set moves (SQS_JOB_COLLECTIVE),
+kicks of overlapped replicas (SQS_JOB_KICK) and the quench of every replica
+at exchange rounds (SQS_JOB_QUENCH_ALL).  Each option runs to a
 certified packing, changes the trajectory, and keeps a job's result
 independent of batching, slicing and launch shape."""
 from __future__ import annotations
@@ -13,7 +14,8 @@ pytestmark = pytest.mark.gpu
 
 KEYS = ("L", "L_cert", "L_polished", "proposals", "accepted", "shrinks", "improvements",
         "exchange_attempts", "exchange_accepts", "q")
-OPTIONS = [dict(adapt=True), dict(collective=True), dict(kick=True), dict(adapt=True, collective=True, kick=True)]
+OPTIONS = [dict(adapt=True), dict(collective=True), dict(kick=True), dict(quench_all=True),
+           dict(adapt=True, collective=True, kick=True, quench_all=True)]
 
 
 def _job(n=40, seed=13, sweeps=200, replicas=16, **kw):
