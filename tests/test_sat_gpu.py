@@ -141,3 +141,25 @@ def test_host_call_in_overlapped_chunks_equals_device_call(ctx, oracle):
     assert np.all(np.abs(he.array[:100].astype(np.float64) - eo) <= E_REL * np.abs(eo) + E_ABS)
     for h in (hin, hs, he, hg, hc):
         h.free()
+
+
+def test_reference_selftest_fixture(ctx, oracle):
+    """The reference's device self-test (cuda/tests/selftest.cu:34-53) as a
+    fixture: 100 configurations of 50 squares, centres U(-0.2, 12.2), angles
+    U(-3.14, 3.14), plus axis-aligned pairs that touch exactly, or are 1e-6
+    apart, across a cell boundary of the grid (side 12: 8 cells of 1.5).
+    Energies within the stated tolerance of the FP64 oracle; the touching
+    and separated pairs add no pair energy."""
+    rng = np.random.default_rng(923)
+    xya = np.concatenate([rng.uniform(-0.2, 12.2, (100, 50, 2)), rng.uniform(-3.14, 3.14, (100, 50, 1))], axis=2)
+    out, x32, s32 = _run(ctx, xya, 12.0)
+    _check(oracle, out, x32, s32, grad_quantile=0.99)
+    # boundary pairs, well inside the container (no wall term)
+    pairs = []
+    for gap in (0.0, 1e-6):
+        for b in (3.0, 4.5, 6.0):  # cell boundaries x = 1.5 k
+            pairs.append([[b - 0.5, 6.0, 0.0], [b + 0.5 + gap, 6.0, 0.0]])
+            pairs.append([[6.0, b - 0.5, 0.0], [6.0, b + 0.5 + gap, 0.0]])
+    out, x32, s32 = _run(ctx, np.array(pairs, np.float64), 12.0)
+    _check(oracle, out, x32, s32)
+    assert np.all(out[0] == 0.0), out[0]
