@@ -163,3 +163,16 @@ def test_reference_selftest_fixture(ctx, oracle):
     out, x32, s32 = _run(ctx, np.array(pairs, np.float64), 12.0)
     _check(oracle, out, x32, s32)
     assert np.all(out[0] == 0.0), out[0]
+
+
+def test_reference_near_contact_grid(ctx, oracle):
+    """The reference's large-n check (cuda/tests/globaltest.cu:49): a square
+    grid at pitch 1.000001 -- every neighbour pair 1e-6 from contact once the
+    centres are rounded to FP32 -- in a container that just holds it, through
+    both kernels (n = 1024, one CTA per configuration; n = 256, one warp)."""
+    for k in (32, 16):
+        c = 0.5 + 1.000001 * np.arange(k)
+        gx, gy = np.meshgrid(c, c)
+        xya = np.stack([gx.ravel(), gy.ravel(), np.zeros(k * k)], axis=1)[None]
+        out, x32, s32 = _run(ctx, xya, 1.000001 * k + 1e-6)
+        _check(oracle, out, x32, s32)
