@@ -201,6 +201,12 @@ typedef struct sqs_job {
  * counterpart of the reference search's per-epoch gradient polish of every
  * chain (seeded.cu:621-713).  Costs one quench per replica per round. */
 #define SQS_JOB_QUENCH_ALL 32
+/* Dilation-certify every replica at each checkpoint, not only those whose
+ * overlap energy is below 1e-4: the reference search measures every chain's
+ * certified side after its polish, whatever its overlap (seeded.cu:716-720,
+ * device_certified_side :175-226; a dilation above 1.008 still rejects).
+ * Costs one FP64 side measurement per replica per checkpoint. */
+#define SQS_JOB_CERT_ALL 64
 /* Pin the launch shape instead: a cluster of `cs` CTAs (1..16; it must
  * divide the replica count and fit) and cell side index k (0: 1.59, 1: 1.75,
  * 2: 1.95, 3: 2.2).  Same trajectory as any other shape (see above). */

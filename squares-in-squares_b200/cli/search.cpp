@@ -35,7 +35,11 @@
 //     reference's build_portfolio and structured_init), always for packing
 //     and under SEED_STRUCTURED for seeded;
 //   * the angle proposal width is 2.5 x the move width (PACK_ROTATION is
-//     validated and reported but, as in the reference, not used).
+//     validated and reported but, as in the reference, not used);
+//   * two variables of this build's own, validated like the others (0 or 1):
+//     *_QUENCH_ALL quenches every replica at each exchange round (default 1
+//     for seeded, 0 for packing) and *_CERT_ALL dilation-certifies every
+//     replica at each checkpoint whatever its overlap (default 0).
 // "target_L" is the FP64 dilation-certified side of the best state and "q"
 // that state (the packing the interval certifier accepted); when no ladder
 // finds a certified state the seed is reported with its side, as the
@@ -137,6 +141,16 @@ int main(int argc, char** argv) {
     const int collective = 1;  // packing always mixes collective moves in (packing.cu:525)
     const int structured = 1;  // and always starts from the portfolio (packing.cu:806, 821)
 #endif
+    // options of this build, not the reference's: SQS_JOB_CERT_ALL and
+    // SQS_JOB_QUENCH_ALL on every ladder.  seeded quenches every replica at
+    // each exchange round by default, the counterpart of its per-epoch polish
+    // of every chain (seeded.cu:621-713); packing keeps the coldest-only quench
+    const int cert_all = (int)env("CERT_ALL", 0, 0, 1);
+#if defined(SQS_FLAVOR_SEEDED)
+    const int quench_all = (int)env("QUENCH_ALL", 1, 0, 1);
+#else
+    const int quench_all = (int)env("QUENCH_ALL", 0, 0, 1);
+#endif
     const unsigned long long rng_seed = std::strtoull(argv[5], nullptr, 10);
 
     sqs_ctx* ctx = nullptr;
@@ -175,7 +189,8 @@ int main(int argc, char** argv) {
         j.sweeps = sweeps;
         j.exchange_every = per_epoch;
         j.polish_iters = polish;
-        j.flags = (autotune ? SQS_JOB_AUTOTUNE : 0) | SQS_JOB_ADAPT | SQS_JOB_KICK | (collective ? SQS_JOB_COLLECTIVE : 0);
+        j.flags = (autotune ? SQS_JOB_AUTOTUNE : 0) | SQS_JOB_ADAPT | SQS_JOB_KICK | (collective ? SQS_JOB_COLLECTIVE : 0) |
+                  (cert_all ? SQS_JOB_CERT_ALL : 0) | (quench_all ? SQS_JOB_QUENCH_ALL : 0);
         j.L0 = L;
         j.tmin = tmin;
         j.tmax = tmax;

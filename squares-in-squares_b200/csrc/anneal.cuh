@@ -30,8 +30,14 @@ struct JobDev {
 };
 
 // Move-set options of a job (the same bits as SQS_JOB_ADAPT, _COLLECTIVE, _KICK).
-// kMoveSerial selects the one-at-a-time kernel instance and changes nothing else
-enum : int32_t { kMoveAdapt = 2, kMoveCollective = 4, kMoveKick = 8, kMoveSerial = 16, kMoveQuenchAll = 32 };
+// kMoveSerial selects the one-at-a-time kernel instance and changes nothing else;
+// kCertAll (SQS_JOB_CERT_ALL) only drops the energy gate of the checkpoint's
+// dilation certificate and keeps the kernel instance the other bits select
+enum : int32_t { kMoveAdapt = 2, kMoveCollective = 4, kMoveKick = 8, kMoveSerial = 16, kMoveQuenchAll = 32,
+                 kCertAll = 64 };
+
+// Whether a job's flags select the move-set kernel instance.
+inline bool uses_moves(int32_t flags) { return (flags & ~kCertAll) != 0; }
 
 // Per job, advanced by every slice.
 struct JobMut {

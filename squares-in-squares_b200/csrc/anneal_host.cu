@@ -109,7 +109,7 @@ int prepare_job(const sqs_job& J, int j, JobDev& d, JobMut& m, Plan& p, const Sh
     d.cell = p.cell;
     d.seed = J.seed;
     d.quench_iters = 64;
-    d.flags = J.flags & (kMoveAdapt | kMoveCollective | kMoveKick | kMoveSerial | kMoveQuenchAll);
+    d.flags = J.flags & (kMoveAdapt | kMoveCollective | kMoveKick | kMoveSerial | kMoveQuenchAll | kCertAll);
     std::memset(&m, 0, sizeof m);
     m.L = (float)J.L0;
     m.best_L = 1e30;
@@ -252,8 +252,8 @@ static int trial_ms(sqs_ctx* ctx, const sqs_job& J0, const Plan& p, int copies, 
             SQS_CUDA(cudaMemcpyAsync(D + o_pos + sizeof(float4) * (size_t)pe * c, pos.data(), sizeof(float4) * pos.size(),
                                      cudaMemcpyHostToDevice, ctx->stream));
         SQS_CUDA(cudaEventRecord(ctx->ev[60], ctx->stream));
-        if (int r = launch_anneal(ctx->stream, copies, p.cs, p.Rl, anneal_smem(p.cs, p.Rl, p.rb, J.n, d.flags != 0),
-                                  d.flags != 0, (const int32_t*)(D + o_list),
+        if (int r = launch_anneal(ctx->stream, copies, p.cs, p.Rl, anneal_smem(p.cs, p.Rl, p.rb, J.n, uses_moves(d.flags)),
+                                  uses_moves(d.flags), (const int32_t*)(D + o_list),
                                   (const JobDev*)(D + o_jd), (JobMut*)(D + o_jm), (float4*)(D + o_pos),
                                   (double*)(D + o_best), sweeps))
             return r;
@@ -403,7 +403,7 @@ static int autotune(sqs_ctx* ctx, const sqs_job& job, int mode, sqs_tuning& out)
 int resolve_job(sqs_ctx* ctx, const sqs_job& job, int mode, sqs_job& eff, Shape& shape) {
     eff = job;
     shape = Shape{};
-    SQS_REQUIRE((job.flags & ~0xfff3f) == 0, "unknown job flags 0x%x", (unsigned)job.flags);
+    SQS_REQUIRE((job.flags & ~0xfff7f) == 0, "unknown job flags 0x%x", (unsigned)job.flags);
     const int pin_cs = (job.flags >> 8) & 0xff, pin_cell = (job.flags >> 16) & 0xf;
     if (pin_cs || pin_cell) {
         SQS_REQUIRE(!(job.flags & SQS_JOB_AUTOTUNE), "SQS_JOB_AUTOTUNE and a pinned shape exclude each other");
@@ -588,7 +588,7 @@ extern "C" int sqs_anneal_batch(sqs_ctx* ctx, const sqs_job* jobs, int njobs, in
     // instance); shared memory of the largest
     std::map<std::tuple<int, int, int>, std::vector<int32_t>> groups;
     for (int j = 0; j < njobs; ++j)
-        groups[{plan[(size_t)j].cs, plan[(size_t)j].Rl, (int)(jd[(size_t)j].flags != 0)}].push_back(j);
+        groups[{plan[(size_t)j].cs, plan[(size_t)j].Rl, (int)uses_moves(jd[(size_t)j].flags)}].push_back(j);
     std::vector<int32_t> lists;
     std::vector<std::pair<size_t, size_t>> spans;  // (start, count) in lists
     std::vector<size_t> smems;

@@ -1023,8 +1023,11 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
         if (active) {
             double Lc = 1e30, lam = 0, x0 = 0, y0 = 0;
             // any state whose overlaps a dilation of at most 0.8% removes is a
-            // certified candidate (penetrations of depth d cost about d^2 each)
-            if (E < qe(1e-4f)) Lc = cert_side(rep, n, g, lane, lam, x0, y0);
+            // certified candidate (penetrations of depth d cost about d^2 each,
+            // so the energy gate skips states that cannot pass); under
+            // SQS_JOB_CERT_ALL every replica is measured, as the reference
+            // search measures every chain after its polish (seeded.cu:716)
+            if (E < qe(1e-4f) || (jd.flags & kCertAll)) Lc = cert_side(rep, n, g, lane, lam, x0, y0);
             if (lane == 0) {
                 S.wE[w] = E;
                 S.wL[w] = Lc;

@@ -455,7 +455,7 @@ int launch_idle(sqs_server* s, const std::vector<int32_t>& fin, int& launched) {
     for (int k = 0; k < s->max_active; ++k) {
         if (s->slot_job[(size_t)k] < 0 || s->flying[(size_t)k] || retiring[(size_t)k] || s->retiring[(size_t)k]) continue;
         const SJob& j = s->jobs[s->slot_job[(size_t)k]];
-        const Key key = std::make_tuple(j.plan.cs, j.plan.Rl, (int)(j.jd.flags != 0));
+        const Key key = std::make_tuple(j.plan.cs, j.plan.Rl, (int)uses_moves(j.jd.flags));
         groups[key].push_back(k);
         rb[key] = std::max(rb[key], j.plan.rb);
         nmax[key] = std::max(nmax[key], j.job.n);

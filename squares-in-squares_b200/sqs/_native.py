@@ -80,6 +80,7 @@ JOB_COLLECTIVE = 4
 JOB_KICK = 8
 JOB_SERIAL = 16
 JOB_QUENCH_ALL = 32
+JOB_CERT_ALL = 64
 TUNE_LATENCY = 1
 
 

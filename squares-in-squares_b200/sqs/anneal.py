@@ -41,6 +41,7 @@ class AnnealJob:
     kick: bool = False              # kick and reseed of overlapped replicas at exchange rounds (SQS_JOB_KICK)
     serial: bool = False            # one proposal at a time (SQS_JOB_SERIAL): same trajectory, for checking
     quench_all: bool = False        # quench every replica at exchange rounds (SQS_JOB_QUENCH_ALL)
+    cert_all: bool = False          # dilation-certify every replica at checkpoints (SQS_JOB_CERT_ALL)
     cluster: int = 0                # pinned cluster size (0: default / tuned)
     cell_index: int = 0             # pinned cell side index (0: 1.59, 1: 1.75, 2: 1.95, 3: 2.2)
     xya_rep: np.ndarray | None = None  # (replicas, n, 3) per-replica starts, e.g. from portfolio()
@@ -57,6 +58,7 @@ def _flags(j: AnnealJob) -> int:
     return ((N.JOB_AUTOTUNE if j.autotune else 0) | (N.JOB_ADAPT if j.adapt else 0) |
             (N.JOB_COLLECTIVE if j.collective else 0) | (N.JOB_KICK if j.kick else 0) |
             (N.JOB_SERIAL if j.serial else 0) | (N.JOB_QUENCH_ALL if j.quench_all else 0) |
+            (N.JOB_CERT_ALL if j.cert_all else 0) |
             (j.cluster << 8) | (j.cell_index << 16))
 
 

@@ -1,7 +1,8 @@
 """The reference's richer move set on the GPU annealer: step adaptation with
 the cooling cycle (SQS_JOB_ADAPT), collective set moves (SQS_JOB_COLLECTIVE),
-kicks of overlapped replicas (SQS_JOB_KICK) and the quench of every replica
-at exchange rounds (SQS_JOB_QUENCH_ALL).  Each option runs to a
+kicks of overlapped replicas (SQS_JOB_KICK), the quench of every replica
+at exchange rounds (SQS_JOB_QUENCH_ALL) and the certificate of every replica
+at checkpoints (SQS_JOB_CERT_ALL).  Each option runs to a
 certified packing, changes the trajectory, and keeps a job's result
 independent of batching, slicing and launch shape."""
 from __future__ import annotations
@@ -37,6 +38,32 @@ def test_move_options_are_reproducible(ctx, oracle, opts):
     assert alone["proposals"] == 16 * 200 * 40
     assert alone["launch"]["overflows"] == 0
     assert alone["q"] != plain["q"] or alone["accepted"] != plain["accepted"]  # the option acts
+    if alone["certified"]:
+        ok, L, reason, _ = oracle.certify(40, alone["rows"])
+        assert ok and L == alone["L"], reason
+    mixed = anneal_batch([_job(n=25, seed=2), job, _job(n=60, seed=5, **opts)], ctx=ctx)[1]
+    sliced = anneal_batch([job], ctx=ctx, slice_sweeps=50)[0]
+    wide = anneal_batch([replace(job, cluster=4)], ctx=ctx)[0]
+    for k in KEYS:
+        assert mixed[k] == alone[k], ("mixed", k)
+        assert sliced[k] == alone[k], ("sliced", k)
+        assert wide[k] == alone[k], ("cluster 4", k)
+
+
+@pytest.mark.parametrize("opts", [dict(cert_all=True), dict(cert_all=True, adapt=True, collective=True, kick=True)],
+                         ids=lambda o: "+".join(o))
+def test_cert_all_is_reproducible(ctx, oracle, opts):
+    """SQS_JOB_CERT_ALL measures every replica's dilation-certified side at
+    each checkpoint, whatever its overlap energy: the job still runs to a
+    result the oracle certifies, and that result does not depend on batching,
+    slicing or launch shape."""
+    from sqs.anneal import anneal_batch
+    job = _job(**opts)
+    alone = anneal_batch([job], ctx=ctx)[0]
+    assert alone["status"] == 0, alone["reason"]
+    assert alone["proposals"] == 16 * 200 * 40
+    assert alone["launch"]["overflows"] == 0
+    assert alone["improvements"] >= 1
     if alone["certified"]:
         ok, L, reason, _ = oracle.certify(40, alone["rows"])
         assert ok and L == alone["L"], reason
