@@ -207,6 +207,12 @@ typedef struct sqs_job {
  * device_certified_side :175-226; a dilation above 1.008 still rejects).
  * Costs one FP64 side measurement per replica per checkpoint. */
 #define SQS_JOB_CERT_ALL 64
+/* Checkpoint quench budget, k = 1..127: up to 16 k gradient iterations per
+ * quench, ending only at zero overlap or when no trial step improves, as the
+ * reference's per-epoch polish runs its iterations uninterrupted
+ * (seeded.cu:621-713).  k = 0: 64 iterations, also ending after three
+ * accepted steps in a row that each gained less than 0.1%. */
+#define SQS_JOB_QUENCH_STEPS(k) ((int32_t)(k) << 24)
 /* Pin the launch shape instead: a cluster of `cs` CTAs (1..16; it must
  * divide the replica count and fit) and cell side index k (0: 1.59, 1: 1.75,
  * 2: 1.95, 3: 2.2).  Same trajectory as any other shape (see above). */

@@ -36,10 +36,13 @@
 //     and under SEED_STRUCTURED for seeded;
 //   * the angle proposal width is 2.5 x the move width (PACK_ROTATION is
 //     validated and reported but, as in the reference, not used);
-//   * two variables of this build's own, validated like the others (0 or 1):
-//     *_QUENCH_ALL quenches every replica at each exchange round (default 1
-//     for seeded, 0 for packing) and *_CERT_ALL dilation-certifies every
-//     replica at each checkpoint whatever its overlap (default 0).
+//   * three variables of this build's own, validated like the others:
+//     *_QUENCH_ALL (0 or 1) quenches every replica at each exchange round,
+//     *_CERT_ALL (0 or 1) dilation-certifies every replica at each
+//     checkpoint whatever its overlap, and *_QUENCH_STEPS (-1..2032) sets the
+//     quench iterations per checkpoint with no exit on slow progress (0 keeps
+//     the library's, -1 takes the polish iterations of the epochs one
+//     checkpoint spans); seeded defaults to 1, 1, -1 and packing to 0, 0, 0.
 // "target_L" is the FP64 dilation-certified side of the best state and "q"
 // that state (the packing the interval certifier accepted); when no ladder
 // finds a certified state the seed is reported with its side, as the
@@ -141,15 +144,21 @@ int main(int argc, char** argv) {
     const int collective = 1;  // packing always mixes collective moves in (packing.cu:525)
     const int structured = 1;  // and always starts from the portfolio (packing.cu:806, 821)
 #endif
-    // options of this build, not the reference's: SQS_JOB_CERT_ALL and
-    // SQS_JOB_QUENCH_ALL on every ladder.  seeded quenches every replica at
-    // each exchange round by default, the counterpart of its per-epoch polish
-    // of every chain (seeded.cu:621-713); packing keeps the coldest-only quench
-    const int cert_all = (int)env("CERT_ALL", 0, 0, 1);
+    // options of this build, not the reference's: SQS_JOB_CERT_ALL,
+    // SQS_JOB_QUENCH_ALL and SQS_JOB_QUENCH_STEPS on every ladder.  seeded
+    // turns all three on by default, the counterparts of its per-epoch
+    // uninterrupted polish of every chain and certificate of every chain
+    // (seeded.cu:621-720); packing keeps the library's defaults.  Quench
+    // iterations per checkpoint: 0 = the library's default, -1 = the polish
+    // iterations of the epochs one checkpoint spans.
 #if defined(SQS_FLAVOR_SEEDED)
+    const int cert_all = (int)env("CERT_ALL", 1, 0, 1);
     const int quench_all = (int)env("QUENCH_ALL", 1, 0, 1);
+    const int quench_steps = (int)env("QUENCH_STEPS", -1, -1, 2032);
 #else
+    const int cert_all = (int)env("CERT_ALL", 0, 0, 1);
     const int quench_all = (int)env("QUENCH_ALL", 0, 0, 1);
+    const int quench_steps = (int)env("QUENCH_STEPS", 0, -1, 2032);
 #endif
     const unsigned long long rng_seed = std::strtoull(argv[5], nullptr, 10);
 
@@ -172,6 +181,13 @@ int main(int argc, char** argv) {
     const int sweeps = (int)std::max<long long>(1, (proposals_per_chain + n - 1) / n);
     const int per_epoch = std::max(1, (int)std::lround((double)steps / (double)n));
     const int ladders = chains / 8;
+    int quench_k = 0;  // SQS_JOB_QUENCH_STEPS(k): 16 k iterations
+    if (quench_steps > 0) {
+        quench_k = (quench_steps + 15) / 16;
+    } else if (quench_steps < 0 && polish > 0) {
+        const double iters = (double)polish * per_epoch * n / steps;
+        quench_k = (int)std::min(127.0, std::ceil(iters / 16.0));
+    }
 
     // every chain's start: the structured portfolio (the seed on every chain
     // when SEED_STRUCTURED=0); ladder k's 8 chains are job k's replicas
@@ -190,7 +206,8 @@ int main(int argc, char** argv) {
         j.exchange_every = per_epoch;
         j.polish_iters = polish;
         j.flags = (autotune ? SQS_JOB_AUTOTUNE : 0) | SQS_JOB_ADAPT | SQS_JOB_KICK | (collective ? SQS_JOB_COLLECTIVE : 0) |
-                  (cert_all ? SQS_JOB_CERT_ALL : 0) | (quench_all ? SQS_JOB_QUENCH_ALL : 0);
+                  (cert_all ? SQS_JOB_CERT_ALL : 0) | (quench_all ? SQS_JOB_QUENCH_ALL : 0) |
+                  SQS_JOB_QUENCH_STEPS(quench_k);
         j.L0 = L;
         j.tmin = tmin;
         j.tmax = tmax;

@@ -26,7 +26,8 @@ struct JobDev {
     int64_t best_off;                 // double index of the best state (n x 3)
     int64_t scr_off;                  // float4 index of the job's quench scratch (2n)
     int32_t quench_iters, flags;      // gradient steps of the coldest replica per checkpoint; kMove* bits
-    int32_t slice, pad3;              // sweeps per launch for this job (0: the launch's slice)
+    int32_t slice;                    // sweeps per launch for this job (0: the launch's slice)
+    int32_t quench_stall;             // accepted slow steps (< 0.1% gained each) that end a quench
 };
 
 // Move-set options of a job (the same bits as SQS_JOB_ADAPT, _COLLECTIVE, _KICK).

@@ -108,7 +108,11 @@ int prepare_job(const sqs_job& J, int j, JobDev& d, JobMut& m, Plan& p, const Sh
     d.L0 = (float)J.L0;
     d.cell = p.cell;
     d.seed = J.seed;
-    d.quench_iters = 64;
+    // the checkpoint quench: 64 iterations ending after three slow steps, or
+    // under SQS_JOB_QUENCH_STEPS(k) 16 k iterations with no slow-step exit
+    const int qk = (J.flags >> 24) & 0x7f;
+    d.quench_iters = qk ? 16 * qk : 64;
+    d.quench_stall = qk ? 0x7fffffff : 3;
     d.flags = J.flags & (kMoveAdapt | kMoveCollective | kMoveKick | kMoveSerial | kMoveQuenchAll | kCertAll);
     std::memset(&m, 0, sizeof m);
     m.L = (float)J.L0;
@@ -403,7 +407,7 @@ static int autotune(sqs_ctx* ctx, const sqs_job& job, int mode, sqs_tuning& out)
 int resolve_job(sqs_ctx* ctx, const sqs_job& job, int mode, sqs_job& eff, Shape& shape) {
     eff = job;
     shape = Shape{};
-    SQS_REQUIRE((job.flags & ~0xfff7f) == 0, "unknown job flags 0x%x", (unsigned)job.flags);
+    SQS_REQUIRE((job.flags & ~0x7f0fff7f) == 0, "unknown job flags 0x%x", (unsigned)job.flags);
     const int pin_cs = (job.flags >> 8) & 0xff, pin_cell = (job.flags >> 16) & 0xf;
     if (pin_cs || pin_cell) {
         SQS_REQUIRE(!(job.flags & SQS_JOB_AUTOTUNE), "SQS_JOB_AUTOTUNE and a pinned shape exclude each other");

@@ -342,11 +342,11 @@ __device__ __forceinline__ int qg(float v) { return __float2int_rn(v * kQScale);
 // neighbouring cell) work item for the gradient and the energies:
 // Jacobi gradient descent on the overlap energy with a backtracking step
 // (up to 6 trials per iteration), at most `iters` iterations, ending early at
-// zero energy, when no trial improves, or after three accepted steps in a
-// row that each gained less than 0.1%.  Gradients and energies are integer
+// zero energy, when no trial improves, or after `stall_limit` accepted steps
+// in a row that each gained less than 0.1%.  Gradients and energies are integer
 // sums, so the result does not depend on the CTA's width.
-__device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters, float4* grad, float4* saved,
-                                long long E, long long* red) {
+__device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters, int stall_limit, float4* grad,
+                                float4* saved, long long E, long long* red) {
     float alpha = 0.05f;
     int stall = 0;  // consecutive accepted steps that gained less than 0.1%
     int4* acc = reinterpret_cast<int4*>(grad);  // the gradient buffer holds the integer sums first
@@ -439,7 +439,7 @@ __device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters
                 alpha *= 0.3f;
             }
         }
-        if (!moved || stall >= 3) {
+        if (!moved || stall >= stall_limit) {
             if (!moved) {  // no improvement: restore the saved state (its lists are current)
                 for (int i = threadIdx.x; i < n; i += blockDim.x) {
                     const float4 o = saved[i];
@@ -998,7 +998,7 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                 float4* qs = (int64_t)dyn_bytes >= (int64_t)Rl * rb + 32 * (int64_t)n
                                  ? reinterpret_cast<float4*>(dyn + (int64_t)Rl * rb)
                                  : pos + jd.scr_off;
-                const long long qe_out = quench_cta(cr, n, g, L, jd.quench_iters, qs, qs + n, S.qE, S.red);
+                const long long qe_out = quench_cta(cr, n, g, L, jd.quench_iters, jd.quench_stall, qs, qs + n, S.qE, S.red);
                 if (w == lr) E = qe_out;
                 __syncthreads();
             }
@@ -1015,7 +1015,7 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                 float4* qs = (int64_t)dyn_bytes >= (int64_t)Rl * rb + 32 * (int64_t)n
                                  ? reinterpret_cast<float4*>(dyn + (int64_t)Rl * rb)
                                  : pos + jd.scr_off;
-                const long long qe_out = quench_cta(cr, n, g, L, jd.quench_iters, qs, qs + n, S.qE, S.red);
+                const long long qe_out = quench_cta(cr, n, g, L, jd.quench_iters, jd.quench_stall, qs, qs + n, S.qE, S.red);
                 if (w == cold % Rl) E = qe_out;
                 __syncthreads();
             }

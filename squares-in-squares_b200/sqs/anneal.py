@@ -42,6 +42,7 @@ class AnnealJob:
     serial: bool = False            # one proposal at a time (SQS_JOB_SERIAL): same trajectory, for checking
     quench_all: bool = False        # quench every replica at exchange rounds (SQS_JOB_QUENCH_ALL)
     cert_all: bool = False          # dilation-certify every replica at checkpoints (SQS_JOB_CERT_ALL)
+    quench_steps: int = 0           # 1..127: 16 k-iteration quenches without a slow-step exit (SQS_JOB_QUENCH_STEPS)
     cluster: int = 0                # pinned cluster size (0: default / tuned)
     cell_index: int = 0             # pinned cell side index (0: 1.59, 1: 1.75, 2: 1.95, 3: 2.2)
     xya_rep: np.ndarray | None = None  # (replicas, n, 3) per-replica starts, e.g. from portfolio()
@@ -50,6 +51,8 @@ class AnnealJob:
     def __post_init__(self):
         self.xya = np.ascontiguousarray(self.xya, dtype=np.float64).reshape(-1, 3)
         self.n = self.xya.shape[0]
+        if not 0 <= self.quench_steps <= 127:
+            raise ValueError("quench_steps must be in 0..127")
         if self.xya_rep is not None:
             self.xya_rep = np.ascontiguousarray(self.xya_rep, dtype=np.float64).reshape(self.replicas, self.n, 3)
 
@@ -58,7 +61,7 @@ def _flags(j: AnnealJob) -> int:
     return ((N.JOB_AUTOTUNE if j.autotune else 0) | (N.JOB_ADAPT if j.adapt else 0) |
             (N.JOB_COLLECTIVE if j.collective else 0) | (N.JOB_KICK if j.kick else 0) |
             (N.JOB_SERIAL if j.serial else 0) | (N.JOB_QUENCH_ALL if j.quench_all else 0) |
-            (N.JOB_CERT_ALL if j.cert_all else 0) |
+            (N.JOB_CERT_ALL if j.cert_all else 0) | (j.quench_steps << 24) |
             (j.cluster << 8) | (j.cell_index << 16))
 
 

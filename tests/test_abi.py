@@ -39,3 +39,24 @@ def test_version_and_error_reporting_without_gpu():
             N.Context(0)
         assert e.value.code == -1
         assert "not present" in str(e.value)
+
+
+def test_job_flag_constants_match_the_header():
+    from sqs import _native as N
+    text = (ROOT / "include" / "sqs.h").read_text()
+    defs = dict(re.findall(r"#define SQS_(JOB_[A-Z_]+) (\d+)\b", text))
+    assert {"JOB_AUTOTUNE", "JOB_SERIAL", "JOB_QUENCH_ALL", "JOB_CERT_ALL"} <= set(defs)
+    for name, value in defs.items():
+        assert getattr(N, name) == int(value), name
+    # the packed fields sit above the single-bit options and below the sign bit
+    assert "#define SQS_JOB_QUENCH_STEPS(k) ((int32_t)(k) << 24)" in text
+
+
+def test_anneal_job_checks_the_quench_budget():
+    import numpy as np
+
+    from sqs.anneal import AnnealJob, _flags
+    xya = np.zeros((4, 3))
+    assert _flags(AnnealJob(xya, L0=2.0, quench_steps=127, cert_all=True)) == (127 << 24) | 64
+    with pytest.raises(ValueError):
+        AnnealJob(xya, L0=2.0, quench_steps=128)

@@ -62,7 +62,7 @@ def test_search_argument_checks(built, tmp_path, prog):
     ("packing", "PACK_TMAX", "2"), ("packing", "PACK_MOVE", "0.5"), ("packing", "PACK_SHRINK", "x"),
     ("packing", "PACK_MAX_CHAINS", "4"), ("seeded", "SEED_TMAX", "0.2"), ("seeded", "SEED_POLISH", "5000"),
     ("seeded", "SEED_COLLECTIVE", "2"), ("seeded", "SEED_MOVE", "0.02x"), ("seeded", "SEED_QUENCH_ALL", "2"),
-    ("packing", "PACK_CERT_ALL", "-1")])
+    ("packing", "PACK_CERT_ALL", "-1"), ("seeded", "SEED_QUENCH_STEPS", "-2"), ("packing", "PACK_QUENCH_STEPS", "3000")])
 def test_search_environment_checks(built, tmp_path, prog, var, value):
     seed = _seed(tmp_path, "2 2\n0.5 0.5 0\n1.5 0.5 0\n")
     r = _run([built / prog, seed, 1, 1, 8, 1, tmp_path / "o.json"], env={var: value})

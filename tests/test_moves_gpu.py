@@ -50,20 +50,23 @@ def test_move_options_are_reproducible(ctx, oracle, opts):
         assert wide[k] == alone[k], ("cluster 4", k)
 
 
-@pytest.mark.parametrize("opts", [dict(cert_all=True), dict(cert_all=True, adapt=True, collective=True, kick=True)],
-                         ids=lambda o: "+".join(o))
-def test_cert_all_is_reproducible(ctx, oracle, opts):
+@pytest.mark.parametrize("opts", [dict(cert_all=True), dict(cert_all=True, adapt=True, collective=True, kick=True),
+                                  dict(quench_steps=8), dict(quench_all=True, quench_steps=4, kick=True)],
+                         ids=lambda o: "+".join(f"{k}={v}" for k, v in o.items()))
+def test_checkpoint_options_are_reproducible(ctx, oracle, opts):
     """SQS_JOB_CERT_ALL measures every replica's dilation-certified side at
-    each checkpoint, whatever its overlap energy: the job still runs to a
-    result the oracle certifies, and that result does not depend on batching,
-    slicing or launch shape."""
+    each checkpoint, whatever its overlap energy; SQS_JOB_QUENCH_STEPS(k)
+    gives the checkpoint quench 16 k iterations with no slow-progress exit.
+    Either way the job runs to a result the oracle certifies, and that result
+    does not depend on batching, slicing or launch shape."""
     from sqs.anneal import anneal_batch
     job = _job(**opts)
     alone = anneal_batch([job], ctx=ctx)[0]
     assert alone["status"] == 0, alone["reason"]
     assert alone["proposals"] == 16 * 200 * 40
     assert alone["launch"]["overflows"] == 0
-    assert alone["improvements"] >= 1
+    if opts.get("cert_all"):
+        assert alone["improvements"] >= 1
     if alone["certified"]:
         ok, L, reason, _ = oracle.certify(40, alone["rows"])
         assert ok and L == alone["L"], reason
