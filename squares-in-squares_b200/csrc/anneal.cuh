@@ -25,7 +25,7 @@ struct JobDev {
     int64_t pos_off;                  // float4 index of replica 0, square 0
     int64_t best_off;                 // double index of the best state (n x 3)
     int64_t scr_off;                  // float4 index of the job's quench scratch (2n)
-    int32_t quench_iters, flags;      // gradient steps of the coldest replica per checkpoint; kMove* bits
+    int32_t quench_iters, flags;      // gradient steps of a checkpoint quench (at most); kMove* bits
     int32_t slice;                    // sweeps per launch for this job (0: the launch's slice)
     int32_t quench_stall;             // accepted slow steps (< 0.1% gained each) that end a quench
 };

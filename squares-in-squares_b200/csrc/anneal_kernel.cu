@@ -338,13 +338,14 @@ __device__ long long full_energy_cta(const Rep& R, int n, const Grid& g, float L
 constexpr float kQScale = 1048576.0f;
 __device__ __forceinline__ int qg(float v) { return __float2int_rn(v * kQScale); }
 
-// The quench of the coldest replica by the whole CTA, one thread per (square,
-// neighbouring cell) work item for the gradient and the energies:
-// Jacobi gradient descent on the overlap energy with a backtracking step
-// (up to 6 trials per iteration), at most `iters` iterations, ending early at
-// zero energy, when no trial improves, or after `stall_limit` accepted steps
-// in a row that each gained less than 0.1%.  Gradients and energies are integer
-// sums, so the result does not depend on the CTA's width.
+// The checkpoint quench of one replica (the coldest, or each one under
+// SQS_JOB_QUENCH_ALL) by the whole CTA, one thread per (square, neighbouring
+// cell) work item for the gradient and the energies: Jacobi gradient descent
+// on the overlap energy with a backtracking step (up to 6 trials per
+// iteration), at most `iters` iterations, ending early at zero energy, when
+// no trial improves, or after `stall_limit` accepted steps in a row that each
+// gained less than 0.1%.  Gradients and energies are integer sums, so the
+// result does not depend on the CTA's width.
 __device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters, int stall_limit, float4* grad,
                                 float4* saved, long long E, long long* red) {
     float alpha = 0.05f;
