@@ -568,23 +568,27 @@ def bench_batched(ctx, sweeps: int = 50, instances: int = 512):
                 squares=int(sum(j.n for j in jobs)) * 32, certified=sum(r["certified"] for r in res))
 
 
-def bench_search(cases: str = "10:200:64:64,50:60:64:64,200:10:48:64,50:600:64:64,200:100:48:64"):
+def bench_search(cases: str = "10:200:64:64,50:60:64:64,200:10:48:64,50:600:64:64,200:100:48:64",
+                 prog: str = "seeded"):
     """The search programs head to head on the same B200: this library's
-    `seeded` drop-in and the reference's own `seeded` (built for sm_100a from
-    its sources into oracle/_ref), same seed file (grid centres + U(+-0.05)
-    jitter, angles U[0, 0.1), seed 42, side ceil(sqrt n)), epochs, steps,
-    chains and environment (SEED_AUTOTUNE=0 so both keep the chain count).
-    Reports each program's own seconds, wall time, proposals and the side the
-    official gate certifies for its raw result (demo.certified_candidate)."""
+    `seeded` (or `packing`) drop-in and the reference's own program of that
+    name (built for sm_100a from its sources into oracle/_ref), same seed file
+    (grid centres + U(+-0.05) jitter, angles U[0, 0.1), seed 42, side
+    ceil(sqrt n)), epochs, steps, chains and environment (*_AUTOTUNE=0 so both
+    keep the chain count).  Reports each program's own seconds, wall time,
+    proposals and the side the official gate certifies for its raw result
+    (demo.certified_candidate)."""
     import subprocess
     import tempfile
 
     from sqs.anneal import jittered_grid
     from sqs.demo import certified_candidate
 
-    progs = {"sqs": ROOT / "squares-in-squares_b200" / "bin" / "seeded",
-             "reference": ROOT / "oracle" / "_ref" / "seeded"}
-    env = dict(os.environ, SEED_AUTOTUNE="0")
+    if prog not in ("seeded", "packing"):
+        raise ValueError(f"unknown search program {prog!r}")
+    progs = {"sqs": ROOT / "squares-in-squares_b200" / "bin" / prog,
+             "reference": ROOT / "oracle" / "_ref" / prog}
+    env = dict(os.environ, **{"SEED_AUTOTUNE" if prog == "seeded" else "PACK_AUTOTUNE": "0"})
     out = {}
     with tempfile.TemporaryDirectory() as tmp:
         for case in cases.split(","):
@@ -619,7 +623,7 @@ def bench_search(cases: str = "10:200:64:64,50:60:64:64,200:10:48:64,50:600:64:6
                                  target_L=raw["target_L"], certified_L=side, dilation=dil, chains=raw["chains"])
             if "seconds" in row.get("sqs", {}) and "seconds" in row.get("reference", {}):
                 row["wall_speedup"] = row["reference"]["wall_seconds"] / row["sqs"]["wall_seconds"]
-            out[f"n={n} epochs={epochs} steps={steps} chains={chains}"] = row
+            out[f"{prog} n={n} epochs={epochs} steps={steps} chains={chains}"] = row
     return out
 
 
@@ -663,6 +667,8 @@ def main():
     ap.add_argument("--served-jobs", type=int, default=960, help="most jobs in one served stream")
     ap.add_argument("--served-sweeps", type=int, default=200, help="sweep budget of every served job")
     ap.add_argument("--served-slice", type=int, default=4000, help="proposals per replica per server slice")
+    ap.add_argument("--search-prog", choices=("seeded", "packing"), default="seeded",
+                    help="which search program the search section compares")
     args = ap.parse_args()
     if args.section:
         from sqs import Context
@@ -674,7 +680,7 @@ def main():
                       plain_pt=lambda: bench_plain_pt(ctx),
                       batched=lambda: bench_batched(ctx, args.batched_sweeps, args.batched_instances),
                       batched_fixed=lambda: bench_batched_fixed(ctx, args.batched_sweeps, args.batched_instances),
-                      search=lambda: bench_search())[args.section]
+                      search=lambda: bench_search(prog=args.search_prog))[args.section]
             print(json.dumps({args.section: fn()}), flush=True)
         return
     if args.warmup < 3:
