@@ -42,7 +42,7 @@
 //     checkpoint whatever its overlap, and *_QUENCH_STEPS (-1..2032) sets the
 //     quench iterations per checkpoint with no exit on slow progress (0 keeps
 //     the library's, -1 takes the polish iterations of the epochs one
-//     checkpoint spans); seeded defaults to 1, 1, -1 and packing to 0, 0, 0.
+//     checkpoint spans); both default to 1, 1, -1.
 // "target_L" is the FP64 dilation-certified side of the best state and "q"
 // that state (the packing the interval certifier accepted); when no ladder
 // finds a certified state the seed is reported with its side, as the
@@ -145,21 +145,14 @@ int main(int argc, char** argv) {
     const int structured = 1;  // and always starts from the portfolio (packing.cu:806, 821)
 #endif
     // options of this build, not the reference's: SQS_JOB_CERT_ALL,
-    // SQS_JOB_QUENCH_ALL and SQS_JOB_QUENCH_STEPS on every ladder.  seeded
-    // turns all three on by default, the counterparts of its per-epoch
-    // uninterrupted polish of every chain and certificate of every chain
-    // (seeded.cu:621-720); packing keeps the library's defaults.  Quench
-    // iterations per checkpoint: 0 = the library's default, -1 = the polish
-    // iterations of the epochs one checkpoint spans.
-#if defined(SQS_FLAVOR_SEEDED)
+    // SQS_JOB_QUENCH_ALL and SQS_JOB_QUENCH_STEPS on every ladder, all three
+    // on by default: the counterparts of the per-epoch uninterrupted polish
+    // and certificate of every chain (seeded.cu:621-720, packing.cu:630-689).
+    // Quench iterations per checkpoint: 0 = the library's
+    // default, -1 = the polish iterations of the epochs one checkpoint spans.
     const int cert_all = (int)env("CERT_ALL", 1, 0, 1);
     const int quench_all = (int)env("QUENCH_ALL", 1, 0, 1);
     const int quench_steps = (int)env("QUENCH_STEPS", -1, -1, 2032);
-#else
-    const int cert_all = (int)env("CERT_ALL", 0, 0, 1);
-    const int quench_all = (int)env("QUENCH_ALL", 0, 0, 1);
-    const int quench_steps = (int)env("QUENCH_STEPS", 0, -1, 2032);
-#endif
     const unsigned long long rng_seed = std::strtoull(argv[5], nullptr, 10);
 
     sqs_ctx* ctx = nullptr;
