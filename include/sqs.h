@@ -213,7 +213,7 @@ typedef struct sqs_job {
  * (seeded.cu:621-713).  k = 0: 64 iterations, also ending after three
  * accepted steps in a row that each gained less than 0.1%. */
 #define SQS_JOB_QUENCH_STEPS(k) ((int32_t)(k) << 24)
-/* Pin the launch shape instead: a cluster of `cs` CTAs (1..16; it must
+/* Pin the launch shape instead of SQS_JOB_AUTOTUNE: a cluster of `cs` CTAs (1..16; it must
  * divide the replica count and fit) and cell side index k (0: 1.59, 1: 1.75,
  * 2: 1.95, 3: 2.2).  Same trajectory as any other shape (see above). */
 #define SQS_JOB_CLUSTER(cs) ((int32_t)(cs) << 8)
