@@ -63,6 +63,12 @@ int sqs_event_elapsed(sqs_ctx* ctx, int a, int b, float* ms);
 /* Overwrite a 256 MiB device buffer (twice the 126 MB L2) so the next
  * launch reads its inputs from HBM. */
 int sqs_flush_l2(sqs_ctx* ctx);
+/* Device memory now free and in total (cudaMemGetInfo), and the bytes the
+ * context's own staging buffers hold on the device and in pinned host memory
+ * (they only grow, and are released by sqs_ctx_destroy).  Any pointer may be
+ * NULL. */
+int sqs_ctx_memory(sqs_ctx* ctx, size_t* device_free, size_t* device_total, size_t* staging_device,
+                   size_t* staging_host);
 /* Kernel launches this context issued since creation (all of libsqs's own
  * kernels; library copies/memsets are not counted). */
 int64_t sqs_launch_count(sqs_ctx* ctx);
@@ -116,20 +122,27 @@ int sqs_certify_batch(sqs_ctx* ctx, int count, const int32_t* n_of, const int64_
                       sqs_verdict* out);
 
 /* Allocation-free form of sqs_certify_batch, for callers that cannot
- * allocate GPU memory while they run: a host that owns all device memory
- * through its own pool, or a latency-critical loop that forbids allocation
- * after start-up.  No counterpart in the reference, which always certifies
- * on the CPU.  Same arguments, results and errors as sqs_certify_batch, but
- * it calls no cudaMalloc, cudaFree or other allocating routine: all device
- * scratch is one static array of about 7.6 MiB that every device holds from
- * library load until process exit, and host staging is static too.  Limits
- * per call: 4,096 packings, 16,384 squares, 2 MiB of literal text (and, with
- * SQS_CERT_ROUNDTRIP, literals under 4,096 bytes); larger calls fail with
- * SQS_EINVAL.  The first call on a device looks up the array's device
- * address and uploads constants, so make that first call before any stream
- * capture.  The scratch keeps the last call's contents (what must start at
- * zero is cleared on entry); calls that overlap -- from several threads, or
- * on several contexts of one device -- race on it and must not be issued. */
+ * allocate GPU memory while they run: a host that hands all device memory to
+ * its own pool at start-up, or a latency-critical loop that forbids
+ * allocation once it runs.  No counterpart in the reference, which always
+ * certifies on the CPU.  Same arguments, results and errors as
+ * sqs_certify_batch, but it calls no cudaMalloc, cudaFree or other allocating
+ * routine: all device scratch is one static array of about 7.6 MiB that
+ * every device loading the library holds until process exit, and host
+ * staging is static too.  Limits per call: 4,096 packings, 16,384 squares,
+ * 2 MiB of literal text (and, with SQS_CERT_ROUNDTRIP, literals under 4,096
+ * bytes); larger calls fail with SQS_EINVAL.
+ * Set-up: the first call on a device looks up the array's device address
+ * (which, under CUDA's lazy module loading, is when the driver loads the
+ * module holding it), uploads constants and launches each kernel of the path
+ * once with nothing to do (loading it and letting the driver size the local
+ * memory its stack needs).  A call with count = 0 does only this set-up.
+ * Make that first call at start-up, before a pool takes the device's memory
+ * and before any stream capture; afterwards calls allocate nothing.
+ * The scratch keeps the last call's contents (what must start at zero is
+ * cleared on entry).  Every call in the process shares it -- calls from
+ * several threads, contexts or devices -- so calls must not overlap; one
+ * that would overlap another call still running fails with SQS_EBUSY. */
 int sqs_certify_batch_static(sqs_ctx* ctx, int count, const int32_t* n_of, const int64_t* row_start,
                              const int32_t* square_id, const char* text, const int64_t* lit_off, int flags,
                              sqs_verdict* out);

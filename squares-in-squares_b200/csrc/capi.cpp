@@ -219,6 +219,25 @@ int sqs_flush_l2(sqs_ctx* ctx) {
     return SQS_OK;
 }
 
+int sqs_ctx_memory(sqs_ctx* ctx, size_t* device_free, size_t* device_total, size_t* staging_device,
+                   size_t* staging_host) {
+    if (int r = sqs::enter(ctx)) return r;
+    size_t fr = 0, tot = 0;
+    SQS_CUDA(cudaMemGetInfo(&fr, &tot));
+    if (device_free) *device_free = fr;
+    if (device_total) *device_total = tot;
+    if (staging_device) {
+        const sqs::DevBuf* bufs[] = {&ctx->d_in,    &ctx->d_side,  &ctx->d_out,  &ctx->d_grad,
+                                     &ctx->d_cand,  &ctx->d_misc,  &ctx->d_anneal, &ctx->d_cert,
+                                     &ctx->d_tune,  &ctx->d_polish};
+        size_t b = ctx->flush_bytes;
+        for (const sqs::DevBuf* d : bufs) b += d->bytes;
+        *staging_device = b;
+    }
+    if (staging_host) *staging_host = ctx->h_cert.bytes + ctx->h_text.bytes;
+    return SQS_OK;
+}
+
 int64_t sqs_launch_count(sqs_ctx* ctx) { return ctx ? ctx->launches : -1; }
 int64_t sqs_graph_replay_count(sqs_ctx* ctx) { return ctx ? ctx->graph_replays : -1; }
 

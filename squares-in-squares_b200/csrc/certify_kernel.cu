@@ -753,11 +753,13 @@ static int upload_consts(int device) {
     return SQS_OK;
 }
 
-static std::string fifty(const Fix<9>& v) {
+// The side rounded half-to-even at 50 decimals (format_50_decimals,
+// certifier.cpp:60-104), written into dst (cap >= 80 holds every side here).
+static void fifty_into(const Fix<9>& v, char* dst, size_t cap) {
     const uint64_t B = 1000000000ULL;
     uint64_t low = v.d[6] % 10000ULL, top = v.d[6] / 10000ULL;
-    bool tail = v.d[7] || v.d[8] || v.d[9];
-    bool up = low > 5000ULL || (low == 5000ULL && (tail || (top & 1ULL)));
+    const bool tail = v.d[7] || v.d[8] || v.d[9];
+    const bool up = low > 5000ULL || (low == 5000ULL && (tail || (top & 1ULL)));
     uint64_t o[7] = {v.d[0], v.d[1], v.d[2], v.d[3], v.d[4], v.d[5], top};
     if (up && ++o[6] >= 100000ULL) {
         o[6] -= 100000ULL;
@@ -770,27 +772,41 @@ static std::string fifty(const Fix<9>& v) {
     }
     bool allz = true;
     for (uint64_t w : o) allz &= w == 0;
-    char buf[128];
-    std::snprintf(buf, sizeof buf, "%s%llu.%09llu%09llu%09llu%09llu%09llu%05llu", (v.neg && !allz) ? "-" : "",
+    std::snprintf(dst, cap, "%s%llu.%09llu%09llu%09llu%09llu%09llu%05llu", (v.neg && !allz) ? "-" : "",
                   (unsigned long long)o[0], (unsigned long long)o[1], (unsigned long long)o[2],
                   (unsigned long long)o[3], (unsigned long long)o[4], (unsigned long long)o[5],
                   (unsigned long long)o[6]);
+}
+
+static std::string fifty(const Fix<9>& v) {
+    char buf[128];
+    fifty_into(v, buf, sizeof buf);
     return buf;
 }
 
 static double grid_score(int n) { return std::ceil(std::sqrt((double)n)) / std::sqrt((double)n) - 1.0; }
 
+// The pandas float round trip of one value (roundtrip_float_str,
+// certifier.cpp:914-929): the shortest of %.15g, %.16g, %.17g that reads back
+// as v, with ".0" appended to a plain integer; returns its length (< 40).
+static size_t roundtrip_into(double v, char out[40]) {
+    for (int p = 15; p <= 17; ++p) {
+        std::snprintf(out, 40, "%.*g", p, v);
+        if (std::strtod(out, nullptr) == v) break;
+    }
+    size_t len = std::strlen(out);
+    if (std::strpbrk(out, ".eE") == nullptr) {
+        std::memcpy(out + len, ".0", 3);
+        len += 2;
+    }
+    return len;
+}
+
 static std::string roundtrip(const char* s, size_t len) {
     std::string in(s, len);
-    double v = std::strtod(in.c_str(), nullptr);
-    char buf[64];
-    for (int p = 15; p <= 17; ++p) {
-        std::snprintf(buf, sizeof buf, "%.*g", p, v);
-        if (std::strtod(buf, nullptr) == v) break;
-    }
-    std::string r(buf);
-    if (r.find_first_of(".eE") == std::string::npos) r += ".0";
-    return r;
+    char buf[40];
+    const size_t k = roundtrip_into(std::strtod(in.c_str(), nullptr), buf);
+    return std::string(buf, k);
 }
 
 static void put(char* dst, size_t cap, const std::string& s) {
@@ -1161,6 +1177,12 @@ constexpr size_t kStaticScratchBytes = kSoCnt + 256;  // about 7.6 MiB
 // cudaGetSymbolAddress, taken once per device.
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 static void* s_scratch_addr[64] = {nullptr};
+static std::atomic<bool> s_ready[64];
+static std::mutex s_setup_mu;
+// Set while a call runs: the scratch and the host staging below are shared
+// by every call in the process, so a call that would overlap another is
+// refused instead of racing with it.
+static std::atomic_flag s_busy = ATOMIC_FLAG_INIT;
 
 // Host staging (static, not heap): literal slices in square-id order, packing
 // tables, round-tripped literals, the per-packing records read back.
@@ -1175,28 +1197,56 @@ static char s_rt_text[kStaticMaxText];
 static char s_lit_tmp[4096];
 static PkOut s_out[kStaticMaxPackings];
 
-static void fifty_into(const Fix<9>& v, char* dst, size_t cap) {
-    const uint64_t B = 1000000000ULL;
-    uint64_t low = v.d[6] % 10000ULL, top = v.d[6] / 10000ULL;
-    const bool tail = v.d[7] || v.d[8] || v.d[9];
-    const bool up = low > 5000ULL || (low == 5000ULL && (tail || (top & 1ULL)));
-    uint64_t o[7] = {v.d[0], v.d[1], v.d[2], v.d[3], v.d[4], v.d[5], top};
-    if (up && ++o[6] >= 100000ULL) {
-        o[6] -= 100000ULL;
-        int i = 5;
-        for (; i >= 1; --i) {
-            if (++o[i] < B) break;
-            o[i] -= B;
-        }
-        if (i < 1) o[0] += 1;
-    }
-    bool allz = true;
-    for (uint64_t w : o) allz &= w == 0;
-    std::snprintf(dst, cap, "%s%llu.%09llu%09llu%09llu%09llu%09llu%05llu", (v.neg && !allz) ? "-" : "",
-                  (unsigned long long)o[0], (unsigned long long)o[1], (unsigned long long)o[2],
-                  (unsigned long long)o[3], (unsigned long long)o[4], (unsigned long long)o[5],
-                  (unsigned long long)o[6]);
+// Per-device set-up of the allocation-free path, once, with that device
+// current: the device address of the static array (cudaGetSymbolAddress;
+// under lazy module loading this is also what loads the module holding the
+// array), the certifier's constants, and one launch of each stage kernel
+// with nothing to do, which loads the kernels and lets the driver size the
+// local memory their stacks need.  Everything a later call uses is then in
+// place, so later calls allocate nothing.
+template <int T, int NMAX>
+static int packing_attr() {
+    const size_t smem = (size_t)NMAX * (sizeof(FSq) + 5 * sizeof(double) + sizeof(int16_t));
+    SQS_CUDA(cudaFuncSetAttribute(cert_packing_kernel<T, NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    return SQS_OK;
 }
+
+static int static_setup(sqs_ctx* ctx) {
+    const int dev = ctx->device & 63;
+    if (s_ready[dev]) return SQS_OK;
+    std::lock_guard<std::mutex> lk(s_setup_mu);
+    if (s_ready[dev]) return SQS_OK;
+    void* p = nullptr;
+    SQS_CUDA(cudaGetSymbolAddress(&p, g_static_scratch));
+    if (int r = upload_consts(ctx->device)) return r;
+    if (int r = packing_attr<64, 64>()) return r;
+    if (int r = packing_attr<128, 256>()) return r;
+    if (int r = packing_attr<256, 1024>()) return r;
+    char* D = (char*)p;
+    Pair* pa = (Pair*)(D + kSoPa);
+    uint32_t* cnt = (uint32_t*)(D + kSoCnt);
+    SQS_CUDA(cudaMemsetAsync(cnt, 0, 64, ctx->stream));
+    const int64_t* d_s0 = (const int64_t*)(D + kSoS0);
+    const Lit* d_lits = (const Lit*)(D + kSoLits);
+    PkOut* d_out = (PkOut*)(D + kSoOut);
+    if (int r = launch_stage<7>(ctx, pa, cnt, 0, nullptr, nullptr, 0, d_s0, d_lits, D, d_out, 1)) return r;
+    if (int r = launch_stage<15>(ctx, pa, cnt, 0, nullptr, nullptr, 0, d_s0, d_lits, D, d_out, 1)) return r;
+    if (int r = launch_stage<58>(ctx, pa, cnt, 0, nullptr, nullptr, 0, d_s0, d_lits, D, d_out, 1)) return r;
+    SQS_CUDA(cudaStreamSynchronize(ctx->stream));
+    s_scratch_addr[dev] = p;
+    s_ready[dev] = true;
+    return SQS_OK;
+}
+
+namespace {
+struct BusyGuard {
+    bool held;
+    BusyGuard() : held(!s_busy.test_and_set(std::memory_order_acquire)) {}
+    ~BusyGuard() {
+        if (held) s_busy.clear(std::memory_order_release);
+    }
+};
+}  // namespace
 
 }  // namespace cert
 }  // namespace sqs
@@ -1205,17 +1255,19 @@ extern "C" int sqs_certify_batch_static(sqs_ctx* ctx, int count, const int32_t* 
                                         const int32_t* square_id, const char* text, const int64_t* lit_off,
                                         int flags, sqs_verdict* out) {
     if (int r = enter(ctx)) return r;
+    BusyGuard busy;
+    if (!busy.held) {
+        set_error("sqs_certify_batch_static: another call is in progress (all calls share one static scratch "
+                  "array and must not overlap)");
+        return SQS_EBUSY;
+    }
     SQS_REQUIRE(count >= 0 && count <= kStaticMaxPackings, "count %d out of 0..%d (static certifier limit)", count,
                 kStaticMaxPackings);
+    // the first call on a device (count == 0 does only this) sets the path up
+    if (int r = static_setup(ctx)) return r;
     if (count == 0) return SQS_OK;
     SQS_REQUIRE(n_of && row_start && text && lit_off && out, "null host pointer");
     const int dev = ctx->device & 63;
-    if (!s_scratch_addr[dev]) {  // once per device, with that device current (sqs::enter)
-        void* p = nullptr;
-        SQS_CUDA(cudaGetSymbolAddress(&p, g_static_scratch));
-        s_scratch_addr[dev] = p;
-    }
-    if (int r = upload_consts(ctx->device)) return r;
     const bool do_rt = (flags & SQS_CERT_ROUNDTRIP) != 0;
     // envelope checks and literal slices, as sqs_certify_batch does them
     int64_t S = 0;
@@ -1261,20 +1313,10 @@ extern "C" int sqs_certify_batch_static(sqs_ctx* ctx, int count, const int32_t* 
                                 sizeof(s_lit_tmp) - 1);
                     std::memcpy(s_lit_tmp, text + a, (size_t)(b - a));
                     s_lit_tmp[b - a] = 0;
-                    const double val = std::strtod(s_lit_tmp, nullptr);
                     char buf[40];
-                    for (int prec = 15; prec <= 17; ++prec) {
-                        std::snprintf(buf, sizeof buf, "%.*g", prec, val);
-                        if (std::strtod(buf, nullptr) == val) break;
-                    }
-                    size_t len = std::strlen(buf);
-                    const bool plain = std::strpbrk(buf, ".eE") == nullptr;
-                    SQS_REQUIRE(rt_used + len + 2 <= kStaticMaxText, "literals exceed %zu bytes", kStaticMaxText);
+                    const size_t len = roundtrip_into(std::strtod(s_lit_tmp, nullptr), buf);
+                    SQS_REQUIRE(rt_used + len <= kStaticMaxText, "literals exceed %zu bytes", kStaticMaxText);
                     std::memcpy(s_rt_text + rt_used, buf, len);
-                    if (plain) {
-                        std::memcpy(s_rt_text + rt_used + len, ".0", 2);
-                        len += 2;
-                    }
                     s_raw_off[q] = (int64_t)rt_used;
                     s_raw_len[q] = (int32_t)len;
                     rt_used += len;

@@ -103,6 +103,8 @@ SIGNATURES: dict[str, tuple] = {
     "sqs_event_record": (C.c_int, [_vp, C.c_int]),
     "sqs_event_elapsed": (C.c_int, [_vp, C.c_int, C.c_int, _fp]),
     "sqs_flush_l2": (C.c_int, [_vp]),
+    "sqs_ctx_memory": (C.c_int, [_vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
+                                 C.POINTER(C.c_size_t)]),
     "sqs_launch_count": (C.c_int64, [_vp]),
     "sqs_graph_replay_count": (C.c_int64, [_vp]),
     "sqs_sat_energy": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_int]),
@@ -251,6 +253,14 @@ class Context:
 
     def launches(self) -> int:
         return int(lib().sqs_launch_count(self.handle))
+
+    def memory(self) -> dict:
+        """Device memory free / total and the bytes the context's own staging
+        buffers hold on the device and in pinned host memory."""
+        v = [C.c_size_t(0) for _ in range(4)]
+        check(lib().sqs_ctx_memory(self.handle, *[C.byref(x) for x in v]))
+        return dict(device_free=v[0].value, device_total=v[1].value, staging_device=v[2].value,
+                    staging_host=v[3].value)
 
     def graph_replays(self) -> int:
         return int(lib().sqs_graph_replay_count(self.handle))

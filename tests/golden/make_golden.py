@@ -1,9 +1,9 @@
 """Generate the golden fixtures under tests/golden/ from the reference itself.
 
-Run in a checkout that has the reference sources (default /root/reference, or
-$SQS_REFERENCE) and the compiled reference in oracle/_ref:
+Run with $SQS_REFERENCE naming a checkout of the reference sources (there is
+no default) and the compiled reference in oracle/_ref:
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref REF=$SQS_REFERENCE && python tests/golden/make_golden.py
 
 Outputs (committed):
   certify_cases.json  packings with the verdict, reason and 50-decimal side
@@ -32,7 +32,9 @@ from pathlib import Path
 
 import numpy as np
 
-REF = Path(os.environ.get("SQS_REFERENCE", "/root/reference"))
+if not os.environ.get("SQS_REFERENCE"):
+    sys.exit("make_golden.py: set SQS_REFERENCE to a checkout of the reference sources")
+REF = Path(os.environ["SQS_REFERENCE"])
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
 sys.path.insert(0, str(REF / "src"))

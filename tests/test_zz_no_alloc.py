@@ -7,6 +7,11 @@ whose scratch is one static device array.  Its verdicts must equal the
 regular entry point's exactly, call after call, because the shared scratch
 keeps the previous call's contents.
 
+The first call on a device (a call with count = 0 does only this) sets the
+path up: it loads the module and kernels and lets the driver size their
+local memory.  After it, calls must leave the device's free memory and the
+context's staging buffers exactly as they were.
+
 This file is collected last on purpose: it must pass on its own in a fresh
 process and after every other test.
 """
@@ -50,6 +55,49 @@ def test_static_certifier_matches_regular_entry_point_on_two_calls(ctx):
     assert sum(v[0] for v in a1) > 0 and sum(not v[0] for v in a1) > 0
     # and once more in the other order, so a call following a larger one is covered
     assert _call("sqs_certify_batch_static", ctx, first) == b1
+
+
+def _deep_cases():
+    # two squares whose separation is decided only past 63 digits (the 15-
+    # and 58-limb stages of the per-pair kernel), both signs
+    from test_certify_gpu import _deep_pair
+    items = []
+    for theta in ("0.5", "1.1", "0.25", "1.5"):
+        for k in (70, 80, 90, 120):
+            for sign in (1, -1):
+                items.append((2, _deep_pair(theta, k, sign)))
+    return items
+
+
+def test_static_certifier_deep_stages_match_regular_entry_point(ctx):
+    deep = _deep_cases()
+    a = _call("sqs_certify_batch_static", ctx, deep)
+    b = _call("sqs_certify_batch", ctx, deep)
+    assert a == b
+    reasons = {v[4] for v in a}
+    assert "ok" in reasons and "infeasible: Squares overlap (certified)" in reasons
+    assert _call("sqs_certify_batch_static", ctx, deep) == b
+
+
+def test_static_certifier_allocates_nothing_after_set_up():
+    import json as _json
+
+    from sqs import Context
+    from sqs.workloads import certify_corpus
+    cases = _json.loads((GOLDEN / "certify_cases.json").read_text())
+    batches = [[(c["n"], c["rows"]) for c in cases], _deep_cases(), certify_corpus(60, seed=31, n_hi=300)]
+    with Context(0) as c:
+        # set-up call: count = 0
+        assert _call("sqs_certify_batch_static", c, []) == []
+        m0 = c.memory()
+        assert m0["staging_device"] == 0 and m0["staging_host"] == 0
+        for _ in range(2):
+            for items in batches:
+                _call("sqs_certify_batch_static", c, items)
+            _call("sqs_certify_batch_static", c, batches[2], roundtrip=True)
+        m1 = c.memory()
+        assert m1["device_free"] == m0["device_free"], (m0, m1)
+        assert m1["staging_device"] == 0 and m1["staging_host"] == 0, m1
 
 
 def test_static_certifier_rejects_oversized_calls(ctx):
