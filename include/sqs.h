@@ -265,6 +265,49 @@ typedef struct sqs_job_result {
 int sqs_anneal_batch(sqs_ctx* ctx, const sqs_job* jobs, int njobs, int slice_sweeps, double* const* xya_out,
                      sqs_job_result* out);
 
+/* Each replica's final state, for checking the annealer against an FP64
+ * recomputation.  Caller buffers sized by the job's replicas R and n; any of
+ * them may be NULL. */
+typedef struct sqs_replica_trace {
+    float* xya;              /* R * n * 3: each replica's final (x, y, angle), FP32 as annealed */
+    double* energy;          /* R: the annealer's running energy of each replica (walls + pairs:
+                                its exact fixed-point sum, in energy units)                        */
+    double* energy_full;     /* R: the same recomputed from scratch on the final state            */
+    double* L_cert;          /* R: FP64 dilation-certified side of the final state, by the device
+                                function the checkpoints use (1e9: dilation above 1.008)          */
+    double* dilation;        /* R: that dilation                                                   */
+    float* side;             /* R: the container side each energy is measured in                  */
+    float* temperature;      /* R: temperature of each replica's next proposal (rung x cooling)  */
+    float* step_scale;       /* R: step scale of its next proposal, in units of sigma (1 without
+                                SQS_JOB_ADAPT)                                                     */
+    int32_t* rung;           /* R: temperature index of each replica                               */
+    int32_t exchange_rounds; /* out: exchange rounds the job completed                             */
+    int32_t cells_ok;        /* out: every final state fitted its cell list                        */
+} sqs_replica_trace;
+
+/* sqs_anneal_batch, then each job's replicas read back into trace[j] (one
+ * record per job): their final states, running energies and the checks
+ * above, measured after the timed region (result.device_ms excludes it).
+ * The reference's counterpart is its device self-tests, which compare the
+ * search's running FP32 energy with a host FP64 sum (cuda/tests/
+ * globaltest.cu:21-49). */
+int sqs_anneal_batch_trace(sqs_ctx* ctx, const sqs_job* jobs, int njobs, int slice_sweeps, double* const* xya_out,
+                           sqs_job_result* out, sqs_replica_trace* trace);
+
+/* FP64 energy (walls + sum over pairs of the squared SAT penetration) and
+ * its gradient of `count` packings, one CTA each, all pairs: the FP64
+ * recompute of a candidate state.  Packing k has n_of[k] rows (1..1000) of
+ * (x, y, angle) in xya, back to back, and container side side[k]; energy[k]
+ * and, when grad is not NULL, grad (the layout of xya) = d energy /
+ * d (x, y, angle).  The pair term is the reference's pair_cached
+ * (seeded.cu:41-65), the gradient its polish's pair_cached_smooth
+ * (seeded.cu:67-90) with the smooth wall derivative (seeded.cu:96-113),
+ * summed per square as seeded.cu:637-650 does; cos and sin are taken of the
+ * angles as given.  Replaces the reference's FP64 total_cached
+ * (seeded.cu:148-162) and its polish gradient. */
+int sqs_energy_fp64(sqs_ctx* ctx, int count, const int32_t* n_of, const double* xya, const double* side,
+                    double* energy, double* grad);
+
 /* Initial states of `chains` search chains (out: chains * n rows of x, y,
  * angle), the reference's structured portfolio (build_portfolio,
  * seeded.cu:233-425): by chain b's group b % 8 within its ladder b / 8, the

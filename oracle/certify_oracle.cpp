@@ -762,9 +762,28 @@ void sqo_roundtrip(const char* s, char* out, int cap) {
 
 // Batch form of sqo_certify, threaded over packings (the layout of
 // ref_evaluate_batch in ref_certifier.cpp).
+// The same with each packing's 50-decimal side and reason written to
+// L_out + 80 p and reason_out + 112 p (either may be NULL).
+extern "C" int sqo_certify_batch_text(int count, const int* n_of, const long long* row_start, const int* sid,
+                                      const char* text, const long long* lit_off, int threads, int* ok_out,
+                                      double* score_out, char* L_out, char* reason_out);
+
 extern "C" int sqo_certify_batch(int count, const int* n_of, const long long* row_start, const int* sid,
                                  const char* text, const long long* lit_off, int threads, int* ok_out,
                                  double* score_out) {
+    return sqo_certify_batch_text(count, n_of, row_start, sid, text, lit_off, threads, ok_out, score_out, nullptr,
+                                  nullptr);
+}
+
+static void put_text(char* dst, size_t cap, const std::string& s) {
+    const size_t k = std::min(cap - 1, s.size());
+    std::memcpy(dst, s.data(), k);
+    dst[k] = 0;
+}
+
+extern "C" int sqo_certify_batch_text(int count, const int* n_of, const long long* row_start, const int* sid,
+                                      const char* text, const long long* lit_off, int threads, int* ok_out,
+                                      double* score_out, char* L_out, char* reason_out) {
     std::atomic<int> next{0};
     auto work = [&]() {
         for (int p = next.fetch_add(1); p < count; p = next.fetch_add(1)) {
@@ -786,6 +805,8 @@ extern "C" int sqo_certify_batch(int count, const int* n_of, const long long* ro
             orc::Verdict v = orc::evaluate(n_of[p], (int)rows, ids.data(), px.data(), py.data(), pa.data());
             ok_out[p] = v.ok ? 1 : 0;
             if (score_out) score_out[p] = v.score;
+            if (L_out) put_text(L_out + 80 * (size_t)p, 80, v.ok ? v.L : std::string());
+            if (reason_out) put_text(reason_out + 112 * (size_t)p, 112, v.reason);
         }
     };
     std::vector<std::thread> pool;

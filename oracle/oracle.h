@@ -13,6 +13,7 @@ double sqo_pair_cached(const double p[3], const double q[3], double c, double s,
 double sqo_pair(const double p[3], const double q[3], double* grad);
 double sqo_boundary(const double p[3], double L, double* g);
 double sqo_total(int n, double L, const double* xya, double* grad, int64_t* cand);
+double sqo_total_smooth(int n, double L, const double* xya, double* grad);
 int sqo_total_batch(int configs, int n, const double* xya, const double* L,
                     double* energy, double* grad, int64_t* cand, int threads);
 /* ptsa_oracle.c: dilation-certified side of a state and the CPU PT-SA */

@@ -45,6 +45,8 @@ def lib():
         L.sqo_boundary.argtypes = [_dp, C.c_double, _dp]
         L.sqo_total.restype = C.c_double
         L.sqo_total.argtypes = [C.c_int, C.c_double, _dp, _dp, _i64p]
+        L.sqo_total_smooth.restype = C.c_double
+        L.sqo_total_smooth.argtypes = [C.c_int, C.c_double, _dp, _dp]
         L.sqo_total_batch.restype = C.c_int
         L.sqo_total_batch.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp, _i64p, C.c_int]
         L.sqo_certified_side.restype = C.c_double
@@ -56,6 +58,9 @@ def lib():
         L.sqo_roundtrip.argtypes = [C.c_char_p, C.c_char_p, C.c_int]
         L.sqo_ptsa_batch.restype = C.c_int
         L.sqo_ptsa_batch.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int]
+        L.sqo_certify_batch_text.restype = C.c_int
+        L.sqo_certify_batch_text.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_void_p,
+                                             C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.sqo_certify_batch.restype = C.c_int
         L.sqo_certify_batch.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_void_p,
                                         C.c_int, C.c_void_p, C.c_void_p]
@@ -94,6 +99,9 @@ def ref_certifier():
                                    C.c_char_p, C.c_int, _dp]
         L.ref_roundtrip.restype = None
         L.ref_roundtrip.argtypes = [C.c_char_p, C.c_char_p, C.c_int]
+        L.ref_evaluate_batch_text.restype = C.c_int
+        L.ref_evaluate_batch_text.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_void_p,
+                                              C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ref_evaluate_batch.restype = C.c_int
         L.ref_evaluate_batch.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_void_p,
                                          C.c_int, C.c_void_p, C.c_void_p]
@@ -124,6 +132,24 @@ def total_batch(xya, L, grad=True, threads=None):
     lib().sqo_total_batch(configs, n, _ptr(xya, _dp), _ptr(L, _dp), _ptr(e, _dp), _ptr(g, _dp),
                           _ptr(cand, _i64p), threads)
     return e, g, cand
+
+
+def total_smooth(xya, L):
+    """FP64 energy and smooth-variant gradient (the polish's) of one state."""
+    xya = np.ascontiguousarray(xya, dtype=np.float64)
+    g = np.zeros_like(xya)
+    e = lib().sqo_total_smooth(xya.shape[0], float(L), _ptr(xya, _dp), _ptr(g, _dp))
+    return e, g
+
+
+def pair_cached(p, q, smooth=False):
+    """sqo_pair_cached with cos/sin of the given angles: (energy, d/dp)."""
+    p = np.ascontiguousarray(p, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    g = np.zeros(3)
+    e = lib().sqo_pair_cached(_ptr(p, _dp), _ptr(q, _dp), np.cos(p[2]), np.sin(p[2]), np.cos(q[2]),
+                              np.sin(q[2]), _ptr(g, _dp), 1 if smooth else 0)
+    return e, g
 
 
 def ref_total_batch(xya, L, grad=True, threads=None):
@@ -234,3 +260,25 @@ def certify_batch(n_of, row_start, sid, text, lit_off, which="oracle", threads=N
     used = fn(count, n_of.ctypes.data, row_start.ctypes.data, sid.ctypes.data, text, lit_off.ctypes.data,
               threads, ok.ctypes.data, score.ctypes.data)
     return ok, score, used
+
+
+def certify_batch_text(n_of, row_start, sid, text, lit_off, which="oracle", threads=None):
+    """Threaded batch certification with the 50-decimal sides and reasons,
+    by the oracle restatement (which="oracle") or the compiled reference
+    ("ref"): (ok int32[count], score float64[count], L strings, reasons)."""
+    n_of = np.ascontiguousarray(n_of, np.int32)
+    row_start = np.ascontiguousarray(row_start, np.int64)
+    sid = np.ascontiguousarray(sid, np.int32)
+    lit_off = np.ascontiguousarray(lit_off, np.int64)
+    count = len(n_of)
+    ok = np.zeros(count, np.int32)
+    score = np.zeros(count)
+    Lb = C.create_string_buffer(80 * max(1, count))
+    rb = C.create_string_buffer(112 * max(1, count))
+    fn = lib().sqo_certify_batch_text if which == "oracle" else ref_certifier().ref_evaluate_batch_text
+    fn(count, n_of.ctypes.data, row_start.ctypes.data, sid.ctypes.data, text, lit_off.ctypes.data,
+       threads or os.cpu_count() or 1, ok.ctypes.data, score.ctypes.data, C.addressof(Lb), C.addressof(rb))
+    raw_L, raw_r = Lb.raw, rb.raw
+    Ls = [raw_L[80 * p:80 * (p + 1)].split(b"\0", 1)[0].decode() for p in range(count)]
+    rs = [raw_r[112 * p:112 * (p + 1)].split(b"\0", 1)[0].decode() for p in range(count)]
+    return ok, score, Ls, rs

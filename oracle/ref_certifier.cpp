@@ -43,9 +43,22 @@ extern "C" void ref_roundtrip(const char* s, char* out, int cap) {
 // an atomic counter, as certifier.cpp's main does (:1011-1032).  Packing p
 // has rows row_start[p] .. row_start[p+1]-1; row r's literals are
 // text[lit_off[3r+k] .. lit_off[3r+k+1]).  ok_out[p] = 1 when accepted.
+// The same with each packing's 50-decimal side and reason written to
+// L_out + 80 p and reason_out + 112 p (either may be NULL).
+extern "C" int ref_evaluate_batch_text(int count, const int* n_of, const long long* row_start, const int* sid,
+                                       const char* text, const long long* lit_off, int threads, int* ok_out,
+                                       double* score_out, char* L_out, char* reason_out);
+
 extern "C" int ref_evaluate_batch(int count, const int* n_of, const long long* row_start, const int* sid,
                                   const char* text, const long long* lit_off, int threads, int* ok_out,
                                   double* score_out) {
+    return ref_evaluate_batch_text(count, n_of, row_start, sid, text, lit_off, threads, ok_out, score_out, nullptr,
+                                   nullptr);
+}
+
+extern "C" int ref_evaluate_batch_text(int count, const int* n_of, const long long* row_start, const int* sid,
+                                       const char* text, const long long* lit_off, int threads, int* ok_out,
+                                       double* score_out, char* L_out, char* reason_out) {
     std::atomic<int> next{0};
     auto work = [&]() {
         for (int p = next.fetch_add(1); p < count; p = next.fetch_add(1)) {
@@ -61,6 +74,8 @@ extern "C" int ref_evaluate_batch(int count, const int* n_of, const long long* r
             cert::PuzzleResult res = cert::evaluate_single_puzzle(n_of[p], rd);
             ok_out[p] = res.ok ? 1 : 0;
             if (score_out) score_out[p] = res.score;
+            if (L_out) put(L_out + 80 * (size_t)p, 80, res.ok ? res.L : std::string());
+            if (reason_out) put(reason_out + 112 * (size_t)p, 112, res.reason);
         }
     };
     std::vector<std::thread> pool;

@@ -95,7 +95,19 @@ double sqo_boundary(const double p[3], double L, double* g) {
 /* Total energy of one configuration (walls + sum_{i<j} pair) and, when grad
  * is given (n*3 doubles, overwritten), its gradient.  *cand (nullable)
  * receives the number of pairs with centre distance^2 < 2. */
+static double total_ex(int n, double L, const double* xya, double* grad, int64_t* cand, int smooth);
+
 double sqo_total(int n, double L, const double* xya, double* grad, int64_t* cand) {
+    return total_ex(n, L, xya, grad, cand, 0);
+}
+
+/* The same with the polish's smooth pair gradient (pair_cached_smooth,
+ * seeded.cu:67-90) when smooth != 0; the energy is unchanged. */
+double sqo_total_smooth(int n, double L, const double* xya, double* grad) {
+    return total_ex(n, L, xya, grad, NULL, 1);
+}
+
+static double total_ex(int n, double L, const double* xya, double* grad, int64_t* cand, int smooth) {
     double e = 0.0;
     int64_t pairs = 0;
     if (grad) memset(grad, 0, sizeof(double) * 3 * (size_t)n);
@@ -110,9 +122,9 @@ double sqo_total(int n, double L, const double* xya, double* grad, int64_t* cand
             if (j > i && dx * dx + dy * dy < 2.0) pairs++;
             if (j > i) {
                 e += sqo_pair_cached(p, q, c, s, cos(q[2]), sin(q[2]),
-                                     grad ? grad + 3 * i : NULL, 0);
+                                     grad ? grad + 3 * i : NULL, smooth);
             } else if (grad) {
-                sqo_pair_cached(p, q, c, s, cos(q[2]), sin(q[2]), grad + 3 * i, 0);
+                sqo_pair_cached(p, q, c, s, cos(q[2]), sin(q[2]), grad + 3 * i, smooth);
             }
         }
     }

@@ -56,6 +56,18 @@ struct JobMut {
     int32_t win[kMaxR];               // accepted proposals in its current window of 16
 };
 
+// One replica's final state as sqs_anneal_batch_trace reports it.
+struct TraceRec {
+    long long E_full;   // fixed-point energy recomputed from scratch (kEScale units)
+    double L_cert;      // FP64 dilation-certified side (1e9: dilation above 1.008)
+    double lam;         // that dilation
+    float temp;         // temperature of its next proposal (rung temperature x cooling)
+    float step;         // its step scale (SQS_JOB_ADAPT; else 1)
+    float side;         // container side its energy is measured in
+    int32_t rung;       // temperature index
+    int32_t cells_ok;   // its cell list fitted
+    int32_t pad;
+};
 // Energies are accumulated as integers in units of 2^-40: every pair and
 // wall term is rounded once, so sums are exact and independent of the order
 // in which neighbours are visited (cell lists are rebuilt with atomics), and

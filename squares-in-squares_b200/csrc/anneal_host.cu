@@ -541,8 +541,10 @@ int certify_states(sqs_ctx* ctx, const std::vector<int>& ns, const std::vector<c
 }  // namespace ann
 }  // namespace sqs
 
-extern "C" int sqs_anneal_batch(sqs_ctx* ctx, const sqs_job* jobs, int njobs, int slice_sweeps,
-                                double* const* xya_out, sqs_job_result* out) {
+// sqs_anneal_batch, and with `trace` (one record per job, or NULL) each
+// replica's final state read back after the anneal (sqs_anneal_batch_trace).
+static int anneal_run(sqs_ctx* ctx, const sqs_job* jobs, int njobs, int slice_sweeps, double* const* xya_out,
+                      sqs_job_result* out, sqs_replica_trace* trace) {
     if (int r = enter(ctx)) return r;
     SQS_REQUIRE(njobs >= 0 && (njobs == 0 || (jobs && out)), "bad job array");
     SQS_REQUIRE(slice_sweeps >= 0, "slice_sweeps %d < 0", slice_sweeps);
@@ -570,6 +572,15 @@ extern "C" int sqs_anneal_batch(sqs_ctx* ctx, const sqs_job* jobs, int njobs, in
     const size_t o_jd = seg(sizeof(JobDev) * njobs), o_jm = seg(sizeof(JobMut) * njobs);
     const size_t o_pos = seg(sizeof(float4) * (size_t)pos_total), o_best = seg(sizeof(double) * (size_t)best_total);
     const size_t o_list = seg(sizeof(int32_t) * njobs);
+    // trace: one (job, replica) item and one record per replica
+    int64_t ntrace = 0;
+    size_t trace_smem = 0;
+    if (trace)
+        for (int j = 0; j < njobs; ++j) {
+            ntrace += jobs[j].replicas;
+            trace_smem = std::max(trace_smem, (size_t)plan[(size_t)j].rb);
+        }
+    const size_t o_titem = seg(sizeof(int2) * (size_t)ntrace), o_trec = seg(sizeof(TraceRec) * (size_t)ntrace);
     if (int r = ctx->d_anneal.reserve(tot)) return r;
     char* D = (char*)ctx->d_anneal.p;
     JobDev* d_jd = (JobDev*)(D + o_jd);
@@ -664,6 +675,24 @@ extern "C" int sqs_anneal_batch(sqs_ctx* ctx, const sqs_job* jobs, int njobs, in
     if (int r = launch_polish(ctx->stream, njobs, d_list, d_jd, d_jm, d_best, psmem)) return r;
     ctx->launches += 1;
     SQS_CUDA(cudaEventRecord(e1, ctx->stream));
+    std::vector<TraceRec> trec((size_t)ntrace);
+    std::vector<float4> tpos;
+    if (ntrace > 0) {
+        std::vector<int2> items;
+        for (int j = 0; j < njobs; ++j)
+            for (int r = 0; r < jobs[j].replicas; ++r) items.push_back(make_int2(j, r));
+        SQS_CUDA(cudaMemcpyAsync(D + o_titem, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+        if (int r = launch_trace(ctx->stream, (int)ntrace, (const int2*)(D + o_titem), d_jd, d_jm, d_pos,
+                                 (TraceRec*)(D + o_trec), trace_smem))
+            return r;
+        ctx->launches += 1;
+        SQS_CUDA(cudaMemcpyAsync(trec.data(), D + o_trec, sizeof(TraceRec) * trec.size(), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+        tpos.resize((size_t)pos_total);
+        SQS_CUDA(cudaMemcpyAsync(tpos.data(), d_pos, sizeof(float4) * tpos.size(), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    }
     std::vector<double> hbest((size_t)best_total);
     SQS_CUDA(cudaMemcpyAsync(jm.data(), d_jm, sizeof(JobMut) * njobs, cudaMemcpyDeviceToHost, ctx->stream));
     SQS_CUDA(cudaMemcpyAsync(hbest.data(), d_best, sizeof(double) * hbest.size(), cudaMemcpyDeviceToHost,
@@ -671,6 +700,36 @@ extern "C" int sqs_anneal_batch(sqs_ctx* ctx, const sqs_job* jobs, int njobs, in
     SQS_CUDA(cudaStreamSynchronize(ctx->stream));
     float dev_ms = 0.f;
     SQS_CUDA(cudaEventElapsedTime(&dev_ms, e0, e1));
+    if (ntrace > 0) {
+        size_t k = 0;
+        for (int j = 0; j < njobs; ++j) {
+            sqs_replica_trace& t = trace[j];
+            const JobMut& m = jm[(size_t)j];
+            const int n = jobs[j].n;
+            t.exchange_rounds = m.xround;
+            t.cells_ok = 1;
+            for (int r = 0; r < jobs[j].replicas; ++r, ++k) {
+                const TraceRec& q = trec[k];
+                t.cells_ok &= q.cells_ok;
+                if (t.energy) t.energy[r] = (double)m.E[r] * (1.0 / (double)kEScale);
+                if (t.energy_full) t.energy_full[r] = (double)q.E_full * (1.0 / (double)kEScale);
+                if (t.L_cert) t.L_cert[r] = q.L_cert;
+                if (t.dilation) t.dilation[r] = q.lam;
+                if (t.side) t.side[r] = q.side;
+                if (t.temperature) t.temperature[r] = q.temp;
+                if (t.step_scale) t.step_scale[r] = q.step;
+                if (t.rung) t.rung[r] = q.rung;
+                if (t.xya) {
+                    const float4* src = tpos.data() + jd[(size_t)j].pos_off + (int64_t)r * n;
+                    for (int i = 0; i < n; ++i) {
+                        t.xya[3 * ((size_t)r * n + i)] = src[i].x;
+                        t.xya[3 * ((size_t)r * n + i) + 1] = src[i].y;
+                        t.xya[3 * ((size_t)r * n + i) + 2] = src[i].z;
+                    }
+                }
+            }
+        }
+    }
 
     // jobs that never certified a state: rescue from the coldest replica
     {
@@ -695,6 +754,17 @@ extern "C" int sqs_anneal_batch(sqs_ctx* ctx, const sqs_job* jobs, int njobs, in
     }
     if (int r = certify_states(ctx, ns, bptr, optr, xptr)) return r;
     return SQS_OK;
+}
+
+extern "C" int sqs_anneal_batch(sqs_ctx* ctx, const sqs_job* jobs, int njobs, int slice_sweeps,
+                                double* const* xya_out, sqs_job_result* out) {
+    return anneal_run(ctx, jobs, njobs, slice_sweeps, xya_out, out, nullptr);
+}
+
+extern "C" int sqs_anneal_batch_trace(sqs_ctx* ctx, const sqs_job* jobs, int njobs, int slice_sweeps,
+                                      double* const* xya_out, sqs_job_result* out, sqs_replica_trace* trace) {
+    SQS_REQUIRE(trace != nullptr || njobs == 0, "null trace array");
+    return anneal_run(ctx, jobs, njobs, slice_sweeps, xya_out, out, trace);
 }
 
 extern "C" int sqs_autotune(sqs_ctx* ctx, const sqs_job* job, int mode, sqs_tuning* out) {
@@ -743,5 +813,44 @@ extern "C" int sqs_polish_batch(sqs_ctx* ctx, int count, const int32_t* n_of, co
         out[k].iterations = (int32_t)res[3 * (size_t)k + 2];
         out[k].improved = out[k].L_out < out[k].L_in;
     }
+    return SQS_OK;
+}
+
+extern "C" int sqs_energy_fp64(sqs_ctx* ctx, int count, const int32_t* n_of, const double* xya, const double* side,
+                               double* energy, double* grad) {
+    if (int r = enter(ctx)) return r;
+    SQS_REQUIRE(count >= 0, "count %d < 0", count);
+    if (count == 0) return SQS_OK;
+    SQS_REQUIRE(n_of && xya && side && energy, "null host pointer");
+    std::vector<int64_t> row0((size_t)count + 1, 0);
+    int nmax = 1;
+    for (int k = 0; k < count; ++k) {
+        SQS_REQUIRE(n_of[k] >= 1 && n_of[k] <= kMaxN, "packing %d: n=%d out of 1..%d", k, n_of[k], kMaxN);
+        SQS_REQUIRE(std::isfinite(side[k]) && side[k] > 0, "packing %d: side must be finite and positive", k);
+        row0[(size_t)k + 1] = row0[(size_t)k] + n_of[k];
+        nmax = std::max(nmax, n_of[k]);
+    }
+    const int64_t rows = row0[(size_t)count];
+    for (int64_t i = 0; i < 3 * rows; ++i) SQS_REQUIRE(std::isfinite(xya[i]), "non-finite coordinate at %lld", (long long)i);
+    size_t tot = 0;
+    auto seg = [&](size_t b) { size_t o = tot; tot += (b + 255) & ~(size_t)255; return o; };
+    const size_t o_n = seg(sizeof(int32_t) * count), o_r = seg(sizeof(int64_t) * count);
+    const size_t o_s = seg(sizeof(double) * count), o_x = seg(sizeof(double) * 3 * (size_t)rows);
+    const size_t o_e = seg(sizeof(double) * count), o_g = seg(grad ? sizeof(double) * 3 * (size_t)rows : 0);
+    if (int r = ctx->d_polish.reserve(tot)) return r;
+    char* D = (char*)ctx->d_polish.p;
+    SQS_CUDA(cudaMemcpyAsync(D + o_n, n_of, sizeof(int32_t) * count, cudaMemcpyHostToDevice, ctx->stream));
+    SQS_CUDA(cudaMemcpyAsync(D + o_r, row0.data(), sizeof(int64_t) * count, cudaMemcpyHostToDevice, ctx->stream));
+    SQS_CUDA(cudaMemcpyAsync(D + o_s, side, sizeof(double) * count, cudaMemcpyHostToDevice, ctx->stream));
+    SQS_CUDA(cudaMemcpyAsync(D + o_x, xya, sizeof(double) * 3 * (size_t)rows, cudaMemcpyHostToDevice, ctx->stream));
+    if (int r = launch_energy_states(ctx->stream, count, (const int32_t*)(D + o_n), (const int64_t*)(D + o_r),
+                                     (const double*)(D + o_s), (const double*)(D + o_x), (double*)(D + o_e),
+                                     grad ? (double*)(D + o_g) : nullptr, energy_smem_bytes(nmax)))
+        return r;
+    ctx->launches += 1;
+    SQS_CUDA(cudaMemcpyAsync(energy, D + o_e, sizeof(double) * count, cudaMemcpyDeviceToHost, ctx->stream));
+    if (grad)
+        SQS_CUDA(cudaMemcpyAsync(grad, D + o_g, sizeof(double) * 3 * (size_t)rows, cudaMemcpyDeviceToHost, ctx->stream));
+    SQS_CUDA(cudaStreamSynchronize(ctx->stream));
     return SQS_OK;
 }

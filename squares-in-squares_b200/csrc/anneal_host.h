@@ -23,6 +23,11 @@ struct Shape {
 };
 
 int prime_anneal();
+int launch_trace(cudaStream_t stream, int items, const int2* list, const JobDev* jdev, const JobMut* jmut,
+                 const float4* pos, TraceRec* out, size_t smem);
+size_t energy_smem_bytes(int n);
+int launch_energy_states(cudaStream_t stream, int count, const int32_t* n_of, const int64_t* row0, const double* side,
+                         const double* xya, double* energy_out, double* grad, size_t smem);
 
 // One launch of the anneal kernel: the jobs job_list[0 .. njobs) sharing a
 // cluster shape, with the shared memory of the largest.

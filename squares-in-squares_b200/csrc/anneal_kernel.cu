@@ -654,6 +654,28 @@ __device__ __forceinline__ long long kick_replica(const Rep& rep, const Grid& g,
     return E;
 }
 
+// Ladder temperature of rung k: geometric from tmin (k = 0) to tmax
+// (k = R - 1), the reference's ladder T_b = tmin (tmax / tmin)^(b / 7) for
+// R = 8 (seeded.cu:493-494).
+__device__ __forceinline__ float rung_temp(const JobDev& jd, int k) {
+    const float lt = logf(jd.tmin), lh = logf(jd.tmax);
+    return jd.R > 1 ? expf(lt + (lh - lt) * (float)k / (float)(jd.R - 1)) : jd.tmin;
+}
+
+// Cooling factor of exchange round x under SQS_JOB_ADAPT: 0.002^((x mod 200)
+// / 199), the reference's cool (seeded.cu:493); 1 otherwise.
+__device__ __forceinline__ float cool_of(bool adaptive, int xround) {
+    return adaptive ? powf(0.002f, (float)(xround % 200) / 199.f) : 1.f;
+}
+
+// Step scale of a replica on rung `rung` under SQS_JOB_ADAPT: adaptation
+// factor x (0.15 + 1.85 rung / (R - 1)) x sqrt(cool), the reference's
+// scale = adapt * baseMove * (.15 + 1.85 (b % 8) / 7) * sqrt(cool)
+// (seeded.cu:506), in units of the job's sigma.
+__device__ __forceinline__ float step_scale(float adapt, int rung, int R, float cool) {
+    return adapt * (R > 1 ? 0.15f + 1.85f * (float)rung / (float)(R - 1) : 1.f) * sqrtf(cool);
+}
+
 struct CtaShared {
     JobDev jd;
     JobMut jm;
@@ -714,10 +736,7 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
     const int n = jd.n, R = jd.R, Rl = jd.Rl;
     const int r = rank * Rl + w;  // global replica index of this warp
     const bool active = w < Rl;
-    if (tid < R) {
-        const float lt = logf(jd.tmin), lh = logf(jd.tmax);
-        S.temps[tid] = R > 1 ? expf(lt + (lh - lt) * (float)tid / (float)(R - 1)) : jd.tmin;
-    }
+    if (tid < R) S.temps[tid] = rung_temp(jd, tid);
     const int64_t rb = replica_smem_bytes(n, jd.Gmax);
     Rep rep = rep_view(dyn + (active ? w : 0) * rb, n, jd.Gmax);
     float L = S.jm.L;
@@ -764,7 +783,7 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
     const bool adaptive = MOVES && (jd.flags & kMoveAdapt) != 0;
     float adapt = (MOVES && active) ? S.jm.adapt[r] : 1.f;
     int win = (MOVES && active) ? S.jm.win[r] : 0;
-    float cool = adaptive ? powf(0.002f, (float)(S.jm.xround % 200) / 199.f) : 1.f;
+    float cool = cool_of(adaptive, S.jm.xround);
     float invT = active ? 1.0f / (S.temps[S.jm.perm[r]] * cool) : 0.f;
     float4* save = pos + jd.pos_off + (int64_t)r * n;  // this replica's HBM slot: free while the slice runs
 
@@ -825,7 +844,7 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                     const int pidx = kb + q;
                     if (adaptive) {
                         const int rung = S.jm.perm[r];
-                        sc = adapt * (R > 1 ? 0.15f + 1.85f * (float)rung / (float)(R - 1) : 1.f) * sqrtf(cool);
+                        sc = step_scale(adapt, rung, R, cool);
                         if ((((uint64_t)sweep * (uint64_t)n + (uint64_t)pidx) & 15u) == 0) sc *= 3.5f;
                     }
                     const float dx = fminf(kMaxStep, fmaxf(-kMaxStep, sdx * sc));
@@ -1091,7 +1110,7 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
         }
         cluster.sync();
         __syncthreads();
-        if (adaptive) cool = powf(0.002f, (float)(S.jm.xround % 200) / 199.f);
+        if (adaptive) cool = cool_of(true, S.jm.xround);
         if (active) {
             invT = 1.0f / (S.temps[S.jm.perm[r]] * cool);
             if (S.decision_win == r) {
@@ -1169,6 +1188,70 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
         m.xacc = S.jm.xacc;
         for (int q = 0; q < R; ++q) m.perm[q] = S.jm.perm[q];
     }
+}
+
+// Final state of every replica, read back by sqs_anneal_batch_trace: one
+// warp per (job, replica) loads the replica as the annealer left it, rebuilds
+// its cell list on the job's grid and recomputes, with the annealer's own
+// device functions, its fixed-point energy from scratch (equal, bit for bit,
+// to the running energy the proposals kept when nothing drifts) and its FP64
+// dilation-certified side, and reports the temperature and step scale its
+// next proposal would use.
+__global__ void __launch_bounds__(32) trace_kernel(const int2* __restrict__ items, const JobDev* __restrict__ jdev,
+                                                   const JobMut* __restrict__ jmut, const float4* __restrict__ pos,
+                                                   TraceRec* __restrict__ out) {
+    extern __shared__ __align__(16) unsigned char dyn[];
+    const int2 it = items[blockIdx.x];
+    const JobDev& jd = jdev[it.x];
+    const JobMut& jm = jmut[it.x];
+    const int n = jd.n, r = it.y, lane = threadIdx.x;
+    const Rep rep = rep_view(dyn, n, jd.Gmax);
+    const float L = jm.L;
+    const Grid g = make_grid(L, jd.Gmax, jd.cell);
+    const float4* src = pos + jd.pos_off + (int64_t)r * n;
+    for (int i = lane; i < n; i += 32) {
+        const float4 p = src[i];
+        float sn, cs;
+        state_trig(p.z, &sn, &cs);
+        rep.sq[i] = make_float4(p.x, p.y, cs, sn);
+        rep.ang[i] = p.z;
+    }
+    __syncwarp();
+    const bool ok = build_cells(rep, n, g, lane);
+    const long long E = full_energy(rep, n, g, L, lane);
+    double lam = 0, x0 = 0, y0 = 0;
+    const double Lc = cert_side(rep, n, g, lane, lam, x0, y0);
+    if (lane == 0) {
+        const bool adaptive = (jd.flags & kMoveAdapt) != 0;
+        const float cool = cool_of(adaptive, jm.xround);
+        const int rung = jm.perm[r];
+        TraceRec t;
+        t.E_full = E;
+        t.L_cert = Lc;
+        t.lam = lam;
+        t.temp = rung_temp(jd, rung) * cool;
+        t.step = adaptive ? step_scale(jm.adapt[r], rung, jd.R, cool) : 1.f;
+        t.side = L;
+        t.rung = rung;
+        t.cells_ok = ok ? 1 : 0;
+        t.pad = 0;
+        out[blockIdx.x] = t;
+    }
+}
+
+int launch_trace(cudaStream_t stream, int items, const int2* list, const JobDev* jdev, const JobMut* jmut,
+                 const float4* pos, TraceRec* out, size_t smem) {
+    static bool attr_done[64] = {false};
+    int dev = 0;
+    SQS_CUDA(cudaGetDevice(&dev));
+    if (!attr_done[dev & 63]) {
+        SQS_CUDA(cudaFuncSetAttribute(trace_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAnnealSmemLimit));
+        attr_done[dev & 63] = true;
+    }
+    if (items <= 0) return SQS_OK;
+    trace_kernel<<<items, 32, smem, stream>>>(list, jdev, jmut, pos, out);
+    SQS_CUDA(cudaGetLastError());
+    return SQS_OK;
 }
 
 // Kernel attributes (dynamic shared memory up to the opt-in limit,

@@ -409,6 +409,57 @@ __global__ void __launch_bounds__(kPT) polish_states_kernel(const int32_t* __res
     }
 }
 
+// FP64 energy and gradient of arbitrary states, one CTA per state: the
+// polish's own energy function over all pairs (pair_smooth / wall_smooth
+// above), with cos and sin taken of the angles as given.  State k has n_of[k]
+// rows at xya + 3 * row0[k] and side side[k]; energy[k], and the gradient rows
+// at the same offsets of grad when grad is not null.
+__global__ void __launch_bounds__(kPT) energy_states_kernel(const int32_t* __restrict__ n_of,
+                                                            const int64_t* __restrict__ row0,
+                                                            const double* __restrict__ side,
+                                                            const double* __restrict__ xya,
+                                                            double* __restrict__ energy_out,
+                                                            double* __restrict__ grad) {
+    extern __shared__ __align__(16) unsigned char dyn[];
+    __shared__ double red[kPT / 32];
+    const int k = blockIdx.x;
+    const int n = n_of[k];
+    double3* q = reinterpret_cast<double3*>(dyn);
+    double3* g = q + n;
+    double2* cs = reinterpret_cast<double2*>(g + n);
+    const double* st = xya + 3 * row0[k];
+    for (int i = threadIdx.x; i < n; i += kPT) q[i] = make_double3(st[3 * i], st[3 * i + 1], st[3 * i + 2]);
+    __syncthreads();
+    trig_of(n, q, cs);
+    const double e = energy(n, q, cs, side[k], grad ? g : nullptr, red, nullptr);
+    if (threadIdx.x == 0) energy_out[k] = e;
+    if (grad) {
+        double* go = grad + 3 * row0[k];
+        for (int i = threadIdx.x; i < n; i += kPT) {
+            go[3 * i] = g[i].x;
+            go[3 * i + 1] = g[i].y;
+            go[3 * i + 2] = g[i].z;
+        }
+    }
+}
+
+size_t energy_smem_bytes(int n) { return (size_t)n * (2 * sizeof(double3) + sizeof(double2)) + 64; }
+
+int launch_energy_states(cudaStream_t stream, int count, const int32_t* n_of, const int64_t* row0, const double* side,
+                         const double* xya, double* energy_out, double* grad, size_t smem) {
+    static std::atomic<bool> attr_done[64];  // set-up once per device (idempotent if repeated)
+    int dev = 0;
+    SQS_CUDA(cudaGetDevice(&dev));
+    if (!attr_done[dev & 63]) {
+        SQS_CUDA(cudaFuncSetAttribute(energy_states_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        attr_done[dev & 63] = true;
+    }
+    if (count <= 0) return SQS_OK;
+    energy_states_kernel<<<count, kPT, smem, stream>>>(n_of, row0, side, xya, energy_out, grad);
+    SQS_CUDA(cudaGetLastError());
+    return SQS_OK;
+}
+
 int launch_polish_states(cudaStream_t stream, int count, const int32_t* n_of, const int64_t* row0, int iters,
                          double* xya, double* res, size_t smem) {
     static std::atomic<bool> attr_done[64];  // set-up once per device (idempotent if repeated)

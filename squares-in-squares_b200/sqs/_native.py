@@ -56,6 +56,15 @@ class JobResult(C.Structure):
                 ("L", C.c_char * 80), ("reason", C.c_char * 112)]
 
 
+class ReplicaTrace(C.Structure):
+    """sqs_replica_trace (include/sqs.h)."""
+    _fields_ = [("xya", C.POINTER(C.c_float)), ("energy", C.POINTER(C.c_double)),
+                ("energy_full", C.POINTER(C.c_double)), ("L_cert", C.POINTER(C.c_double)),
+                ("dilation", C.POINTER(C.c_double)), ("side", C.POINTER(C.c_float)),
+                ("temperature", C.POINTER(C.c_float)), ("step_scale", C.POINTER(C.c_float)),
+                ("rung", C.POINTER(C.c_int32)), ("exchange_rounds", C.c_int32), ("cells_ok", C.c_int32)]
+
+
 class Tuning(C.Structure):
     """sqs_tuning (include/sqs.h)."""
     _fields_ = [("cluster_ctas", C.c_int32), ("replicas_per_cta", C.c_int32), ("exchange_every", C.c_int32),
@@ -114,6 +123,10 @@ SIGNATURES: dict[str, tuple] = {
                                            C.POINTER(Verdict)]),
     "sqs_anneal_batch": (C.c_int, [_vp, C.POINTER(Job), C.c_int, C.c_int, C.POINTER(C.POINTER(C.c_double)),
                                    C.POINTER(JobResult)]),
+    "sqs_anneal_batch_trace": (C.c_int, [_vp, C.POINTER(Job), C.c_int, C.c_int, C.POINTER(C.POINTER(C.c_double)),
+                                         C.POINTER(JobResult), C.POINTER(ReplicaTrace)]),
+    "sqs_energy_fp64": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                  C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "sqs_server_create": (C.c_int, [_vp, C.c_size_t, C.c_int, C.c_int, C.POINTER(_vp)]),
     "sqs_server_destroy": (C.c_int, [_vp]),
     "sqs_server_submit": (C.c_int, [_vp, C.POINTER(Job), C.POINTER(C.c_int64)]),

@@ -73,21 +73,47 @@ def _cjob(j: AnnealJob) -> N.Job:
                  xya_rep=j.xya_rep.ctypes.data_as(C.POINTER(C.c_double)) if j.xya_rep is not None else None)
 
 
-def anneal_batch(jobs: list[AnnealJob], *, ctx: N.Context | None = None, slice_sweeps: int = 0) -> list[dict]:
-    """Run jobs in batched launches; returns one result dict per job."""
+def _trace_buffers(j: AnnealJob) -> dict:
+    R, n = j.replicas, j.n
+    return dict(xya=np.zeros((R, n, 3), np.float32), energy=np.zeros(R), energy_full=np.zeros(R),
+                L_cert=np.zeros(R), dilation=np.zeros(R), side=np.zeros(R, np.float32),
+                temperature=np.zeros(R, np.float32), step_scale=np.zeros(R, np.float32),
+                rung=np.zeros(R, np.int32))
+
+
+def _ctrace(b: dict) -> N.ReplicaTrace:
+    t = N.ReplicaTrace()
+    for name, arr in b.items():
+        ct = {np.dtype(np.float32): C.c_float, np.dtype(np.float64): C.c_double,
+              np.dtype(np.int32): C.c_int32}[arr.dtype]
+        setattr(t, name, arr.ctypes.data_as(C.POINTER(ct)))
+    return t
+
+
+def anneal_batch(jobs: list[AnnealJob], *, ctx: N.Context | None = None, slice_sweeps: int = 0,
+                 trace: bool = False) -> list[dict]:
+    """Run jobs in batched launches; returns one result dict per job.  With
+    trace=True (sqs_anneal_batch_trace) each dict also has "trace": every
+    replica's final FP32 state, its running and recomputed energies, its FP64
+    certified side, side, temperature, step scale and rung."""
     own = ctx is None
     ctx = ctx or N.Context(0)
+    tbufs = [_trace_buffers(j) for j in jobs] if trace else None
+    tstructs = (N.ReplicaTrace * max(1, len(jobs)))(*[_ctrace(b) for b in tbufs]) if trace else None
     try:
         arr = (N.Job * max(1, len(jobs)))(*[_cjob(j) for j in jobs])
         res = (N.JobResult * max(1, len(jobs)))()
         outs = [np.zeros((j.n, 3)) for j in jobs]
         ptrs = (C.POINTER(C.c_double) * max(1, len(jobs)))(*[o.ctypes.data_as(C.POINTER(C.c_double)) for o in outs])
-        N.check(N.lib().sqs_anneal_batch(ctx.handle, arr, len(jobs), slice_sweeps, ptrs, res))
+        if trace:
+            N.check(N.lib().sqs_anneal_batch_trace(ctx.handle, arr, len(jobs), slice_sweeps, ptrs, res, tstructs))
+        else:
+            N.check(N.lib().sqs_anneal_batch(ctx.handle, arr, len(jobs), slice_sweeps, ptrs, res))
     finally:
         if own:
             ctx.close()
     out = []
-    for j, r, q in zip(jobs, res, outs):
+    for k, (j, r, q) in enumerate(zip(jobs, res, outs)):
         ok = bool(r.certified)
         rows = [dict(square_id=str(i), x=format(float(x), ".17g"), y=format(float(y), ".17g"),
                      angle=format(float(a), ".17g")) for i, (x, y, a) in enumerate(q)] if ok else None
@@ -102,6 +128,11 @@ def anneal_batch(jobs: list[AnnealJob], *, ctx: N.Context | None = None, slice_s
             launch=dict(cluster_ctas=int(r.cluster_ctas), replicas_per_cta=int(r.replicas_per_cta),
                         exchange_every=int(r.exchange_every), cell_side=float(r.cell_side),
                         overflows=int(r.overflows))))
+        if trace:
+            t = dict(tbufs[k])
+            t["exchange_rounds"] = int(tstructs[k].exchange_rounds)
+            t["cells_ok"] = bool(tstructs[k].cells_ok)
+            out[-1]["trace"] = t
     return out
 
 

@@ -6,6 +6,8 @@ pairs of the squared separating-axis penetration (seeded.cu:41-65, 96-113,
 """
 from __future__ import annotations
 
+import ctypes as C
+
 import numpy as np
 
 from . import _native as N
@@ -46,3 +48,33 @@ def energy_device(ctx: N.Context, configs: int, n: int, xya: N.DeviceArray, side
     N.check(N.lib().sqs_sat_energy(ctx.handle, configs, n, xya.ptr, side.ptr, out.ptr,
                                    grad.ptr if grad is not None else None,
                                    cand.ptr if cand is not None else None, threads))
+
+
+def energy_fp64(states, sides, *, ctx: N.Context | None = None, grad: bool = True):
+    """FP64 energy (and gradient) of packings of any sizes (sqs_energy_fp64):
+    walls plus pairs, all pairs, with the polish's smooth gradient.
+
+    states: list of (n_k, 3) arrays (or one (configs, n, 3) array); sides:
+    scalar or one per packing.  Returns (energy float64[count], list of
+    (n_k, 3) gradients | None)."""
+    if isinstance(states, np.ndarray) and states.ndim == 3:
+        states = list(states)
+    states = [np.ascontiguousarray(q, dtype=np.float64).reshape(-1, 3) for q in states]
+    count = len(states)
+    n_of = np.array([q.shape[0] for q in states], dtype=np.int32)
+    flat = np.ascontiguousarray(np.concatenate(states, axis=0)) if count else np.zeros((0, 3))
+    side = np.ascontiguousarray(np.broadcast_to(np.asarray(sides, dtype=np.float64), (count,)))
+    e = np.zeros(count)
+    g = np.zeros_like(flat) if grad else None
+    own = ctx is None
+    ctx = ctx or N.Context(0)
+    try:
+        N.check(N.lib().sqs_energy_fp64(ctx.handle, count, N.ptr(n_of, C.POINTER(C.c_int32)),
+                                        N.ptr(flat, N._dp), N.ptr(side, N._dp), N.ptr(e, N._dp),
+                                        N.ptr(g, N._dp)))
+    finally:
+        if own:
+            ctx.close()
+    if g is None:
+        return e, None
+    return e, np.split(g, np.cumsum(n_of)[:-1])

@@ -144,3 +144,29 @@ def test_python_api_mirror(ctx):
     report = core.score({2: core.grid(2), 3: [dict(square_id="0", x=".5", y=".5", angle="0")]}, max_n=4, ctx=ctx)
     assert report["accepted"] == 1 and report["rejected"] == 1 and report["missing"] == 2
     assert report["score"] == pytest.approx(sum(core.infeasible_score(n) for n in (1, 3, 4)) + (2 / math.sqrt(2) - 1))
+
+
+def test_full_seed42_corpus_equals_reference(ctx, oracle):
+    """The whole certifier batch of the benchmark -- 10,000 packings, n
+    log-uniform in [5, 1000], grids, tilted near-contact lattices, injected
+    overlaps, seed 42 -- certified on the GPU in one call: verdict, reason,
+    score and 50-decimal side equal to the compiled reference certifier
+    (certifier.cpp, evaluate_single_puzzle :738-912) on every packing, or to
+    the oracle restatement where the reference was not compiled."""
+    from sqs import core
+    from sqs.workloads import certify_corpus
+    items = certify_corpus(10000, seed=42)
+    arrs = core.pack_batch(items)
+    out = core.certify_arrays(*arrs, ctx=ctx)
+    which = "ref" if oracle.ref_available() else "oracle"
+    ok, score, Ls, reasons = oracle.certify_batch_text(*arrs, which=which)
+    bad = []
+    for p in range(len(items)):
+        v = out[p]
+        got = (int(v.ok), float(v.score), v.L.decode(), v.reason.decode())
+        want = (int(ok[p]), float(score[p]), Ls[p], reasons[p])
+        if got != want:
+            bad.append((p, items[p][0], got, want))
+    assert not bad, (len(bad), bad[:3])
+    assert 0 < ok.sum() < len(items)
+    assert max(n for n, _ in items) > 900

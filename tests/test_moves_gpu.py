@@ -38,9 +38,9 @@ def test_move_options_are_reproducible(ctx, oracle, opts):
     assert alone["proposals"] == 16 * 200 * 40
     assert alone["launch"]["overflows"] == 0
     assert alone["q"] != plain["q"] or alone["accepted"] != plain["accepted"]  # the option acts
-    if alone["certified"]:
-        ok, L, reason, _ = oracle.certify(40, alone["rows"])
-        assert ok and L == alone["L"], reason
+    assert alone["certified"], alone["reason"]
+    ok, L, reason, _ = oracle.certify(40, alone["rows"])
+    assert ok and L == alone["L"], reason
     mixed = anneal_batch([_job(n=25, seed=2), job, _job(n=60, seed=5, **opts)], ctx=ctx)[1]
     sliced = anneal_batch([job], ctx=ctx, slice_sweeps=50)[0]
     wide = anneal_batch([replace(job, cluster=4)], ctx=ctx)[0]
@@ -67,9 +67,9 @@ def test_checkpoint_options_are_reproducible(ctx, oracle, opts):
     assert alone["launch"]["overflows"] == 0
     if opts.get("cert_all"):
         assert alone["improvements"] >= 1
-    if alone["certified"]:
-        ok, L, reason, _ = oracle.certify(40, alone["rows"])
-        assert ok and L == alone["L"], reason
+    assert alone["certified"], alone["reason"]
+    ok, L, reason, _ = oracle.certify(40, alone["rows"])
+    assert ok and L == alone["L"], reason
     mixed = anneal_batch([_job(n=25, seed=2), job, _job(n=60, seed=5, **opts)], ctx=ctx)[1]
     sliced = anneal_batch([job], ctx=ctx, slice_sweeps=50)[0]
     wide = anneal_batch([replace(job, cluster=4)], ctx=ctx)[0]
