@@ -155,9 +155,14 @@ int sqs_certify_batch_static(sqs_ctx* ctx, int count, const int32_t* n_of, const
 typedef struct sqs_job {
     int32_t n;               /* squares, 1..1000                                  */
     int32_t replicas;        /* temperature rungs, 1..64                          */
-    int32_t sweeps;          /* sweep budget; one sweep = n proposals per replica */
-    int32_t exchange_every;  /* sweeps between replica-exchange rounds; 0 = chosen
-                                by the autotuner (needs SQS_JOB_AUTOTUNE)         */
+    int32_t sweeps;          /* budget in sweeps (one sweep = n proposals per
+                                replica); negative: -sweeps proposals per replica */
+    int32_t exchange_every;  /* sweeps between checkpoints (best-state search,
+                                shrink, replica exchange); negative: every
+                                -exchange_every proposals per replica, as the
+                                reference checkpoints after every epoch of
+                                `steps` proposals; 0 = chosen by the autotuner
+                                (needs SQS_JOB_AUTOTUNE)                          */
     int32_t polish_iters;    /* FP64 gradient-polish iterations on the best state */
     int32_t flags;           /* SQS_JOB_* bits, 0 = fixed default launch shape    */
     double L0;               /* initial container side                            */
@@ -226,6 +231,23 @@ typedef struct sqs_job {
  * (seeded.cu:621-713).  k = 0: 64 iterations, also ending after three
  * accepted steps in a row that each gained less than 0.1%. */
 #define SQS_JOB_QUENCH_STEPS(k) ((int32_t)(k) << 24)
+/* The reference search's target-side ladder (seeded.cu:474-481, 908-943): from
+ * the first proposal every rung anneals in its own container below the best
+ * side B found so far (the initial side before the first certificate):
+ * side max(sqrt n + 1e-6, B (1 - shrink m)) with m the reference's offsets
+ * {0.02, 0.1, 0.4, 1, 2.5, 5, 10, 20} for the rung's place in its ladder.  A
+ * new certified best becomes B (no further factor), every ladder's head rung
+ * (and, after a gain above 5e-4, every rung of ladder 0) restarts from the
+ * new best state scaled into its side, and replicas exchange only at
+ * checkpoints without a new best.  Energies are measured in each replica's
+ * own side. */
+#define SQS_JOB_TARGETS 128
+/* Split the job's rungs into l ladders of replicas / l rungs each (l = 1..15,
+ * dividing replicas): temperatures, step scales and target offsets run over a
+ * ladder's rungs, and exchange pairs neighbours within a ladder, as the
+ * reference runs its chains as ladders of 8 (seeded.cu:493, 791-817); the
+ * ladders share the job's best side.  0 or 1: one ladder. */
+#define SQS_JOB_LADDERS(l) ((int32_t)(l) << 20)
 /* Pin the launch shape instead of SQS_JOB_AUTOTUNE: a cluster of `cs` CTAs (1..16; it must
  * divide the replica count and fit) and cell side index k (0: 1.59, 1: 1.75,
  * 2: 1.95, 3: 2.2).  Same trajectory as any other shape (see above). */

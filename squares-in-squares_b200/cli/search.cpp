@@ -14,14 +14,17 @@
 // autotune.summarize) work unchanged.
 //
 // Mapping onto sqs_anneal_batch:
-//   * every ladder of 8 chains is one job of 8 replicas (temperature rungs);
-//     the chains/8 jobs run side by side in one batched call, each with its
-//     own seed, and the report takes the job with the smallest certified side;
-//   * a reference step is one proposal per chain, so a job runs
-//     ceil(epochs * steps / n) sweeps of n proposals per replica, and
-//     exchanges replicas once per epoch's worth of sweeps;
-//   * the absolute shrink step becomes a relative one (shrink / L), times
-//     the multiplier of the ladder's place among the reference's 8 targets;
+//   * every ladder of 8 chains is a ladder of 8 rungs (SQS_JOB_LADDERS), up to
+//     8 ladders to a job so that they share one best side, as all of the
+//     reference's chains share its bestL; the jobs run side by side in one
+//     batched call, and the report takes the smallest certified side;
+//   * every rung anneals in its own container below the best,
+//     best - shrink * {0.02 .. 20}[rung], restarts ladder heads from a new
+//     best and exchanges only in epochs without one (SQS_JOB_TARGETS);
+//   * a reference step is one proposal per chain: a job runs epochs * steps
+//     proposals per replica and checkpoints (quench, certificate, kick,
+//     exchange) after every epoch of `steps` proposals;
+//   * the absolute shrink step becomes a relative one (shrink / L);
 //   * chains = 0 (or *_AUTOTUNE=1 with chains >= 64) takes one ladder per SM,
 //     capped at *_MAX_CHAINS, as the reference sizes chains to a wave;
 //     *_AUTOTUNE=1 also lets the launch autotuner pick each job's shape;
@@ -36,13 +39,16 @@
 //     and under SEED_STRUCTURED for seeded;
 //   * the angle proposal width is 2.5 x the move width (PACK_ROTATION is
 //     validated and reported but, as in the reference, not used);
-//   * three variables of this build's own, validated like the others:
-//     *_QUENCH_ALL (0 or 1) quenches every replica at each exchange round,
-//     *_CERT_ALL (0 or 1) dilation-certifies every replica at each
-//     checkpoint whatever its overlap, and *_QUENCH_STEPS (-1..2032) sets the
-//     quench iterations per checkpoint with no exit on slow progress (0 keeps
-//     the library's, -1 takes the polish iterations of the epochs one
-//     checkpoint spans); both default to 1, 1, -1.
+//   * four variables of this build's own, validated like the others:
+//     *_TARGETS (0 or 1) selects the target-side ladders above (0: one job per
+//     ladder, checkpoints every max(1, round(steps / n)) sweeps, the side
+//     shrunk after each certificate by the ladder's place among the
+//     reference's 8 offsets), *_QUENCH_ALL (0 or 1) quenches every replica at
+//     each checkpoint, *_CERT_ALL (0 or 1) dilation-certifies every replica at
+//     each checkpoint whatever its overlap, and *_QUENCH_STEPS (-1..2032) sets
+//     the quench iterations per checkpoint with no exit on slow progress (0
+//     keeps the library's, -1 takes the polish iterations of the epochs one
+//     checkpoint spans); they default to 1, 1, 1, -1.
 // "target_L" is the FP64 dilation-certified side of the best state and "q"
 // that state (the packing the interval certifier accepted); when no ladder
 // finds a certified state the seed is reported with its side, as the
@@ -150,6 +156,7 @@ int main(int argc, char** argv) {
     // and certificate of every chain (seeded.cu:621-720, packing.cu:630-689).
     // Quench iterations per checkpoint: 0 = the library's
     // default, -1 = the polish iterations of the epochs one checkpoint spans.
+    const int targets = (int)env("TARGETS", 1, 0, 1);
     const int cert_all = (int)env("CERT_ALL", 1, 0, 1);
     const int quench_all = (int)env("QUENCH_ALL", 1, 0, 1);
     const int quench_steps = (int)env("QUENCH_STEPS", -1, -1, 2032);
@@ -178,7 +185,8 @@ int main(int argc, char** argv) {
     if (quench_steps > 0) {
         quench_k = (quench_steps + 15) / 16;
     } else if (quench_steps < 0 && polish > 0) {
-        const double iters = (double)polish * per_epoch * n / steps;
+        // the polish iterations of the epochs one checkpoint spans
+        const double iters = targets ? (double)polish : (double)polish * per_epoch * n / steps;
         quench_k = (int)std::min(127.0, std::ceil(iters / 16.0));
     }
 
@@ -187,41 +195,63 @@ int main(int argc, char** argv) {
     std::vector<double> starts(3 * (size_t)n * (size_t)chains);
     if (sqs_portfolio(n, L, seed.data(), chains, structured, rng_seed, 1, starts.data()) != SQS_OK)
         return fail("portfolio");
-    std::vector<sqs_job> jobs((size_t)ladders);
-    std::vector<std::vector<double>> outs((size_t)ladders, std::vector<double>(3 * (size_t)n));
-    std::vector<double*> ptrs((size_t)ladders);
-    for (int k = 0; k < ladders; ++k) {
-        sqs_job& j = jobs[(size_t)k];
-        std::memset(&j, 0, sizeof j);
-        j.n = n;
-        j.replicas = 8;
-        j.sweeps = sweeps;
-        j.exchange_every = per_epoch;
-        j.polish_iters = polish;
-        j.flags = (autotune ? SQS_JOB_AUTOTUNE : 0) | SQS_JOB_ADAPT | SQS_JOB_KICK | (collective ? SQS_JOB_COLLECTIVE : 0) |
-                  (cert_all ? SQS_JOB_CERT_ALL : 0) | (quench_all ? SQS_JOB_QUENCH_ALL : 0) |
-                  SQS_JOB_QUENCH_STEPS(quench_k);
-        j.L0 = L;
-        j.tmin = tmin;
-        j.tmax = tmax;
-        j.sigma_xy = mv;
-        j.sigma_a = std::min(1.0, 2.5 * mv);
-        j.shrink = std::min(0.1, shrink * kShrinkMults[k % 8] / L);
-        j.seed = rng_seed + 0x9E3779B97F4A7C15ull * (unsigned long long)k;
-        j.xya = seed.data();
-        j.xya_rep = starts.data() + 3 * (size_t)n * 8 * (size_t)k;
-        ptrs[(size_t)k] = outs[(size_t)k].data();
+    // Jobs of `per_job` ladders each (one ladder per job without targets); a
+    // job whose ladders do not fit one cluster is retried with half as many.
+    std::vector<sqs_job> jobs;
+    std::vector<std::vector<double>> outs;
+    std::vector<double*> ptrs;
+    std::vector<sqs_job_result> res;
+    double seconds = 0.0;
+    for (int per_job = targets ? std::min(8, ladders) : 1;; per_job = std::max(1, per_job / 2)) {
+        const int njobs = (ladders + per_job - 1) / per_job;
+        jobs.assign((size_t)njobs, sqs_job{});
+        outs.assign((size_t)njobs, std::vector<double>(3 * (size_t)n));
+        ptrs.assign((size_t)njobs, nullptr);
+        res.assign((size_t)njobs, sqs_job_result{});
+        for (int k = 0; k < njobs; ++k) {
+            const int lad = std::min(per_job, ladders - k * per_job);  // ladders of this job
+            sqs_job& j = jobs[(size_t)k];
+            std::memset(&j, 0, sizeof j);
+            j.n = n;
+            j.replicas = 8 * lad;
+            j.polish_iters = polish;
+            j.flags = (autotune ? SQS_JOB_AUTOTUNE : 0) | SQS_JOB_ADAPT | SQS_JOB_KICK |
+                      (collective ? SQS_JOB_COLLECTIVE : 0) | (cert_all ? SQS_JOB_CERT_ALL : 0) |
+                      (quench_all ? SQS_JOB_QUENCH_ALL : 0) | SQS_JOB_QUENCH_STEPS(quench_k);
+            if (targets) {
+                // epochs * steps proposals, a checkpoint after every epoch
+                j.sweeps = (int)std::max<long long>(-2000000000LL, -std::max(1LL, proposals_per_chain));
+                j.exchange_every = -std::max(1, steps);
+                j.flags |= SQS_JOB_TARGETS | SQS_JOB_LADDERS(lad);
+                j.shrink = std::min(0.1 / 20.0, shrink / L);
+            } else {
+                j.sweeps = sweeps;
+                j.exchange_every = per_epoch;
+                j.shrink = std::min(0.1, shrink * kShrinkMults[k % 8] / L);
+            }
+            j.L0 = L;
+            j.tmin = tmin;
+            j.tmax = tmax;
+            j.sigma_xy = mv;
+            j.sigma_a = std::min(1.0, 2.5 * mv);
+            j.seed = rng_seed + 0x9E3779B97F4A7C15ull * (unsigned long long)k;
+            j.xya = seed.data();
+            j.xya_rep = starts.data() + 3 * (size_t)n * 8 * (size_t)k * (size_t)per_job;
+            ptrs[(size_t)k] = outs[(size_t)k].data();
+        }
+        const auto t0 = std::chrono::steady_clock::now();
+        const int rc = sqs_anneal_batch(ctx, jobs.data(), njobs, 0, ptrs.data(), res.data());
+        seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (rc == SQS_OK) break;
+        if (rc != SQS_EINVAL || per_job == 1 || !std::strstr(sqs_last_error(), "does not fit")) return fail("anneal");
     }
-    std::vector<sqs_job_result> res((size_t)ladders);
-    const auto t0 = std::chrono::steady_clock::now();
-    if (sqs_anneal_batch(ctx, jobs.data(), ladders, 0, ptrs.data(), res.data()) != SQS_OK) return fail("anneal");
-    const double seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    const int njobs = (int)jobs.size();
 
     double bestL = L;
     const double* best = seed.data();
     long long proposals = 0, accepted = 0, xatt = 0, xacc = 0;
     int shrinks = 0, feasible = 0;
-    for (int k = 0; k < ladders; ++k) {
+    for (int k = 0; k < njobs; ++k) {
         const sqs_job_result& r = res[(size_t)k];
         proposals += r.proposals;
         accepted += r.accepted;

@@ -17,7 +17,7 @@ constexpr int kMaxN = 1000;
 // Per job, read-only while a slice runs.
 struct JobDev {
     int32_t n, R, cs, Rl;             // squares, replicas, CTAs per job (cluster size), replicas per CTA
-    int32_t sweeps_total, exchange_every;
+    int32_t ladders, exchange_every;  // ladders of R / ladders rungs each; the job's exchange_every (as given)
     int32_t Gmax, polish_iters;       // cell grid side for the initial container; polish iterations
     float sigma_xy, sigma_a, tmin, tmax;
     float shrink, L0, cell, pad1;     // cell: minimum cell side of the cell lists (>= kCellSide)
@@ -25,6 +25,8 @@ struct JobDev {
     int64_t pos_off;                  // float4 index of replica 0, square 0
     int64_t best_off;                 // double index of the best state (n x 3)
     int64_t scr_off;                  // float4 index of the job's quench scratch (2n)
+    int64_t props_total;              // proposals per replica in the job's budget
+    int64_t xprops;                   // proposals per replica between checkpoints
     int32_t quench_iters, flags;      // gradient steps of a checkpoint quench (at most); kMove* bits
     int32_t slice;                    // sweeps per launch for this job (0: the launch's slice)
     int32_t quench_stall;             // accepted slow steps (< 0.1% gained each) that end a quench
@@ -34,20 +36,31 @@ struct JobDev {
 // kMoveSerial selects the one-at-a-time kernel instance and changes nothing else;
 // kCertAll (SQS_JOB_CERT_ALL) only drops the energy gate of the checkpoint's
 // dilation certificate and keeps the kernel instance the other bits select
+// kTargets (SQS_JOB_TARGETS) gives every rung its own side below the best and
+// also selects the move-set instance, which holds the per-replica sides.
 enum : int32_t { kMoveAdapt = 2, kMoveCollective = 4, kMoveKick = 8, kMoveSerial = 16, kMoveQuenchAll = 32,
-                 kCertAll = 64 };
+                 kCertAll = 64, kTargets = 128 };
 
 // Whether a job's flags select the move-set kernel instance.
 inline bool uses_moves(int32_t flags) { return (flags & ~kCertAll) != 0; }
 
+// The reference's ladder of target offsets: rung b % 8 of a ladder anneals at
+// best - shrink * {0.02, 0.1, 0.4, 1, 2.5, 5, 10, 20}[b % 8] (seeded.cu:478-481).
+// A ladder of RL rungs takes entry round(7 pos / (RL - 1)) for its rung pos.
+__host__ __device__ inline float target_mult(int pos, int RL) {
+    const float m[8] = {0.02f, 0.1f, 0.4f, 1.0f, 2.5f, 5.0f, 10.0f, 20.0f};
+    if (RL <= 1) return 1.0f;
+    return m[(pos * 7 + (RL - 1) / 2) / (RL - 1)];
+}
+
 // Per job, advanced by every slice.
 struct JobMut {
-    float L;                          // current container side
-    int32_t sweep;                    // sweeps completed
+    float L;                          // container side (SQS_JOB_TARGETS: the best side the rung sides hang from)
     int32_t xround;                   // exchange rounds completed
     int32_t status;                   // 0 running, 1 finished, < 0 error
     int32_t shrinks, improvements;
-    int32_t overflows, pad1;          // overflows: moves rejected because the target cell was full
+    int32_t overflows;                // moves rejected because the target cell was full
+    int64_t done;                     // proposals per replica completed
     double best_L;                    // best FP64 dilation-certified side (1e30: none yet)
     uint64_t proposals, accepted, xatt, xacc;
     int32_t perm[kMaxR];              // rung (temperature index) of each replica

@@ -75,8 +75,11 @@ void put(char* dst, size_t cap, const std::string& s) {
 int prepare_job(const sqs_job& J, int j, JobDev& d, JobMut& m, Plan& p, const Shape* shape) {
     SQS_REQUIRE(J.n >= 1 && J.n <= kMaxN, "job %d: n=%d out of 1..%d", j, J.n, kMaxN);
     SQS_REQUIRE(J.replicas >= 1 && J.replicas <= kMaxR, "job %d: replicas=%d out of 1..%d", j, J.replicas, kMaxR);
-    SQS_REQUIRE(J.sweeps >= 0 && J.sweeps <= 100000000, "job %d: sweeps=%d out of range", j, J.sweeps);
-    SQS_REQUIRE(J.exchange_every >= 1, "job %d: exchange_every must be >= 1", j);
+    SQS_REQUIRE(J.sweeps >= -2000000000 && J.sweeps <= 100000000, "job %d: sweeps=%d out of range", j, J.sweeps);
+    SQS_REQUIRE(J.exchange_every != 0 && J.exchange_every >= -1000000000,
+                "job %d: exchange_every must be nonzero (sweeps, or -proposals)", j);
+    const int ladders = std::max(1, (J.flags >> 20) & 0xf);
+    SQS_REQUIRE(J.replicas % ladders == 0, "job %d: %d replicas do not split into %d ladders", j, J.replicas, ladders);
     SQS_REQUIRE(std::isfinite(J.L0) && J.L0 > 0 && J.L0 <= 64, "job %d: L0 must be in (0, 64]", j);
     SQS_REQUIRE(J.tmin > 0 && J.tmax >= J.tmin && std::isfinite(J.tmax), "job %d: need 0 < tmin <= tmax", j);
     SQS_REQUIRE(J.sigma_xy > 0 && J.sigma_xy <= 0.3 && J.sigma_a > 0 && J.sigma_a <= 1.0,
@@ -96,8 +99,10 @@ int prepare_job(const sqs_job& J, int j, JobDev& d, JobMut& m, Plan& p, const Sh
     d.R = J.replicas;
     d.cs = p.cs;
     d.Rl = p.Rl;
-    d.sweeps_total = J.sweeps;
+    d.ladders = ladders;
     d.exchange_every = J.exchange_every;
+    d.props_total = job_props(J);
+    d.xprops = J.exchange_every > 0 ? (int64_t)J.exchange_every * J.n : -(int64_t)J.exchange_every;
     d.Gmax = p.Gmax;
     d.polish_iters = J.polish_iters;
     d.sigma_xy = (float)J.sigma_xy;
@@ -113,11 +118,11 @@ int prepare_job(const sqs_job& J, int j, JobDev& d, JobMut& m, Plan& p, const Sh
     const int qk = (J.flags >> 24) & 0x7f;
     d.quench_iters = qk ? 16 * qk : 64;
     d.quench_stall = qk ? 0x7fffffff : 3;
-    d.flags = J.flags & (kMoveAdapt | kMoveCollective | kMoveKick | kMoveSerial | kMoveQuenchAll | kCertAll);
+    d.flags = J.flags & (kMoveAdapt | kMoveCollective | kMoveKick | kMoveSerial | kMoveQuenchAll | kCertAll | kTargets);
     std::memset(&m, 0, sizeof m);
     m.L = (float)J.L0;
     m.best_L = 1e30;
-    m.status = J.sweeps == 0 ? kFinished : kRunning;
+    m.status = d.props_total == 0 ? kFinished : kRunning;
     for (int r = 0; r < J.replicas; ++r) {
         m.perm[r] = r;
         m.adapt[r] = 1.0f;
@@ -127,6 +132,10 @@ int prepare_job(const sqs_job& J, int j, JobDev& d, JobMut& m, Plan& p, const Sh
 }
 
 int64_t job_pos_elems(const sqs_job& J) { return (int64_t)J.replicas * J.n + 2 * (int64_t)J.n; }
+
+int64_t job_props(const sqs_job& J) { return J.sweeps >= 0 ? (int64_t)J.sweeps * J.n : -(int64_t)J.sweeps; }
+
+int64_t job_sweeps(const sqs_job& J) { return J.n > 0 ? (job_props(J) + J.n - 1) / J.n : 0; }
 
 void init_replicas(const sqs_job& J, float4* dst) {
     for (int r = 0; r < J.replicas; ++r) {
@@ -146,7 +155,7 @@ void fill_result(const sqs_job& J, const JobDev& d, const JobMut& m, float dev_m
     o.cell_side = d.cell;
     o.shrinks = m.shrinks;
     o.improvements = m.improvements;
-    o.sweeps_done = m.sweep;
+    o.sweeps_done = (int32_t)(m.done / std::max(1, J.n));
     o.replicas = J.replicas;
     o.L_cert = m.best_L;
     o.L_polished = m.best_L;
@@ -276,7 +285,7 @@ static int copies_for(const sqs_job& J, const Plan& p, int mode, int* copies) {
     *copies = 1;
     if (mode & SQS_TUNE_LATENCY) return SQS_OK;
     int waves = 1;
-    const bool moves = (J.flags & (SQS_JOB_ADAPT | SQS_JOB_COLLECTIVE | SQS_JOB_KICK | SQS_JOB_SERIAL | SQS_JOB_QUENCH_ALL)) != 0;
+    const bool moves = uses_moves(J.flags & 0xfe);  // option bits above SQS_JOB_AUTOTUNE
     if (int r = anneal_max_clusters(p.cs, p.Rl, anneal_smem(p.cs, p.Rl, p.rb, J.n, moves), moves, &waves)) return r;
     const size_t per = sizeof(float4) * (size_t)job_pos_elems(J) + sizeof(double) * 3 * (size_t)J.n + 1024;
     *copies = (int)std::max<int64_t>(1, std::min<int64_t>(waves, (int64_t)(kTuneBytes / per)));
@@ -286,7 +295,7 @@ static int copies_for(const sqs_job& J, const Plan& p, int mode, int* copies) {
 static int autotune(sqs_ctx* ctx, const sqs_job& job, int mode, sqs_tuning& out) {
     std::memset(&out, 0, sizeof out);
     sqs_job J = job;
-    const bool tune_xe = J.exchange_every <= 0;
+    const bool tune_xe = J.exchange_every == 0;
     if (tune_xe) J.exchange_every = 10;  // interval used while shapes are compared
     {
         JobDev d;
@@ -315,9 +324,9 @@ static int autotune(sqs_ctx* ctx, const sqs_job& job, int mode, sqs_tuning& out)
     }
     // a trial is a whole number of exchange intervals (the job's own
     // checkpoint frequency), about 2,000 proposals per replica
-    const int xe = J.exchange_every;
+    const int xe = J.exchange_every;  // sweeps, or (negative) proposals, between checkpoints
     const int want = std::max(2, std::min(100, (2000 + J.n - 1) / J.n));
-    const int sweeps = std::max(xe, (want + xe - 1) / xe * xe);
+    const int sweeps = xe > 0 ? std::max(xe, (want + xe - 1) / xe * xe) : want;
     struct Cand {
         Plan p;
         float per_copy;  // throughput mode: device time per job in a full wave; latency mode: time alone
@@ -407,7 +416,7 @@ static int autotune(sqs_ctx* ctx, const sqs_job& job, int mode, sqs_tuning& out)
 int resolve_job(sqs_ctx* ctx, const sqs_job& job, int mode, sqs_job& eff, Shape& shape) {
     eff = job;
     shape = Shape{};
-    SQS_REQUIRE((job.flags & ~0x7f0fff7f) == 0, "unknown job flags 0x%x", (unsigned)job.flags);
+    SQS_REQUIRE(job.flags >= 0, "unknown job flags 0x%x", (unsigned)job.flags);
     const int pin_cs = (job.flags >> 8) & 0xff, pin_cell = (job.flags >> 16) & 0xf;
     if (pin_cs || pin_cell) {
         SQS_REQUIRE(!(job.flags & SQS_JOB_AUTOTUNE), "SQS_JOB_AUTOTUNE and a pinned shape exclude each other");
@@ -429,13 +438,13 @@ int resolve_job(sqs_ctx* ctx, const sqs_job& job, int mode, sqs_job& eff, Shape&
     if (int r = autotune(ctx, job, mode, t)) return r;
     shape.cs = t.cluster_ctas;
     shape.cell = (float)t.cell_side;
-    if (job.exchange_every <= 0) eff.exchange_every = t.exchange_every;
+    if (job.exchange_every == 0) eff.exchange_every = t.exchange_every;
     return SQS_OK;
 }
 
 void add_rescue(std::vector<Rescue>& out, const sqs_job& J, const JobDev& d, JobMut& m, const float4* d_pos,
                 double* best) {
-    if (m.status != kFinished || m.best_L < 1e29 || J.polish_iters <= 0 || J.sweeps <= 0) return;
+    if (m.status != kFinished || m.best_L < 1e29 || J.polish_iters <= 0 || job_props(J) <= 0) return;
     int cold = 0;
     for (int r = 0; r < J.replicas; ++r)
         if (m.perm[r] == 0) cold = r;
@@ -624,7 +633,7 @@ static int anneal_run(sqs_ctx* ctx, const sqs_job* jobs, int njobs, int slice_sw
                              ctx->stream));
     int max_sweeps = 0, max_xe = 1;
     for (int j = 0; j < njobs; ++j) {
-        max_sweeps = std::max(max_sweeps, jobs[j].sweeps);
+        max_sweeps = std::max(max_sweeps, (int)std::min<int64_t>(job_sweeps(jobs[j]), 1 << 30));
         max_xe = std::max(max_xe, jobs[j].exchange_every);
     }
     // a slice is a whole number of exchange blocks of every job

@@ -65,6 +65,10 @@ int prepare_job(const sqs_job& J, int j, JobDev& d, JobMut& m, Plan& p, const Sh
 int resolve_job(sqs_ctx* ctx, const sqs_job& job, int mode, sqs_job& eff, Shape& shape);
 // float4 elements of a job's state region: R*n replica squares + 2n quench scratch.
 int64_t job_pos_elems(const sqs_job& J);
+// Proposals per replica in a job's budget (sweeps * n, or -sweeps), and that
+// budget in whole sweeps, rounded up.
+int64_t job_props(const sqs_job& J);
+int64_t job_sweeps(const sqs_job& J);
 // Every replica starts from the job's initial state (angles wrapped to [0, pi/2)).
 void init_replicas(const sqs_job& J, float4* dst);
 void fill_result(const sqs_job& J, const JobDev& d, const JobMut& m, float dev_ms, sqs_job_result& o);

@@ -654,12 +654,18 @@ __device__ __forceinline__ long long kick_replica(const Rep& rep, const Grid& g,
     return E;
 }
 
-// Ladder temperature of rung k: geometric from tmin (k = 0) to tmax
-// (k = R - 1), the reference's ladder T_b = tmin (tmax / tmin)^(b / 7) for
-// R = 8 (seeded.cu:493-494).
+// Rungs per ladder (a job's R rungs form `ladders` ladders of RL rungs; rung
+// k is position k % RL of ladder k / RL, as the reference groups its chains
+// into ladders of 8, seeded.cu:493, 791-817).
+__device__ __forceinline__ int rungs_per_ladder(const JobDev& jd) { return jd.R / max(1, jd.ladders); }
+
+// Ladder temperature of rung k: geometric from tmin (position 0) to tmax
+// (position RL - 1), the reference's ladder T_b = tmin (tmax / tmin)^(b / 7)
+// for RL = 8 (seeded.cu:493-494).
 __device__ __forceinline__ float rung_temp(const JobDev& jd, int k) {
+    const int RL = rungs_per_ladder(jd), pos = k % RL;
     const float lt = logf(jd.tmin), lh = logf(jd.tmax);
-    return jd.R > 1 ? expf(lt + (lh - lt) * (float)k / (float)(jd.R - 1)) : jd.tmin;
+    return RL > 1 ? expf(lt + (lh - lt) * (float)pos / (float)(RL - 1)) : jd.tmin;
 }
 
 // Cooling factor of exchange round x under SQS_JOB_ADAPT: 0.002^((x mod 200)
@@ -668,12 +674,24 @@ __device__ __forceinline__ float cool_of(bool adaptive, int xround) {
     return adaptive ? powf(0.002f, (float)(xround % 200) / 199.f) : 1.f;
 }
 
-// Step scale of a replica on rung `rung` under SQS_JOB_ADAPT: adaptation
-// factor x (0.15 + 1.85 rung / (R - 1)) x sqrt(cool), the reference's
-// scale = adapt * baseMove * (.15 + 1.85 (b % 8) / 7) * sqrt(cool)
-// (seeded.cu:506), in units of the job's sigma.
-__device__ __forceinline__ float step_scale(float adapt, int rung, int R, float cool) {
-    return adapt * (R > 1 ? 0.15f + 1.85f * (float)rung / (float)(R - 1) : 1.f) * sqrtf(cool);
+// Step scale of a replica on rung k under SQS_JOB_ADAPT: adaptation factor x
+// (0.15 + 1.85 pos / (RL - 1)) x sqrt(cool), the reference's scale = adapt *
+// baseMove * (.15 + 1.85 (b % 8) / 7) * sqrt(cool) (seeded.cu:506), in units
+// of the job's sigma.
+__device__ __forceinline__ float step_scale(const JobDev& jd, float adapt, int k, float cool) {
+    const int RL = rungs_per_ladder(jd), pos = k % RL;
+    return adapt * (RL > 1 ? 0.15f + 1.85f * (float)pos / (float)(RL - 1) : 1.f) * sqrtf(cool);
+}
+
+// Container side of rung k when the job's side is B: B itself, or under
+// SQS_JOB_TARGETS the reference's target below the best,
+// max(sqrt n + 1e-6, B (1 - shrink m(pos))) (seeded.cu:478-481, with the
+// shrink relative to the side).
+__device__ __forceinline__ float rung_side(const JobDev& jd, float B, int k) {
+    if (!(jd.flags & kTargets)) return B;
+    const int RL = rungs_per_ladder(jd);
+    const float lb = sqrtf((float)jd.n) + 1e-6f;
+    return fmaxf(lb, B * (1.f - jd.shrink * target_mult(k % RL, RL)));
 }
 
 struct CtaShared {
@@ -683,9 +701,11 @@ struct CtaShared {
     long long wE[kMaxRl];      // this CTA's replica energies at a checkpoint
     double wL[kMaxRl];         // this CTA's candidate certified sides at a checkpoint
     double wlam[kMaxRl], wx0[kMaxRl], wy0[kMaxRl];
+    float wside[kMaxRl];       // each replica's container side (per rung under SQS_JOB_TARGETS)
     int wbad[kMaxRl];          // cell-list overflow per warp
     int decision_win;          // global replica index of the new best (-1: none)
     int bad;                   // any overflow in the cluster
+    int reset0;                // SQS_JOB_TARGETS: the gain resets every rung of ladder 0, not only heads
     float newL;
     unsigned long long props[kMaxRl], accs[kMaxRl];
     long long red[kMaxRl];
@@ -739,8 +759,11 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
     if (tid < R) S.temps[tid] = rung_temp(jd, tid);
     const int64_t rb = replica_smem_bytes(n, jd.Gmax);
     Rep rep = rep_view(dyn + (active ? w : 0) * rb, n, jd.Gmax);
-    float L = S.jm.L;
+    float L = S.jm.L;  // the job's side: every replica's, or under SQS_JOB_TARGETS the best the rung sides hang from
     Grid g = make_grid(L, jd.Gmax, jd.cell);
+    // this replica's side (walls, move clamps, kicks, quench)
+    float Lr = active ? rung_side(jd, L, S.jm.perm[r]) : L;
+    if (active && lane == 0) S.wside[w] = Lr;
     const uint32_t k0 = (uint32_t)jd.seed, k1 = (uint32_t)(jd.seed >> 32);
 
     // load the replica
@@ -774,7 +797,7 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
     }
     long long E = 0;
     if (active) {
-        E = S.jm.sweep == 0 ? full_energy(rep, n, g, L, lane) : S.jm.E[r];
+        E = S.jm.done == 0 ? full_energy(rep, n, g, Lr, lane) : S.jm.E[r];
     }
     unsigned long long props = 0, accs = 0;
     int ovf = 0;
@@ -787,19 +810,26 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
     float invT = active ? 1.0f / (S.temps[S.jm.perm[r]] * cool) : 0.f;
     float4* save = pos + jd.pos_off + (int64_t)r * n;  // this replica's HBM slot: free while the slice runs
 
-    const int sweep0 = S.jm.sweep;
-    const int sweep_end = min(jd.sweeps_total, sweep0 + (jd.slice > 0 ? jd.slice : slice_sweeps));
-    for (int sweep = sweep0; sweep < sweep_end; ++sweep) {
+    // Proposals are numbered per replica across the whole job (a sweep is n
+    // of them); checkpoints fall after every xprops proposals and at the end
+    // of the budget; a slice ends after its sweeps' worth of proposals.
+    const int64_t P_total = jd.props_total, xp = jd.xprops;
+    int64_t p_at = S.jm.done;
+    const int64_t p_end = min(P_total, p_at + (int64_t)(jd.slice > 0 ? jd.slice : slice_sweeps) * n);
+    while (p_at < p_end) {
+        const int64_t next_cp = min(P_total, (p_at / xp + 1) * xp);
+        const int64_t stop = min(next_cp, p_end);
         if (active) {
-            for (int kb = 0; kb < n; kb += 32) {
-                // Lane l draws proposal kb + l of this sweep: two Philox blocks
-                // keyed by (sweep * n + k, replica, 0 / 1), Box-Muller for the
-                // centre step and the angle step, the uniform of the
-                // Metropolis test.  Each proposal then broadcasts its draws.
+            for (int64_t base = p_at; base < stop; base += 32) {
+                // Lane l draws proposal base + l: two Philox blocks keyed by
+                // (proposal index, replica, 0 / 1), Box-Muller for the centre
+                // step and the angle step, the uniform of the Metropolis test.
+                // Each proposal then broadcasts its draws.
+                const int kn = (int)(stop - base < 32 ? stop - base : 32);
                 int di = 0;
                 float ddx = 0.f, ddy = 0.f, dda = 0.f, du = 0.f;
-                if (kb + lane < n) {
-                    const uint64_t ev = (uint64_t)sweep * (uint64_t)n + (uint64_t)(kb + lane);
+                if (lane < kn) {
+                    const uint64_t ev = (uint64_t)(base + lane);
                     const U4 ra = philox4x32_10(U4{(uint32_t)ev, (uint32_t)(ev >> 32), (uint32_t)r, 0u}, k0, k1);
                     const U4 rb = philox4x32_10(U4{(uint32_t)ev, (uint32_t)(ev >> 32), (uint32_t)r, 1u}, k0, k1);
                     di = (int)(((uint64_t)ra.x * (uint64_t)n) >> 32);
@@ -814,7 +844,6 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                     du = u01(rb.y);
                     if (MOVES && (jd.flags & kMoveCollective)) di |= (int)(rb.z % 7u) << 16;  // move mode
                 }
-                const int kn = min(32, n - kb);
                 // one lane moves square i to its new state and cell
                 auto apply_move = [&](int i, float nx, float ny, float nc, float ns, float na, int oc, int ncell) {
                     rep.sq[i] = make_float4(nx, ny, nc, ns);
@@ -841,26 +870,25 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                     const float sdx = __shfl_sync(0xffffffffu, ddx, q), sdy = __shfl_sync(0xffffffffu, ddy, q);
                     const float sda = __shfl_sync(0xffffffffu, dda, q), u_acc = __shfl_sync(0xffffffffu, du, q);
                     float sc = 1.f;  // step scale (adaptive moves)
-                    const int pidx = kb + q;
+                    const uint64_t pidx = (uint64_t)(base + q);
                     if (adaptive) {
-                        const int rung = S.jm.perm[r];
-                        sc = step_scale(adapt, rung, R, cool);
-                        if ((((uint64_t)sweep * (uint64_t)n + (uint64_t)pidx) & 15u) == 0) sc *= 3.5f;
+                        sc = step_scale(jd, adapt, S.jm.perm[r], cool);
+                        if ((pidx & 15u) == 0) sc *= 3.5f;
                     }
                     const float dx = fminf(kMaxStep, fmaxf(-kMaxStep, sdx * sc));
                     const float dy = fminf(kMaxStep, fmaxf(-kMaxStep, sdy * sc));
                     const float da = sda * sc;
                     bool acc;
                     if (MOVES && mode != 0) {
-                        acc = collective_move(rep, g, n, L, lane, mode, i, dx, dy, da, u_acc, invT, E, save, &ovf);
+                        acc = collective_move(rep, g, n, Lr, lane, mode, i, dx, dy, da, u_acc, invT, E, save, &ovf);
                         ++props;
                         accs += acc;
                     } else {
                     const float4 P = rep.sq[i];
-                    // keep centres in [0.5, L - 0.5] without ever moving a square
+                    // keep centres in [0.5, Lr - 0.5] without ever moving a square
                     // further than the clamped step (it may start outside)
-                    const float nx = fminf(fmaxf(P.x, L - 0.5f), fmaxf(fminf(P.x, 0.5f), P.x + dx));
-                    const float ny = fminf(fmaxf(P.y, L - 0.5f), fmaxf(fminf(P.y, 0.5f), P.y + dy));
+                    const float nx = fminf(fmaxf(P.x, Lr - 0.5f), fmaxf(fminf(P.x, 0.5f), P.x + dx));
+                    const float ny = fminf(fmaxf(P.y, Lr - 0.5f), fmaxf(fminf(P.y, 0.5f), P.y + dy));
                     float na = rep.ang[i] + da;
                     na = na - kHalfPiF * floorf(na * (1.0f / kHalfPiF));
                     if (!(na >= 0.f && na < kHalfPiF)) na = 0.f;
@@ -868,7 +896,7 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                     state_trig(na, &ns, &nc);
                     const int ocx = g.cx(P.x), ocy = g.cx(P.y);
                     long long dq = 0;
-                    if (lane == 0) dq = qe(wall_e(nx, ny, nc, ns, L)) - qe(wall_e(P.x, P.y, P.z, P.w, L));
+                    if (lane == 0) dq = qe(wall_e(nx, ny, nc, ns, Lr)) - qe(wall_e(P.x, P.y, P.z, P.w, Lr));
                     for_block(rep, g, ocx, ocy, lane, [&](int j) {
                         const long long d = pair_delta(rep.sq[j], nx, ny, nc, ns, P);
                         dq += j != i ? d : 0;
@@ -892,7 +920,7 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                     }
                     if (adaptive) {  // every 16 proposals: steer toward 25% acceptance
                         win += acc;
-                        if ((((uint64_t)sweep * (uint64_t)n + (uint64_t)pidx + 1u) & 15u) == 0) {
+                        if (((pidx + 1u) & 15u) == 0) {
                             adapt = fmaxf(0.1f, fminf(4.0f, adapt * expf(((float)win / 16.f - 0.25f) * 0.5f)));
                             win = 0;
                         }
@@ -922,8 +950,8 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                     const float dx = fminf(kMaxStep, fmaxf(-kMaxStep, sdx));
                     const float dy = fminf(kMaxStep, fmaxf(-kMaxStep, sdy));
                     const float4 P = rep.sq[i];
-                    const float nx = fminf(fmaxf(P.x, L - 0.5f), fmaxf(fminf(P.x, 0.5f), P.x + dx));
-                    const float ny = fminf(fmaxf(P.y, L - 0.5f), fmaxf(fminf(P.y, 0.5f), P.y + dy));
+                    const float nx = fminf(fmaxf(P.x, Lr - 0.5f), fmaxf(fminf(P.x, 0.5f), P.x + dx));
+                    const float ny = fminf(fmaxf(P.y, Lr - 0.5f), fmaxf(fminf(P.y, 0.5f), P.y + dy));
                     float na = rep.ang[i] + sda;
                     na = na - kHalfPiF * floorf(na * (1.0f / kHalfPiF));
                     if (!(na >= 0.f && na < kHalfPiF)) na = 0.f;
@@ -931,7 +959,7 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                     state_trig(na, &ns, &nc);
                     const int ocx = g.cx(P.x), ocy = g.cx(P.y);
                     long long dq = 0;
-                    if (gl == 0) dq = qe(wall_e(nx, ny, nc, ns, L)) - qe(wall_e(P.x, P.y, P.z, P.w, L));
+                    if (gl == 0) dq = qe(wall_e(nx, ny, nc, ns, Lr)) - qe(wall_e(P.x, P.y, P.z, P.w, Lr));
                     for_block<W>(rep, g, ocx, ocy, gl, [&](int j) {
                         const long long d = pair_delta(rep.sq[j], nx, ny, nc, ns, P);
                         dq += j != i ? d : 0;
@@ -1001,11 +1029,12 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                 }
             }
         }
-        // ---- checkpoint: best-state search, shrink, replica exchange.  Only at
-        // multiples of exchange_every (and at the end of the budget), so a
+        p_at = stop;
+        // ---- checkpoint: best-state search, shrink, replica exchange.  Only
+        // after every xprops proposals (and at the end of the budget), so a
         // job's trajectory does not depend on how it is sliced.
-        const bool xpoint = (sweep + 1) % jd.exchange_every == 0;
-        if (!xpoint && sweep + 1 != jd.sweeps_total) continue;
+        if (p_at != next_cp) break;  // the slice ends between checkpoints
+        const bool xpoint = p_at % xp == 0;
         // the replica on the coldest rung (every replica under
         // SQS_JOB_QUENCH_ALL) is quenched toward zero overlap by every thread
         // of the CTA that holds it
@@ -1018,7 +1047,8 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                 float4* qs = (int64_t)dyn_bytes >= (int64_t)Rl * rb + 32 * (int64_t)n
                                  ? reinterpret_cast<float4*>(dyn + (int64_t)Rl * rb)
                                  : pos + jd.scr_off;
-                const long long qe_out = quench_cta(cr, n, g, L, jd.quench_iters, jd.quench_stall, qs, qs + n, S.qE, S.red);
+                const long long qe_out =
+                    quench_cta(cr, n, g, S.wside[lr], jd.quench_iters, jd.quench_stall, qs, qs + n, S.qE, S.red);
                 if (w == lr) E = qe_out;
                 __syncthreads();
             }
@@ -1035,7 +1065,8 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                 float4* qs = (int64_t)dyn_bytes >= (int64_t)Rl * rb + 32 * (int64_t)n
                                  ? reinterpret_cast<float4*>(dyn + (int64_t)Rl * rb)
                                  : pos + jd.scr_off;
-                const long long qe_out = quench_cta(cr, n, g, L, jd.quench_iters, jd.quench_stall, qs, qs + n, S.qE, S.red);
+                const long long qe_out = quench_cta(cr, n, g, S.wside[cold % Rl], jd.quench_iters, jd.quench_stall, qs,
+                                                    qs + n, S.qE, S.red);
                 if (w == cold % Rl) E = qe_out;
                 __syncthreads();
             }
@@ -1075,23 +1106,36 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
             }
             S.decision_win = win;
             S.newL = L;
+            S.reset0 = 0;
+            const bool targets = (jd.flags & kTargets) != 0;
             if (win >= 0) {
+                const double gain = S.jm.best_L < 1e29 ? S.jm.best_L - bestc : 0.0;
                 S.jm.best_L = bestc;
                 S.jm.improvements += 1;
-                float nl = (float)(fmin((double)L, bestc) * (1.0 - (double)jd.shrink));
                 const float lb = sqrtf((float)n) + 1e-6f;
+                // the job's side: the new best (the rung targets hang below it), or
+                // the best shrunk by the job's factor
+                float nl = targets ? (float)fmin((double)L, bestc)
+                                   : (float)(fmin((double)L, bestc) * (1.0 - (double)jd.shrink));
                 if (nl < lb) nl = lb;
                 if (nl < L) {
                     S.newL = nl;
                     S.jm.shrinks += 1;
                 }
+                // a large gain resets every rung of ladder 0 to the new best (seeded.cu:929)
+                S.reset0 = targets && gain > 5e-4;
             }
-            // replica exchange between neighbouring rungs, alternating parity
-            if (xpoint) {
+            // replica exchange between neighbouring rungs of each ladder, alternating
+            // parity; under SQS_JOB_TARGETS only in rounds without a new best, as the
+            // reference swaps only in epochs that did not improve (seeded.cu:939-941)
+            if (xpoint && !(targets && win >= 0)) {
                 int holder[kMaxR];
                 for (int q = 0; q < R; ++q) holder[S.jm.perm[q]] = q;
                 const int par = S.jm.xround & 1;
-                for (int k = par; k + 1 < R; k += 2) {
+                const int RL = rungs_per_ladder(jd);
+                for (int k = 0; k + 1 < R; ++k) {
+                    const int pos = k % RL;
+                    if ((pos & 1) != par || pos + 1 >= RL) continue;
                     const int a = holder[k], b = holder[k + 1];
                     const U4 u = philox4x32_10(U4{(uint32_t)S.jm.xround, (uint32_t)k, 0u, 0x7fffffffu}, k0, k1);
                     const float d = (1.0f / S.temps[k] - 1.0f / S.temps[k + 1]) *
@@ -1105,12 +1149,13 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                         holder[k + 1] = a;
                     }
                 }
-                S.jm.xround += 1;
             }
+            if (xpoint) S.jm.xround += 1;
         }
         cluster.sync();
         __syncthreads();
         if (adaptive) cool = cool_of(true, S.jm.xround);
+        const bool targets = MOVES && (jd.flags & kTargets) != 0;
         if (active) {
             invT = 1.0f / (S.temps[S.jm.perm[r]] * cool);
             if (S.decision_win == r) {
@@ -1124,40 +1169,73 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                 }
             }
         }
-        if (S.newL < L) {
-            const float f = S.newL / L;
-            L = S.newL;
-            g = make_grid(L, jd.Gmax, jd.cell);
-            if (active) {
-                for (int i = lane; i < n; i += 32) {
-                    rep.sq[i].x *= f;
-                    rep.sq[i].y *= f;
-                }
-                __syncwarp();
-                const bool ok = build_cells(rep, n, g, lane);
-                if (lane == 0) S.wbad[w] = !ok;
-                E = full_energy(rep, n, g, L, lane);
-            }
+        if (targets && S.decision_win >= 0) {  // the new best is read by the ladder heads below
+            __threadfence();
             __syncthreads();
             cluster.sync();
-            if (tid == 0) {
-                int bad = 0;
-                for (int q = 0; q < (int)cluster.num_blocks(); ++q) {
-                    const CtaShared* o = cluster.map_shared_rank(&S, q);
-                    for (int k = 0; k < Rl; ++k) bad |= o->wbad[k];
+        }
+        const bool regrid = S.newL < L;
+        if (regrid || targets) {
+            const float f = S.newL / L;
+            if (regrid) {
+                L = S.newL;
+                g = make_grid(L, jd.Gmax, jd.cell);
+            }
+            if (active) {
+                const int rung = S.jm.perm[r];
+                const float Ln = rung_side(jd, L, rung);
+                const int RL = rungs_per_ladder(jd);
+                const bool reset = targets && S.decision_win >= 0 && (rung % RL == 0 || (S.reset0 && rung < RL));
+                if (reset) {
+                    // ladder head: the new best, scaled into its own side (seeded.cu:928-936)
+                    const double* src = best + jd.best_off;
+                    const double sc = (double)Ln / (double)L;
+                    for (int i = lane; i < n; i += 32) {
+                        const float a = (float)src[3 * i + 2];
+                        float sn, cs;
+                        state_trig(a, &sn, &cs);
+                        rep.sq[i] = make_float4((float)(src[3 * i] * sc), (float)(src[3 * i + 1] * sc), cs, sn);
+                        rep.ang[i] = a;
+                    }
+                } else if (regrid && !targets) {
+                    for (int i = lane; i < n; i += 32) {
+                        rep.sq[i].x *= f;
+                        rep.sq[i].y *= f;
+                    }
                 }
-                S.bad = bad;
+                __syncwarp();
+                if (reset || regrid) {
+                    const bool ok = build_cells(rep, n, g, lane);
+                    if (lane == 0) S.wbad[w] = !ok;
+                }
+                const bool changed = reset || regrid || Ln != Lr;
+                Lr = Ln;
+                if (lane == 0) S.wside[w] = Lr;
+                if (changed) E = full_energy(rep, n, g, Lr, lane);
             }
-            cluster.sync();
-            if (S.bad) {
-                if (rank == 0 && tid == 0) jmut[job].status = kErrCells;
-                return;
+            if (regrid || (targets && S.decision_win >= 0)) {
+                __syncthreads();
+                cluster.sync();
+                if (tid == 0) {
+                    int bad = 0;
+                    for (int q = 0; q < (int)cluster.num_blocks(); ++q) {
+                        const CtaShared* o = cluster.map_shared_rank(&S, q);
+                        for (int k = 0; k < Rl; ++k) bad |= o->wbad[k];
+                    }
+                    S.bad = bad;
+                }
+                cluster.sync();
+                if (S.bad) {
+                    if (rank == 0 && tid == 0) jmut[job].status = kErrCells;
+                    return;
+                }
             }
+            __syncthreads();
         }
         // overlapped replicas are kicked (the round just completed decides
         // whether the worst square is also moved)
         if (MOVES && active && (jd.flags & kMoveKick) && E > qe(1e-12f))
-            E = kick_replica(rep, g, n, L, lane, r, S.jm.xround, k0, k1, E, save);
+            E = kick_replica(rep, g, n, Lr, lane, r, S.jm.xround, k0, k1, E, save);
     }
 
     // ---- write the slice back
@@ -1178,9 +1256,9 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
     if (rank == 0 && tid == 0) {
         JobMut& m = jmut[job];
         m.L = L;
-        m.sweep = sweep_end;
+        m.done = p_end;
         m.xround = S.jm.xround;
-        m.status = sweep_end >= jd.sweeps_total ? kFinished : kRunning;
+        m.status = p_end >= P_total ? kFinished : kRunning;
         m.shrinks = S.jm.shrinks;
         m.improvements = S.jm.improvements;
         m.best_L = S.jm.best_L;
@@ -1206,8 +1284,8 @@ __global__ void __launch_bounds__(32) trace_kernel(const int2* __restrict__ item
     const JobMut& jm = jmut[it.x];
     const int n = jd.n, r = it.y, lane = threadIdx.x;
     const Rep rep = rep_view(dyn, n, jd.Gmax);
-    const float L = jm.L;
-    const Grid g = make_grid(L, jd.Gmax, jd.cell);
+    const Grid g = make_grid(jm.L, jd.Gmax, jd.cell);
+    const float L = rung_side(jd, jm.L, jm.perm[r]);
     const float4* src = pos + jd.pos_off + (int64_t)r * n;
     for (int i = lane; i < n; i += 32) {
         const float4 p = src[i];
@@ -1230,7 +1308,7 @@ __global__ void __launch_bounds__(32) trace_kernel(const int2* __restrict__ item
         t.L_cert = Lc;
         t.lam = lam;
         t.temp = rung_temp(jd, rung) * cool;
-        t.step = adaptive ? step_scale(jm.adapt[r], rung, jd.R, cool) : 1.f;
+        t.step = adaptive ? step_scale(jd, jm.adapt[r], rung, cool) : 1.f;
         t.side = L;
         t.rung = rung;
         t.cells_ok = ok ? 1 : 0;

@@ -96,14 +96,20 @@ __device__ __forceinline__ bool sat_pair_grad(float dx, float dy, float cp, floa
     return true;
 }
 
-// Energy only (no gradient): gap^2 or 0.  Same axis model.
+// Energy only (no gradient): gap^2 or 0.  Same axis model.  Every rounding
+// is spelled out so that the value is the same bit for bit when the two
+// squares swap roles (offset negated, p's and q's cos/sin exchanged): the
+// annealer adds a moved square's pair terms from its own side and takes the
+// total from the lower index's, and the two must agree exactly.
 __device__ __forceinline__ float sat_pair_energy(float dx, float dy, float cp, float sp, float cq,
                                                  float sq) {
     const float cd = __fadd_rn(__fmul_rn(cp, cq), __fmul_rn(sp, sq));
     const float sd = __fsub_rn(__fmul_rn(sp, cq), __fmul_rn(cp, sq));
     const float rad = 0.5f + 0.5f * (fabsf(cd) + fabsf(sd));
-    const float z0 = fabsf(dx * cp + dy * sp), z1 = fabsf(dy * cp - dx * sp);
-    const float z2 = fabsf(dx * cq + dy * sq), z3 = fabsf(dy * cq - dx * sq);
+    const float z0 = fabsf(__fmaf_rn(dx, cp, __fmul_rn(dy, sp)));
+    const float z1 = fabsf(__fmaf_rn(dy, cp, -__fmul_rn(dx, sp)));
+    const float z2 = fabsf(__fmaf_rn(dx, cq, __fmul_rn(dy, sq)));
+    const float z3 = fabsf(__fmaf_rn(dy, cq, -__fmul_rn(dx, sq)));
     const float gap = fmaxf(fmaxf(z0, z1), fmaxf(z2, z3)) - rad;
     return gap < 0.f ? gap * gap : 0.f;
 }

@@ -219,7 +219,7 @@ int admit(sqs_server* s) {
         j.jd.scr_off = j.jd.pos_off + (int64_t)j.job.replicas * j.job.n;
         j.jd.best_off = (int64_t)((off + sizeof(float4) * (size_t)job_pos_elems(j.job)) / sizeof(double));
         if (s->slice < 0) {  // this job's sweeps per step: about -slice proposals, whole exchange intervals
-            const int xe = j.jd.exchange_every;
+            const int xe = std::max(1, j.jd.exchange_every);
             const int64_t sw = std::max<int64_t>(1, (-(int64_t)s->slice + j.job.n - 1) / j.job.n);
             j.jd.slice = (int)std::min<int64_t>((sw + xe - 1) / xe * xe, 1 << 30);
         }
@@ -381,7 +381,7 @@ extern "C" int sqs_server_submit(sqs_server* s, const sqs_job* job, int64_t* id)
         j.job.xya_rep = j.xya_rep.data();
     }
     if (int r = prepare_job(j.job, 0, j.jd, j.jm, j.plan, &shape)) return r;
-    j.left = j.job.sweeps;
+    j.left = job_sweeps(j.job);
     SQS_REQUIRE(job_bytes(j.job) <= s->arena_bytes, "job state (%zu bytes) exceeds the server's HBM budget",
                 job_bytes(j.job));
     *id = j.id;

@@ -90,6 +90,7 @@ JOB_KICK = 8
 JOB_SERIAL = 16
 JOB_QUENCH_ALL = 32
 JOB_CERT_ALL = 64
+JOB_TARGETS = 128
 TUNE_LATENCY = 1
 
 

@@ -26,8 +26,8 @@ class AnnealJob:
     xya: np.ndarray                 # (n, 3) initial state: centre x, centre y, angle (radians)
     L0: float                       # initial container side
     replicas: int = 8
-    sweeps: int = 1000              # one sweep = n proposals per replica
-    exchange_every: int = 10
+    sweeps: int = 1000              # one sweep = n proposals per replica; negative: -sweeps proposals
+    exchange_every: int = 10        # sweeps between checkpoints; negative: -exchange_every proposals
     tmin: float = 1e-3
     tmax: float = 1e-1
     sigma_xy: float = 0.02
@@ -43,6 +43,8 @@ class AnnealJob:
     quench_all: bool = False        # quench every replica at exchange rounds (SQS_JOB_QUENCH_ALL)
     cert_all: bool = False          # dilation-certify every replica at checkpoints (SQS_JOB_CERT_ALL)
     quench_steps: int = 0           # 1..127: 16 k-iteration quenches without a slow-step exit (SQS_JOB_QUENCH_STEPS)
+    targets: bool = False           # every rung in its own side below the best (SQS_JOB_TARGETS)
+    ladders: int = 1                # rungs split into this many ladders (SQS_JOB_LADDERS)
     cluster: int = 0                # pinned cluster size (0: default / tuned)
     cell_index: int = 0             # pinned cell side index (0: 1.59, 1: 1.75, 2: 1.95, 3: 2.2)
     xya_rep: np.ndarray | None = None  # (replicas, n, 3) per-replica starts, e.g. from portfolio()
@@ -53,6 +55,8 @@ class AnnealJob:
         self.n = self.xya.shape[0]
         if not 0 <= self.quench_steps <= 127:
             raise ValueError("quench_steps must be in 0..127")
+        if not 1 <= self.ladders <= 15:
+            raise ValueError("ladders must be in 1..15")
         if self.xya_rep is not None:
             self.xya_rep = np.ascontiguousarray(self.xya_rep, dtype=np.float64).reshape(self.replicas, self.n, 3)
 
@@ -61,7 +65,8 @@ def _flags(j: AnnealJob) -> int:
     return ((N.JOB_AUTOTUNE if j.autotune else 0) | (N.JOB_ADAPT if j.adapt else 0) |
             (N.JOB_COLLECTIVE if j.collective else 0) | (N.JOB_KICK if j.kick else 0) |
             (N.JOB_SERIAL if j.serial else 0) | (N.JOB_QUENCH_ALL if j.quench_all else 0) |
-            (N.JOB_CERT_ALL if j.cert_all else 0) | (j.quench_steps << 24) |
+            (N.JOB_CERT_ALL if j.cert_all else 0) | (N.JOB_TARGETS if j.targets else 0) |
+            ((j.ladders if j.ladders > 1 else 0) << 20) | (j.quench_steps << 24) |
             (j.cluster << 8) | (j.cell_index << 16))
 
 

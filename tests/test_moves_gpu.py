@@ -7,6 +7,7 @@ certified packing, changes the trajectory, and keeps a job's result
 independent of batching, slicing and launch shape."""
 from __future__ import annotations
 
+import math
 from dataclasses import replace
 
 import pytest
@@ -118,3 +119,66 @@ def test_replicas_start_from_a_portfolio(ctx):
     for k in KEYS:
         assert sliced[k] == alone[k], ("sliced", k)
         assert served[k] == alone[k], ("served", k)
+
+
+def test_proposal_counted_budgets_equal_sweep_counted_ones(ctx):
+    """A budget of -k n proposals and checkpoints every -n proposals are the
+    same job as k sweeps with a checkpoint every sweep, bit for bit; a
+    checkpoint between sweeps (every 7 proposals) runs and differs."""
+    from sqs.anneal import anneal_batch
+    n = 30
+    a = _job(n=n, sweeps=60, exchange_every=1, replicas=8)
+    b = replace(a, sweeps=-60 * n, exchange_every=-n)
+    c = replace(a, sweeps=-60 * n, exchange_every=-7)
+    ra, rb, rc = anneal_batch([a, b, c], ctx=ctx)
+    for k in KEYS:
+        assert ra[k] == rb[k], k
+    assert ra["sweeps"] == rb["sweeps"] == 60
+    assert rc["status"] == 0 and rc["proposals"] == 8 * 60 * n
+    assert rc["exchange_attempts"] > 4 * ra["exchange_attempts"]
+
+
+def _target_job(**kw):
+    args = dict(n=48, sweeps=-48 * 60, exchange_every=-24, replicas=16, tmin=1e-11, tmax=1e-4, shrink=0.001 / 7,
+                polish_iters=100, targets=True, ladders=2, adapt=True, kick=True, quench_all=True, cert_all=True,
+                quench_steps=4)
+    args.update(kw)
+    return _job(**args)
+
+
+def test_target_ladders_follow_the_reference_offsets(ctx, oracle):
+    """Under SQS_JOB_TARGETS every rung anneals in side max(sqrt n, B (1 -
+    shrink m)) below the best side B with the reference's offsets m; ladders
+    repeat the temperatures of their rungs; the job certifies a packing."""
+    from sqs.anneal import anneal_batch
+    job = _target_job()
+    r = anneal_batch([job], ctx=ctx, trace=True)[0]
+    assert r["status"] == 0, r["reason"]
+    assert r["certified"], r["reason"]
+    ok, L, reason, _ = oracle.certify(job.n, r["rows"])
+    assert ok and L == r["L"], reason
+    t = r["trace"]
+    mults = [0.02, 0.1, 0.4, 1.0, 2.5, 5.0, 10.0, 20.0]
+    B = max(t["side"]) / (1 - job.shrink * 0.02)
+    for rep in range(job.replicas):
+        k = int(t["rung"][rep])
+        want = max(math.sqrt(job.n) + 1e-6, B * (1 - job.shrink * mults[k % 8]))
+        assert t["side"][rep] == pytest.approx(want, rel=1e-5)
+    temp = {int(k): float(T) for k, T in zip(t["rung"], t["temperature"])}
+    for k in range(8):
+        assert temp[k] == temp[k + 8]
+    assert r["shrinks"] >= 1
+    assert B <= job.L0 + 1e-6
+
+
+def test_target_ladders_are_reproducible(ctx):
+    from sqs.anneal import anneal_batch
+    job = _target_job()
+    alone = anneal_batch([job], ctx=ctx)[0]
+    mixed = anneal_batch([_job(n=25, seed=2), job, _target_job(n=60, seed=5)], ctx=ctx)[1]
+    sliced = anneal_batch([job], ctx=ctx, slice_sweeps=7)[0]
+    wide = anneal_batch([replace(job, cluster=4)], ctx=ctx)[0]
+    for k in KEYS:
+        assert mixed[k] == alone[k], ("mixed", k)
+        assert sliced[k] == alone[k], ("sliced", k)
+        assert wide[k] == alone[k], ("cluster 4", k)
