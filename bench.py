@@ -148,6 +148,17 @@ def peaks() -> tuple[float, str]:
     return FALLBACK_HBM_GBS, "fallback"
 
 
+def ncu_metric(kernel: str, key: str) -> float | None:
+    """A figure of `kernel` from the committed ncu summary (profiles/traffic.json)."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    try:
+        return float(json.loads(p.read_text())[kernel][key])
+    except (KeyError, ValueError, TypeError):
+        return None
+
+
 def ncu_traffic(kernel: str) -> float | None:
     """DRAM bytes per launch of `kernel` from the committed ncu summary."""
     p = ROOT / "profiles" / "traffic.json"
@@ -223,6 +234,68 @@ def accuracy(d_e, d_g, x32, s32, configs: int = 64) -> dict:
     rel = np.abs(e - eo) / np.maximum(np.abs(eo), 1e-30)
     return dict(configs=configs, max_rel_energy_error=float(rel.max()), mean_rel_energy_error=float(rel.mean()),
                 max_abs_grad_error=float(np.abs(g - go).max()), vs="FP64 all-pairs oracle on the same FP32 inputs")
+
+
+def anneal_accuracy(ctx) -> dict:
+    """FP32 annealer energies against the FP64 oracle, per configuration.
+
+    Every replica's final FP32 state is read back with the annealer's running
+    fixed-point energy (sqs_anneal_batch_trace); the oracle's FP64 all-pairs
+    total of the same state and side is the reference.  Reports, per
+    configuration, the largest relative and absolute error and whether every
+    running energy equals its from-scratch recompute bit for bit."""
+    import numpy as np
+
+    sys.path.insert(0, str(ROOT / "oracle"))
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle as O
+
+    from sqs.anneal import AnnealJob, anneal_batch, jittered_grid
+
+    def plain():
+        xya, L0 = jittered_grid(10, seed=42)
+        return [AnnealJob(xya, L0=L0, replicas=8, sweeps=20000, exchange_every=10, tmin=1e-3, tmax=1e-1, seed=42,
+                          polish_iters=0)]
+
+    def batched():
+        rng = np.random.default_rng(42)
+        out = []
+        for k in range(32):
+            n = int(rng.integers(20, 401))
+            xya, L0 = jittered_grid(n, seed=k)
+            out.append(AnnealJob(xya, L0=L0, replicas=32, sweeps=200, exchange_every=10, tmin=1e-4, tmax=5e-2,
+                                 seed=k, polish_iters=0))
+        return out
+
+    def served():
+        out = []
+        for k, job in enumerate(served_jobs(12, sweeps=100)):
+            job.polish_iters = 0
+            out.append(job)
+        return out
+
+    res = {}
+    for name, make, what in (("plain_pt", plain, "n=10, 8 replicas, 20,000 sweeps (all replicas)"),
+                             ("batched", batched, "32 of the batched instances (n U[20,400], 32 replicas), "
+                                                  "200 sweeps"),
+                             ("served", served, "12 jobs of the served stream (n log-uniform [5,1000], "
+                                                "16-64 replicas), 100 sweeps")):
+        jobs = make()
+        out = anneal_batch(jobs, ctx=ctx, trace=True)
+        rel, ab, exact, reps = 0.0, 0.0, True, 0
+        for r in out:
+            t = r["trace"]
+            eo, _, _ = O.total_batch(t["xya"].astype(np.float64), t["side"].astype(np.float64), grad=False)
+            d = np.abs(t["energy"] - eo)
+            ab = max(ab, float(d.max()))
+            rel = max(rel, float((d / np.maximum(eo, 1e-30)).max()))
+            exact &= bool(np.array_equal(t["energy"], t["energy_full"]))
+            reps += len(d)
+        res[name] = dict(workload=what, replicas=reps, max_rel_energy_error=rel, max_abs_energy_error=ab,
+                         running_equals_recompute=exact,
+                         tolerance="1e-5 relative, 1e-5 absolute floor (reference globaltest.cu:49)")
+    res["vs"] = "FP64 all-pairs oracle on the same FP32 states and sides"
+    return res
 
 
 def run_reference(args, D: Dist):
@@ -321,6 +394,11 @@ def run_sqs(args, D: Dist):
     kernel_name = "sat_energy_warp_kernel" if (threads <= 0 and n <= 256) else "sat_energy_kernel"
     algo = algorithmic_bytes(configs, n)
     achieved = algo / (mean_ms / 1e3) / 1e9
+    # FP32 work: 55 flop per candidate pair (energy + gradient), against the
+    # nominal FP32 peak at the sampled SM clock (148 SMs x 128 lanes x 2)
+    sm_mhz = (clk or {}).get("sm_mhz") or 1965.0
+    fp32_peak = sms * 128 * 2 * sm_mhz * 1e6 / 1e12
+    fp32_achieved = pairs_per_step * 55 / (mean_ms / 1e3) / 1e12
     line = dict(
         metric=METRIC, value=value, unit=UNIT, n_gpus=D.world, steps=K, warmup=args.warmup,
         ms_per_step=ms_per_step, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
@@ -333,9 +411,16 @@ def run_sqs(args, D: Dist):
                     parallelism=f"replicas x{D.world}", device=name, sm_count=sms),
         e2e=dict(value=e2e_val, unit=UNIT, h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h,
                  steps=e2e_steps, call="sqs_sat_energy_host (pinned host buffers)"),
-        roofline=dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
+        roofline=dict(bound="issue", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
                       traffic=ncu_traffic(kernel_name), peak_kind=peak_kind,
-                      algorithmic_bytes_per_launch=algo, kernel=kernel_name),
+                      algorithmic_bytes_per_launch=algo, kernel=kernel_name,
+                      limiter="issue slots: the kernel issues instructions most cycles while DRAM and the FP32 "
+                              "pipe are far from their peaks (ncu summary in profiles/)",
+                      issue_active_frac=ncu_metric(kernel_name, "issue_active_frac"),
+                      hbm=dict(achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak),
+                      fp32=dict(achieved=fp32_achieved, peak=fp32_peak, unit="TFLOP/s",
+                                frac=fp32_achieved / fp32_peak, peak_kind="nominal at the sampled SM clock",
+                                flop_per_candidate_pair=55)),
         gpu_launches=launches,
         pairs_per_step=pairs_per_step,
         all_pairs_equivalent_per_s=all_pairs_per_s,
@@ -343,6 +428,8 @@ def run_sqs(args, D: Dist):
     )
     if D.rank == 0:
         line["accuracy"] = accuracy(d_e, d_g, x32, s32)
+        if not args.no_extras:
+            line["anneal_accuracy"] = anneal_accuracy(ctx)
     if D.rank == 0 and D.world == 1 and not args.no_cpu_baseline:
         val, kind, cores, sample, _, _ = cpu_pairs_per_s(x32, s32, args.cpu_seconds)
         line["cpu_baseline"] = dict(value=val, unit=UNIT, cores=cores, kind=kind, sample=sample)

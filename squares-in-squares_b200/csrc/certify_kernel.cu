@@ -11,9 +11,12 @@
 //             sin/cos (:793-854), float corners + padded AABBs, bitonic sort
 //             of the AABBs, sort-and-sweep with the float SAT prefilter
 //             (:856-883); undecided pairs go to a global list;
-//   kernels cert_stage_kernel<7>, <15>, <58>: interval SAT of the undecided
-//           pairs at 63, 135 and 522 decimal digits (:885-899), each stage
-//           taking the pairs the previous one left open;
+//   kernel  cert_fp64_kernel: directed-rounding FP64 interval SAT of the
+//           undecided pairs, deciding those whose sign it certifies (and
+//           exact axis-aligned dyadic pairs) the way the stages below would;
+//   kernels the 7-, 15- and 58-limb interval SAT of the pairs still open at
+//           63, 135 and 522 decimal digits (:885-899), each stage taking the
+//           pairs the previous one left open;
 //   host    reason strings, area bound, score, 50-decimal side (:900-911).
 // The kernel file is compiled without multiply-add contraction so its double
 // arithmetic rounds exactly like the reference's host code.
@@ -63,6 +66,7 @@ struct Pair {
 
 struct Consts {
     Fix<9> half_pi9, two_pi9, half9;
+    Fix<3> half3;
     Iv<7> half_pi7, half7;
     Iv<15> half_pi15, half15;
     Iv<58> half_pi58, half58;
@@ -614,6 +618,175 @@ __global__ void __launch_bounds__(128) cert_stage_kernel(
     }
 }
 
+// ------------------------------------------------------------ FP64 prefilter
+// Directed-rounding FP64 interval SAT of the pairs the float check left open,
+// ahead of the multi-limb stages.  It decides a pair only where those stages
+// are certain to decide it the same way, so verdicts stay the reference's:
+//   * separated (1) when some axis's overlap interval lies strictly below
+//     zero, overlapping (-1) when every axis's lies strictly above: the
+//     intervals enclose the exact overlap of the exact decimal inputs, so its
+//     sign is certain, and an exact value of |v| >= 2^-1074 is resolved the
+//     same way by the 7-, 15- or 58-limb stage (widths below 1e-60);
+//   * two axis-aligned squares (angle literal exactly zero, the reference's
+//     flat path) whose coordinate literals and square 0's are all dyadic
+//     within 25 decimal places are compared exactly in 3-limb fixed point,
+//     the values the 7-limb stage computes exactly: touching edges decide
+//     as separated, as they do there;
+//   * everything else goes on to the 7-limb stage.
+// Bounds: a literal's value from its 27-decimal truncation (error < 1e-27)
+// converted to double (error below (|v| + 1) 2^-47), widened by both; sin
+// and cos from CUDA's double sincos, whose documented error is 2 ulp
+// (below 2^-51 in [-1, 1]), widened by that and by the angle's half-width.
+struct DIv {
+    double lo, hi;
+};
+__device__ __forceinline__ DIv d_add(DIv a, DIv b) { return DIv{__dadd_rd(a.lo, b.lo), __dadd_ru(a.hi, b.hi)}; }
+__device__ __forceinline__ DIv d_sub(DIv a, DIv b) { return DIv{__dsub_rd(a.lo, b.hi), __dsub_ru(a.hi, b.lo)}; }
+__device__ __forceinline__ DIv d_mul(DIv a, DIv b) {
+    const double l0 = __dmul_rd(a.lo, b.lo), l1 = __dmul_rd(a.lo, b.hi), l2 = __dmul_rd(a.hi, b.lo),
+                 l3 = __dmul_rd(a.hi, b.hi);
+    const double h0 = __dmul_ru(a.lo, b.lo), h1 = __dmul_ru(a.lo, b.hi), h2 = __dmul_ru(a.hi, b.lo),
+                 h3 = __dmul_ru(a.hi, b.hi);
+    return DIv{fmin(fmin(l0, l1), fmin(l2, l3)), fmax(fmax(h0, h1), fmax(h2, h3))};
+}
+__device__ __forceinline__ DIv d_half(DIv a) { return DIv{0.5 * a.lo, 0.5 * a.hi}; }  // exact
+__device__ __forceinline__ DIv d_neg(DIv a) { return DIv{-a.hi, -a.lo}; }
+
+// Enclosure of a literal's exact value.
+__device__ __forceinline__ DIv lit_iv(const char* text, const Lit& L) {
+    const double a = fx::approx(fx::parse<3>(text, L, 0));
+    const double eps = __dadd_ru(__dmul_ru(__dadd_ru(fabs(a), 1.0), 0x1p-47), 1e-27);
+    return DIv{__dsub_rd(a, eps), __dadd_ru(a, eps)};
+}
+
+__device__ __forceinline__ bool lit_is_zero(const char* text, const Lit& L) {
+    for (int k = 0; k < L.ndig; ++k)
+        if (fx::lit_digit(text, L, k) != 0) return false;
+    return true;
+}
+
+struct DSq {
+    bool flat;
+    DIv c, s, X, Y;
+    DIv px[4], py[4];
+};
+
+__device__ __noinline__ void make_dsq(const char* text, const Lit* L3, DIv ox, DIv oy, DSq& e) {
+    e.X = d_sub(lit_iv(text, L3[0]), ox);
+    e.Y = d_sub(lit_iv(text, L3[1]), oy);
+    e.flat = lit_is_zero(text, L3[2]);
+    if (e.flat) {
+        e.c = DIv{1.0, 1.0};
+        e.s = DIv{0.0, 0.0};
+    } else {
+        const DIv a = lit_iv(text, L3[2]);
+        const double mid = 0.5 * (a.lo + a.hi);
+        double sn, cs;
+        sincos(mid, &sn, &cs);
+        const double w = __dadd_ru(0x1p-50, __dsub_ru(a.hi, a.lo));
+        e.c = DIv{__dsub_rd(cs, w), __dadd_ru(cs, w)};
+        e.s = DIv{__dsub_rd(sn, w), __dadd_ru(sn, w)};
+    }
+    const DIv hc = d_half(e.c), hs = d_half(e.s);
+    const DIv ux = d_sub(hc, hs), uy = d_add(hs, hc);
+    const DIv vx = d_sub(d_neg(hc), hs), vy = d_add(d_neg(hs), hc);
+    e.px[0] = d_add(e.X, ux); e.py[0] = d_add(e.Y, uy);
+    e.px[1] = d_add(e.X, vx); e.py[1] = d_add(e.Y, vy);
+    e.px[2] = d_sub(e.X, ux); e.py[2] = d_sub(e.Y, uy);
+    e.px[3] = d_sub(e.X, vx); e.py[3] = d_sub(e.Y, vy);
+}
+
+// Exact box test of two axis-aligned squares with dyadic literals (the
+// reference's flat path on exact values): 1 separated or touching, -1 overlapping.
+__device__ __noinline__ int exact_flat_sat(const char* text, const Lit* P, const Lit* Q, const Lit* O) {
+    using F3 = Fix<3>;
+    const F3 ox = fx::parse<3>(text, O[0], 0), oy = fx::parse<3>(text, O[1], 0);
+    const F3 h = c_consts.half3;
+    const F3 px = fx::sub(fx::parse<3>(text, P[0], 0), ox), py = fx::sub(fx::parse<3>(text, P[1], 0), oy);
+    const F3 qx = fx::sub(fx::parse<3>(text, Q[0], 0), ox), qy = fx::sub(fx::parse<3>(text, Q[1], 0), oy);
+    auto mn = [](const F3& a, const F3& b) { return fx::cmp(a, b) < 0 ? a : b; };
+    auto mx = [](const F3& a, const F3& b) { return fx::cmp(a, b) > 0 ? a : b; };
+    F3 z;
+    fx::set_zero(z);
+    const F3 ovx = fx::sub(mn(fx::add(px, h), fx::add(qx, h)), mx(fx::sub(px, h), fx::sub(qx, h)));
+    if (fx::cmp(ovx, z) <= 0) return 1;
+    const F3 ovy = fx::sub(mn(fx::add(py, h), fx::add(qy, h)), mx(fx::sub(py, h), fx::sub(qy, h)));
+    if (fx::cmp(ovy, z) <= 0) return 1;
+    return -1;
+}
+
+// 1 separated, -1 overlapping, 0 left to the multi-limb stages.
+__device__ __noinline__ int fp64_sat(const DSq& p, const DSq& q) {
+    if (p.flat && q.flat) {
+        const DIv ox = DIv{__dsub_rd(fmin(__dadd_rd(p.X.lo, 0.5), __dadd_rd(q.X.lo, 0.5)),
+                                     fmax(__dsub_ru(p.X.hi, 0.5), __dsub_ru(q.X.hi, 0.5))),
+                           __dsub_ru(fmin(__dadd_ru(p.X.hi, 0.5), __dadd_ru(q.X.hi, 0.5)),
+                                     fmax(__dsub_rd(p.X.lo, 0.5), __dsub_rd(q.X.lo, 0.5)))};
+        const DIv oy = DIv{__dsub_rd(fmin(__dadd_rd(p.Y.lo, 0.5), __dadd_rd(q.Y.lo, 0.5)),
+                                     fmax(__dsub_ru(p.Y.hi, 0.5), __dsub_ru(q.Y.hi, 0.5))),
+                           __dsub_ru(fmin(__dadd_ru(p.Y.hi, 0.5), __dadd_ru(q.Y.hi, 0.5)),
+                                     fmax(__dsub_rd(p.Y.lo, 0.5), __dsub_rd(q.Y.lo, 0.5)))};
+        if (ox.hi < 0.0 || oy.hi < 0.0) return 1;
+        if (ox.lo > 0.0 && oy.lo > 0.0) return -1;
+        return 0;
+    }
+    bool all_pos = true;
+    for (int a = 0; a < 4; ++a) {
+        const DSq& o = a < 2 ? p : q;
+        const DIv ax = (a & 1) ? d_neg(o.s) : o.c, ay = (a & 1) ? o.c : o.s;
+        DIv mn1{1e300, 1e300}, mx1{-1e300, -1e300}, mn2{1e300, 1e300}, mx2{-1e300, -1e300};
+        for (int k = 0; k < 4; ++k) {
+            const DIv u = d_add(d_mul(ax, p.px[k]), d_mul(ay, p.py[k]));
+            const DIv v = d_add(d_mul(ax, q.px[k]), d_mul(ay, q.py[k]));
+            mn1 = DIv{fmin(mn1.lo, u.lo), fmin(mn1.hi, u.hi)};
+            mx1 = DIv{fmax(mx1.lo, u.lo), fmax(mx1.hi, u.hi)};
+            mn2 = DIv{fmin(mn2.lo, v.lo), fmin(mn2.hi, v.hi)};
+            mx2 = DIv{fmax(mx2.lo, v.lo), fmax(mx2.hi, v.hi)};
+        }
+        const DIv ov = d_sub(DIv{fmin(mx1.lo, mx2.lo), fmin(mx1.hi, mx2.hi)},
+                             DIv{fmax(mn1.lo, mn2.lo), fmax(mn1.hi, mn2.hi)});
+        if (ov.hi < 0.0) return 1;
+        all_pos &= ov.lo > 0.0;
+    }
+    return all_pos ? -1 : 0;
+}
+
+__global__ void __launch_bounds__(128) cert_fp64_kernel(const Pair* __restrict__ in, const uint32_t* __restrict__ in_count,
+                                                        uint32_t in_cap, Pair* __restrict__ next,
+                                                        uint32_t* __restrict__ next_count, uint32_t next_cap,
+                                                        const int64_t* __restrict__ pk_sq0,
+                                                        const Lit* __restrict__ lits, const char* __restrict__ text,
+                                                        PkOut* __restrict__ out) {
+    const uint32_t total = min(*in_count, in_cap);
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const Pair pr = in[t];
+        PkOut& po = out[pr.pk];
+        if (po.fkey != kNoPair || (po.flags & kCertOverlap)) continue;
+        const int64_t s0 = pk_sq0[pr.pk];
+        const Lit* O = lits + 3 * s0;
+        const Lit* P = lits + 3 * (s0 + pr.u);
+        const Lit* Q = lits + 3 * (s0 + pr.v);
+        int r;
+        if (lit_is_zero(text, P[2]) && lit_is_zero(text, Q[2]) && O[0].dyadic && O[1].dyadic && P[0].dyadic &&
+            P[1].dyadic && Q[0].dyadic && Q[1].dyadic) {
+            r = exact_flat_sat(text, P, Q, O);
+        } else {
+            const DIv ox = lit_iv(text, O[0]), oy = lit_iv(text, O[1]);
+            DSq A, B;
+            make_dsq(text, P, ox, oy, A);
+            make_dsq(text, Q, ox, oy, B);
+            r = fp64_sat(A, B);
+        }
+        if (r < 0) {
+            atomicOr(&po.flags, kCertOverlap);
+        } else if (r == 0) {
+            const uint32_t slot = atomicAdd(next_count, 1u);
+            if (slot < next_cap) next[slot] = pr;
+            else atomicOr(&po.flags, kPairOverflow);
+        }
+    }
+}
+
 // ------------------------------------------------------------ cached stages
 // The same interval test with every square's interval corners computed once
 // per stage, as the reference caches them per square (ensure_sq_iv,
@@ -742,6 +915,7 @@ static int upload_consts(int device) {
     c.half_pi9 = fx::parse<9>(kHalfPi, hp, 0);
     c.two_pi9 = fx::parse<9>(kTwoPi, tp, 0);
     c.half9 = fx::parse<9>("0.5", h, 0);
+    c.half3 = fx::parse<3>("0.5", h, 0);
     c.half_pi7 = fx::parse_iv<7>(kHalfPi, hp);
     c.half7 = fx::parse_iv<7>("0.5", h);
     c.half_pi15 = fx::parse_iv<15>(kHalfPi, hp);
@@ -841,6 +1015,17 @@ static int launch_stage(sqs_ctx* ctx, const Pair* in, const uint32_t* in_count, 
                         const char* text, PkOut* out, int blocks) {
     cert_stage_kernel<F><<<blocks, 128, 0, ctx->stream>>>(in, in_count, in_cap, next, next_count, next_cap,
                                                          pk_sq0, lits, text, out);
+    SQS_CUDA(cudaGetLastError());
+    ctx->launches += 1;
+    return SQS_OK;
+}
+
+// The FP64 prefilter over a pair list (grid-stride; the count stays on the device).
+static int launch_fp64(sqs_ctx* ctx, const Pair* in, const uint32_t* in_count, uint32_t in_cap, Pair* next,
+                       uint32_t* next_count, uint32_t next_cap, const int64_t* pk_sq0, const Lit* lits,
+                       const char* text, PkOut* out, int blocks) {
+    cert_fp64_kernel<<<blocks, 128, 0, ctx->stream>>>(in, in_count, in_cap, next, next_count, next_cap, pk_sq0, lits,
+                                                       text, out);
     SQS_CUDA(cudaGetLastError());
     ctx->launches += 1;
     return SQS_OK;
@@ -1088,12 +1273,16 @@ extern "C" int sqs_certify_batch(sqs_ctx* ctx, int count, const int32_t* n_of, c
                                           d_text, d_off, d_len, d_lits, d_out, pa, cnt, cap)) return r;
     int32_t* slot_of = (int32_t*)(D + g_slot.off);
     SqRef* list = (SqRef*)(D + g_list.off);
-    if (int r = cached_stage<7>(ctx, pa, cnt, cap, pb, cnt + 1, d_s0, d_lits, d_text, d_out, slot_of, list, cnt + 3, S))
+    // FP64 prefilter pa -> pb, then the 7-, 15- and 58-limb stages pb -> pa -> pb
+    if (int r = launch_fp64(ctx, pa, cnt, cap, pb, cnt + 5, cap, d_s0, d_lits, d_text, d_out, ctx->sm_count * 8))
         return r;
-    if (int r = cached_stage<15>(ctx, pb, cnt + 1, cap, pa, cnt + 2, d_s0, d_lits, d_text, d_out, slot_of, list,
+    if (int r = cached_stage<7>(ctx, pb, cnt + 5, cap, pa, cnt + 1, d_s0, d_lits, d_text, d_out, slot_of, list, cnt + 3,
+                                S))
+        return r;
+    if (int r = cached_stage<15>(ctx, pa, cnt + 1, cap, pb, cnt + 2, d_s0, d_lits, d_text, d_out, slot_of, list,
                                  cnt + 3, S))
         return r;
-    if (int r = cached_stage<58>(ctx, pa, cnt + 2, cap, nullptr, nullptr, d_s0, d_lits, d_text, d_out, slot_of, list,
+    if (int r = cached_stage<58>(ctx, pb, cnt + 2, cap, nullptr, nullptr, d_s0, d_lits, d_text, d_out, slot_of, list,
                                  cnt + 3, S))
         return r;
     std::vector<PkOut> h((size_t)count);
@@ -1229,6 +1418,7 @@ static int static_setup(sqs_ctx* ctx) {
     const int64_t* d_s0 = (const int64_t*)(D + kSoS0);
     const Lit* d_lits = (const Lit*)(D + kSoLits);
     PkOut* d_out = (PkOut*)(D + kSoOut);
+    if (int r = launch_fp64(ctx, pa, cnt, 0, nullptr, nullptr, 0, d_s0, d_lits, D, d_out, 1)) return r;
     if (int r = launch_stage<7>(ctx, pa, cnt, 0, nullptr, nullptr, 0, d_s0, d_lits, D, d_out, 1)) return r;
     if (int r = launch_stage<15>(ctx, pa, cnt, 0, nullptr, nullptr, 0, d_s0, d_lits, D, d_out, 1)) return r;
     if (int r = launch_stage<58>(ctx, pa, cnt, 0, nullptr, nullptr, 0, d_s0, d_lits, D, d_out, 1)) return r;
@@ -1373,10 +1563,11 @@ extern "C" int sqs_certify_batch_static(sqs_ctx* ctx, int count, const int32_t* 
                                           d_out, pa, cnt, cap))
         return r;
     const int blocks = ctx->sm_count * 8;
-    if (int r = launch_stage<7>(ctx, pa, cnt, cap, pb, cnt + 1, cap, d_s0, d_lits, d_text, d_out, blocks)) return r;
-    if (int r = launch_stage<15>(ctx, pb, cnt + 1, cap, pa, cnt + 2, cap, d_s0, d_lits, d_text, d_out, blocks))
+    if (int r = launch_fp64(ctx, pa, cnt, cap, pb, cnt + 5, cap, d_s0, d_lits, d_text, d_out, blocks)) return r;
+    if (int r = launch_stage<7>(ctx, pb, cnt + 5, cap, pa, cnt + 1, cap, d_s0, d_lits, d_text, d_out, blocks)) return r;
+    if (int r = launch_stage<15>(ctx, pa, cnt + 1, cap, pb, cnt + 2, cap, d_s0, d_lits, d_text, d_out, blocks))
         return r;
-    if (int r = launch_stage<58>(ctx, pa, cnt + 2, cap, nullptr, nullptr, 0, d_s0, d_lits, d_text, d_out, blocks))
+    if (int r = launch_stage<58>(ctx, pb, cnt + 2, cap, nullptr, nullptr, 0, d_s0, d_lits, d_text, d_out, blocks))
         return r;
     SQS_CUDA(cudaMemcpyAsync(s_out, d_out, sizeof(PkOut) * (size_t)count, cudaMemcpyDeviceToHost, st));
     SQS_CUDA(cudaStreamSynchronize(st));
