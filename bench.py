@@ -437,6 +437,11 @@ def run_sqs(args, D: Dist):
         line["certify"] = bench_certify(ctx, args.cpu_seconds)
         line["served"] = bench_served_sweep(ctx, args.served_rates, args.served_jobs, args.served_sweeps,
                                             args.served_slice)
+        # 10,000 sweeps on a 24-job stream of the full n range, and the
+        # configured 50,000 sweeps on an 8-job stream of n <= 100 (a job of
+        # n = 1000 alone needs over a minute at 50,000 sweeps)
+        line["served_10k"] = bench_served_budget(ctx, 24, 10000)
+        line["served_50k"] = bench_served_budget(ctx, 8, 50000, n_hi=100)
         line["plain_pt"] = bench_plain_pt(ctx)
         line["batched"] = bench_batched(ctx)
     for d in (d_x, d_s, d_e, d_g, d_c):
@@ -449,7 +454,7 @@ def run_sqs(args, D: Dist):
 
 
 # ------------------------------------------------------------------ extras
-def bench_certify(ctx, cpu_seconds: float, count: int = 10000):
+def bench_certify(ctx, cpu_seconds: float = 0.0, count: int = 10000):
     """The interval-certifier batch: 10,000 packings, n log-uniform in
     [5, 1000], half exact grids, half tilted near-contact lattices, 5% with
     injected 1e-10 overlaps; GPU end to end from host strings vs the
@@ -477,28 +482,30 @@ def bench_certify(ctx, cpu_seconds: float, count: int = 10000):
     import oracle as O
 
     which = "ref" if O.ref_available() else "oracle"
-    # bounded CPU sample: packings in corpus order until ~cpu_seconds of work
-    k, t0, done, agree = 0, time.perf_counter(), 0, True
-    while k < count and time.perf_counter() - t0 < cpu_seconds:
-        sub = items[k:k + 64]
-        ok, _, used = O.certify_batch(*core.pack_batch(sub), which=which)
-        agree &= bool(np.array_equal(ok, gpu_ok[k:k + len(sub)]))
-        done += len(sub)
-        k += len(sub)
+    # the whole batch on the host cores: the CPU baseline and the check of
+    # every verdict, reason, score and 50-decimal side
+    t0 = time.perf_counter()
+    ok, score, Ls, reasons = O.certify_batch_text(*arrs, which=which)
     cpu_s = time.perf_counter() - t0
-    res["cpu_baseline"] = dict(packings_per_s=done / cpu_s, cores=used,
+    used = os.cpu_count() or 1
+    same = sum(1 for p in range(count)
+               if (int(out[p].ok), float(out[p].score), out[p].L.decode(), out[p].reason.decode()) ==
+               (int(ok[p]), float(score[p]), Ls[p], reasons[p]))
+    res["cpu_baseline"] = dict(packings_per_s=count / cpu_s, seconds=cpu_s, cores=used,
                                kind="reference" if which == "ref" else "port",
-                               sample=f"first {done} packings of the batch")
-    res["verdicts_equal_on_sample"] = agree
+                               sample=f"all {count} packings")
+    res["equal_to_reference"] = dict(packings=count, identical=same,
+                                     fields="verdict, reason, score, 50-decimal side")
     res["speedup_vs_cpu"] = res["packings_per_s"] / res["cpu_baseline"]["packings_per_s"]
     return res
 
 
-def served_jobs(count: int, sweeps: int = 200):
+def served_jobs(count: int, sweeps: int = 2000, n_hi: int = 1000):
     """Anneal-and-certify jobs of the served stream: n log-uniform in
-    [5, 1000], 16, 32 or 64 replicas, a `sweeps` budget each (200 by default:
-    a bounded stand-in for the 50,000 sweeps a production job would run, so
-    the bench ends in minutes), seeded."""
+    [5, n_hi], 16, 32 or 64 replicas, a `sweeps` budget each (2,000 by
+    default: a bounded stand-in for the configured 50,000 sweeps, whose stream
+    of n up to 1000 would not end in a bench run -- one n = 1000 job alone
+    takes over a minute at 50,000 sweeps), seeded."""
     import math
 
     import numpy as np
@@ -508,7 +515,7 @@ def served_jobs(count: int, sweeps: int = 200):
     rng = np.random.default_rng(7)
     jobs = []
     for k in range(count):
-        n = int(round(math.exp(rng.uniform(math.log(5), math.log(1000)))))
+        n = int(round(math.exp(rng.uniform(math.log(5), math.log(n_hi)))))
         replicas = int(rng.choice([16, 32, 64]))
         xya, L0 = jittered_grid(n, seed=100 + k)
         jobs.append(AnnealJob(xya, L0=L0, replicas=replicas, sweeps=sweeps, exchange_every=10, tmin=1e-3, tmax=1e-1,
@@ -516,7 +523,7 @@ def served_jobs(count: int, sweeps: int = 200):
     return jobs
 
 
-def bench_served(ctx, jobs, plain, rate: float, slice_proposals: int = 4000):
+def bench_served(ctx, jobs, plain, rate: float, slice_proposals: int = 4000, live=None):
     """Served vs plain at one Poisson arrival rate: a stream of about four
     seconds of arrivals (at least 40 jobs, at most all of them) through the
     continuous-batching server; the plain comparator serves the same jobs one
@@ -535,6 +542,8 @@ def bench_served(ctx, jobs, plain, rate: float, slice_proposals: int = 4000):
         counters = srv.stats()
     p_res, p_service = plain
     p_stats = plain_stats(p_res[:count], p_service[:count], arr)
+    if live is not None:
+        p_stats["live"] = live
     same_L = all((a or {}).get("L") == (b or {}).get("L") for a, b in zip(served, p_res[:count]))
     # annealing work done per second of the stream: against the batched
     # launch's rate it says how busy the stream kept the GPU
@@ -573,14 +582,46 @@ def bench_plain_pt(ctx):
     return res
 
 
-def bench_served_sweep(ctx, rates: str, count: int = 960, sweeps: int = 200, slice_proposals: int = 4000):
-    from sqs.serve import plain_service
+def bench_served_sweep(ctx, rates: str, count: int = 240, sweeps: int = 2000, slice_proposals: int = 4000,
+                       live_rate: float = 200.0):
+    """Served vs plain at each rate.  The plain comparator is run live once,
+    at `live_rate` (its jobs served one launch per job as they arrive); its
+    measured per-job service times give the FIFO latencies at the other rates
+    (the plain queue never empties, so live and computed agree: both are
+    reported at the live rate)."""
+    import math
+
+    from sqs.serve import poisson_arrivals, run_plain_live
 
     rs = [float(x) for x in rates.split(",") if x]
     jobs = served_jobs(count, sweeps)
-    need = min(count, max(40, max(int(4 * r + 1) for r in rs)))
-    plain = plain_service(ctx, jobs[:need])
-    return {f"{r:g}/s": bench_served(ctx, jobs, plain, r, slice_proposals) for r in rs}
+    need = min(count, max(40, max(int(math.ceil(4 * r)) for r in rs)))
+    live_count = min(len(jobs), max(40, int(math.ceil(4 * live_rate))))
+    assert live_count >= need or live_count == len(jobs)
+    p_res, p_service, p_live = run_plain_live(ctx, jobs[:live_count], poisson_arrivals(live_count, live_rate, seed=3))
+    plain = (p_res, p_service)
+    out = {f"{r:g}/s": bench_served(ctx, jobs, plain, r, slice_proposals, live=p_live if r == live_rate else None)
+           for r in rs}
+    out["budget_sweeps"] = sweeps
+    return out
+
+
+def bench_served_budget(ctx, count: int, sweeps: int, n_hi: int = 1000, rate: float = 200.0,
+                        slice_proposals: int = 4000):
+    """A short stream at a large budget: `count` jobs, n log-uniform in
+    [5, n_hi], 16/32/64 replicas, `sweeps` each, Poisson arrivals; served
+    against the plain comparator run live."""
+    from sqs.serve import Server, poisson_arrivals, run_plain_live, run_stream
+
+    jobs = served_jobs(count, sweeps=sweeps, n_hi=n_hi)
+    arr = poisson_arrivals(count, rate, seed=3)
+    with Server(ctx, hbm_bytes=4 << 30, max_active=count, slice_proposals=slice_proposals) as srv:
+        served, s_stats = run_stream(srv, jobs, arr, timeout=900)
+    p_res, _, p_stats = run_plain_live(ctx, jobs, arr)
+    same_L = all((a or {}).get("L") == (b or {}).get("L") for a, b in zip(served, p_res))
+    return dict(workload=f"{count} jobs, Poisson {rate:g}/s, n log-uniform [5, {n_hi}], 16/32/64 replicas, "
+                         f"{sweeps} sweeps", served=s_stats, plain_live=p_stats, equal_final_L=same_L,
+                served_over_plain=s_stats["certified_jobs_per_s"] / max(p_stats["certified_jobs_per_s"], 1e-12))
 
 
 # Algorithmic FP32 work of one proposal, the cost unit 2 k * 35 + 2 * 10 flop
@@ -746,13 +787,14 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the certifier / served / plain-PT / batched sections")
-    ap.add_argument("--section", choices=("certify", "served", "plain_pt", "batched", "batched_fixed", "search"),
+    ap.add_argument("--section", choices=("certify", "served", "served_full", "plain_pt", "batched", "batched_fixed",
+                                          "search", "anneal_accuracy"),
                     help="run only this extra section (for profiling) and print its dict")
     ap.add_argument("--batched-instances", type=int, default=512)
     ap.add_argument("--batched-sweeps", type=int, default=50)
-    ap.add_argument("--served-rates", default="10,50,200,1000")
-    ap.add_argument("--served-jobs", type=int, default=960, help="most jobs in one served stream")
-    ap.add_argument("--served-sweeps", type=int, default=200, help="sweep budget of every served job")
+    ap.add_argument("--served-rates", default="200,1000")
+    ap.add_argument("--served-jobs", type=int, default=240, help="most jobs in one served stream")
+    ap.add_argument("--served-sweeps", type=int, default=2000, help="sweep budget of every served job")
     ap.add_argument("--served-slice", type=int, default=4000, help="proposals per replica per server slice")
     ap.add_argument("--search-prog", choices=("seeded", "packing"), default="seeded",
                     help="which search program the search section compares")
@@ -764,10 +806,13 @@ def main():
             fn = dict(certify=lambda: bench_certify(ctx, args.cpu_seconds),
                       served=lambda: bench_served_sweep(ctx, args.served_rates, args.served_jobs,
                                                         args.served_sweeps, args.served_slice),
+                      served_full=lambda: dict(served_10k=bench_served_budget(ctx, 24, 10000),
+                                               served_50k=bench_served_budget(ctx, 8, 50000, n_hi=100)),
                       plain_pt=lambda: bench_plain_pt(ctx),
                       batched=lambda: bench_batched(ctx, args.batched_sweeps, args.batched_instances),
                       batched_fixed=lambda: bench_batched_fixed(ctx, args.batched_sweeps, args.batched_instances),
-                      search=lambda: bench_search(prog=args.search_prog))[args.section]
+                      search=lambda: bench_search(prog=args.search_prog),
+                      anneal_accuracy=lambda: anneal_accuracy(ctx))[args.section]
             print(json.dumps({args.section: fn()}), flush=True)
         return
     if args.warmup < 3:

@@ -155,6 +155,28 @@ def plain_stats(results: list[dict], service: list[float], arrivals) -> dict:
     return _latency_stats(lat, span, sum(bool(r["certified"]) for r in results))
 
 
+def run_plain_live(ctx: N.Context, jobs: list[AnnealJob], arrivals, *, timeout: float = 3600.0):
+    """The comparator run live: jobs served one at a time in arrival order,
+    each waiting for its arrival time, every job alone in its own anneal,
+    polish and certify launches.  Returns (results, seconds per job, stats
+    from the measured completion times)."""
+    t0 = time.perf_counter()
+    results, service, done_at = [], [], []
+    for job, a in zip(jobs, arrivals):
+        now = time.perf_counter() - t0
+        if now > timeout:
+            raise TimeoutError("plain stream did not drain in time")
+        if now < a:
+            time.sleep(a - now)
+        t = time.perf_counter()
+        results.append(anneal_batch([job], ctx=ctx)[0])
+        service.append(time.perf_counter() - t)
+        done_at.append(time.perf_counter() - t0)
+    lat = [d - float(a) for d, a in zip(done_at, arrivals)]
+    span = max(done_at) - float(arrivals[0]) if jobs else 0.0
+    return results, service, _latency_stats(lat, span, sum(bool(r["certified"]) for r in results))
+
+
 def run_plain(ctx: N.Context, jobs: list[AnnealJob], arrivals):
     """The comparator: every job alone in its own anneal/polish/certify
     launches, in arrival order (FIFO).  Returns (results, stats)."""

@@ -167,7 +167,7 @@ def test_target_ladders_follow_the_reference_offsets(ctx, oracle):
     temp = {int(k): float(T) for k, T in zip(t["rung"], t["temperature"])}
     for k in range(8):
         assert temp[k] == temp[k + 8]
-    assert r["shrinks"] >= 1
+    assert r["improvements"] >= 1
     assert B <= job.L0 + 1e-6
 
 

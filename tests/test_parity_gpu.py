@@ -117,28 +117,30 @@ def test_running_energy_survives_slicing_and_moves(ctx, oracle):
     energy_errors(res, oracle)
 
 
-@pytest.mark.parametrize("config", ["plain_n10", "batched_sample"])
-def test_certified_side_matches_oracle(ctx, oracle, config):
+def test_certified_side_matches_oracle(ctx, oracle):
+    """The device certified side on every final replica of the plain and a
+    batched sample: the dilation everywhere (the plain job's final states sit
+    in a side below its best, so most need more than 1.008 and are rejected
+    by both), the side wherever the dilation is accepted."""
     from sqs.anneal import anneal_batch
-    from dataclasses import replace
-    # every replica quenched at the last checkpoint, so most final states certify
-    jobs = {"plain_n10": lambda: [replace(j, quench_all=True) for j in plain_jobs()],
-            "batched_sample": lambda: batched_jobs(count=12, sweeps=400)}[config]()
+    jobs = plain_jobs() + batched_jobs(count=12, sweeps=400)
     res = anneal_batch(jobs, ctx=ctx, trace=True)
-    measured = exact = 0
+    measured = exact = lams = 0
     for r in res:
         t = r["trace"]
         for k in range(len(t["L_cert"])):
             L, lam, _ = oracle.certified_side(t["xya"][k].astype(np.float64))
             assert lam == pytest.approx(t["dilation"][k], rel=SIDE_REL), (k, lam, t["dilation"][k])
+            lams += 1
             if L >= 1e8:
                 assert t["L_cert"][k] >= 1e8
                 continue
             measured += 1
             exact += L == t["L_cert"][k]
             assert t["L_cert"][k] == pytest.approx(L, rel=SIDE_REL), (k, L, t["L_cert"][k])
-    assert measured >= 4, "too few replicas certified to compare"
-    print(f"{config}: {measured} certified sides compared, {exact} bit-identical")
+    assert lams == sum(j.replicas for j in jobs)
+    assert measured >= 8, "too few replicas certified to compare"
+    print(f"{lams} dilations and {measured} certified sides compared, {exact} sides bit-identical")
 
 
 def test_temperature_and_step_schedule(ctx):
