@@ -444,6 +444,8 @@ def run_sqs(args, D: Dist):
         line["served_50k"] = bench_served_budget(ctx, 8, 50000, n_hi=100)
         line["plain_pt"] = bench_plain_pt(ctx)
         line["batched"] = bench_batched(ctx)
+        # the seeded drop-in against the reference's own seeded program on this GPU
+        line["search"] = bench_search()
     for d in (d_x, d_s, d_e, d_g, d_c):
         d.free()
     for h in (hin, hs, he, hg):

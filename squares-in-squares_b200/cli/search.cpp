@@ -223,6 +223,11 @@ int main(int argc, char** argv) {
                 j.sweeps = (int)std::max<long long>(-2000000000LL, -std::max(1LL, proposals_per_chain));
                 j.exchange_every = -std::max(1, steps);
                 j.flags |= SQS_JOB_TARGETS | SQS_JOB_LADDERS(lad);
+                // without the tuner, the widest cluster (up to 16 CTAs): the
+                // checkpoint quenches a CTA's replicas one after another, so
+                // fewer replicas per CTA finish an epoch sooner, as the
+                // reference polishes its chains on separate blocks
+                if (!autotune) j.flags |= SQS_JOB_CLUSTER(std::min(16, 8 * lad));
                 j.shrink = std::min(0.1 / 20.0, shrink / L);
             } else {
                 j.sweeps = sweeps;
