@@ -233,7 +233,9 @@ typedef struct sqs_job {
 #define SQS_JOB_QUENCH_STEPS(k) ((int32_t)(k) << 24)
 /* The reference search's target-side ladder (seeded.cu:474-481, 908-943): from
  * the first proposal every rung anneals in its own container below the best
- * side B found so far (the initial side before the first certificate):
+ * side B found so far (the initial side before the first certificate; only
+ * a certified side below the initial one counts, as the reference's chain
+ * bests start at the seed's side):
  * side max(sqrt n + 1e-6, B (1 - shrink m)) with m the reference's offsets
  * {0.02, 0.1, 0.4, 1, 2.5, 5, 10, 20} for the rung's place in its ladder.  A
  * new certified best becomes B (no further factor), every ladder's head rung

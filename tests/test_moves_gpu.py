@@ -139,7 +139,10 @@ def test_proposal_counted_budgets_equal_sweep_counted_ones(ctx):
 
 
 def _target_job(**kw):
-    args = dict(n=48, sweeps=-48 * 60, exchange_every=-24, replicas=16, tmin=1e-11, tmax=1e-4, shrink=0.001 / 7,
+    # a 7-column grid of 48 squares in a side-7.5 box: certified sides below
+    # the initial side exist, so the ladders improve on it
+    args = dict(n=48, L0=7.5, sweeps=-48 * 60, exchange_every=-24, replicas=16, tmin=1e-11, tmax=1e-4,
+                shrink=0.001 / 7,
                 polish_iters=100, targets=True, ladders=2, adapt=True, kick=True, quench_all=True, cert_all=True,
                 quench_steps=4)
     args.update(kw)
