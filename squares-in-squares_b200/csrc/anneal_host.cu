@@ -117,7 +117,7 @@ int prepare_job(const sqs_job& J, int j, JobDev& d, JobMut& m, Plan& p, const Sh
     // under SQS_JOB_QUENCH_STEPS(k) 16 k iterations with no slow-step exit
     const int qk = (J.flags >> 24) & 0x7f;
     d.quench_iters = qk ? 16 * qk : 64;
-    d.quench_stall = qk ? kQuenchCG : 3;
+    d.quench_stall = qk ? kQuenchNoStall : 3;
     d.flags = J.flags & (kMoveAdapt | kMoveCollective | kMoveKick | kMoveSerial | kMoveQuenchAll | kCertAll | kTargets);
     std::memset(&m, 0, sizeof m);
     m.L = (float)J.L0;
@@ -131,7 +131,7 @@ int prepare_job(const sqs_job& J, int j, JobDev& d, JobMut& m, Plan& p, const Sh
     return SQS_OK;
 }
 
-int64_t job_pos_elems(const sqs_job& J) { return (int64_t)J.replicas * J.n + 4 * (int64_t)J.n; }
+int64_t job_pos_elems(const sqs_job& J) { return (int64_t)J.replicas * J.n + 2 * (int64_t)J.n; }
 
 int64_t job_props(const sqs_job& J) { return J.sweeps >= 0 ? (int64_t)J.sweeps * J.n : -(int64_t)J.sweeps; }
 

@@ -63,7 +63,7 @@ int prepare_job(const sqs_job& J, int j, JobDev& d, JobMut& m, Plan& p, const Sh
 // first sight) and, when the job leaves exchange_every at 0, the tuned
 // interval written into `eff` (a copy of the job).  No flag: eff = job.
 int resolve_job(sqs_ctx* ctx, const sqs_job& job, int mode, sqs_job& eff, Shape& shape);
-// float4 elements of a job's state region: R*n replica squares + 4n quench scratch.
+// float4 elements of a job's state region: R*n replica squares + 2n quench scratch.
 int64_t job_pos_elems(const sqs_job& J);
 // Proposals per replica in a job's budget (sweeps * n, or -sweeps), and that
 // budget in whole sweeps, rounded up.

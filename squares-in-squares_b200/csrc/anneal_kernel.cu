@@ -41,11 +41,14 @@ namespace ann {
 constexpr float kHalfPiF = 1.57079632679489662f;
 
 // cos/sin of a replica's angle, wherever the state's trig is (re)computed:
-// the hardware approximation (absolute error below 4e-7 on [0, pi/2)), the
-// same function everywhere so a state's (cos, sin) never depends on where it
-// was computed (a sliced run reloads what an unsliced one kept).  The FP64
-// certified side recomputes trig from the angle itself.
-__device__ __forceinline__ void state_trig(float a, float* s, float* c) { __sincosf(a, s, c); }
+// CUDA's full-accuracy sincosf, the same function everywhere so a state's
+// (cos, sin) never depends on where it was computed (a sliced run reloads what
+// an unsliced one kept).  Against the hardware approximation it costs about 3%
+// of the proposal rate and cuts the FP32 energies' absolute error against the
+// FP64 oracle about eightfold (measured on the batched and served samples), to
+// well inside the 1e-5 floor.  The FP64 certified side recomputes trig from
+// the angle itself.
+__device__ __forceinline__ void state_trig(float a, float* s, float* c) { sincosf(a, s, c); }
 
 struct Rep {  // one replica's shared-memory view
     float4* sq;        // (x, y, cos a, sin a)
@@ -452,141 +455,6 @@ __device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters
                 __syncthreads();
             }
             break;
-        }
-    }
-    return E;
-}
-
-// The quench under SQS_JOB_QUENCH_STEPS: the reference's per-epoch polish
-// (seeded.cu:621-713) on the FP32 energy -- PRP+ conjugate directions
-// (beta = max(0, g.(g - g_old) / g_old.g_old), reset every 25 iterations), a
-// backtracking line search of up to 5 trials (step x 0.45) from a step that
-// grows 1.25x after a success (at most 0.15), and after a failed search a
-// restart from steepest descent at half the step; it stops at zero energy or
-// after `iters` iterations.  Every coordinate moves at most 0.1 per trial, so
-// the cell lists of the saved state stay valid for the trial energies (as in
-// quench_cta).  The direction's dot products are 64-bit integer sums of the
-// gradients quantized to units of 2^-14 (|g| < 2^24 units, 3n products below
-// 2^59 in all), so the result does not depend on the CTA's width.
-// Scratch: 4n float4 (gradient sums, saved state, direction, previous gradient).
-__device__ long long quench_cg_cta(const Rep& R, int n, Grid& g, float L, int iters, float4* scr, long long E,
-                                   long long* red) {
-    int4* acc = reinterpret_cast<int4*>(scr);
-    float4* saved = scr + n;
-    float4* dir = scr + 2 * n;
-    int4* gold = reinterpret_cast<int4*>(scr + 3 * n);
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        dir[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        gold[i] = make_int4(0, 0, 0, 0);
-    }
-    float step = 0.04f;
-    for (int it = 0; it < iters && E > 0; ++it) {
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            acc[i] = make_int4(0, 0, 0, 0);
-            saved[i] = make_float4(R.sq[i].x, R.sq[i].y, R.ang[i], 0.f);
-        }
-        __syncthreads();
-        for (int w = threadIdx.x; w < 9 * n; w += blockDim.x) {
-            const int i = w / 9, c = w - 9 * i;
-            const float4 P = R.sq[i];
-            int ax = 0, ay = 0, aa = 0;
-            if (c == 0) {
-                float wx = 0.f, wy = 0.f, wa = 0.f;
-                wall_energy_grad(P.x, P.y, P.z, P.w, L, wx, wy, wa);
-                ax = qg(wx);
-                ay = qg(wy);
-                aa = qg(wa);
-            }
-            const int x = g.cx(P.x) + c % 3 - 1, y = g.cx(P.y) + c / 3 - 1;
-            if (x >= 0 && x < g.G && y >= 0 && y < g.G) {
-                const int cell = y * g.G + x, m = R.cnt[cell];
-                for (int k = 0; k < m; ++k) {
-                    const int j = R.slot[cell * kCellK + k];
-                    if (j == i) continue;
-                    const float4 Q = R.sq[j];
-                    const float ex = Q.x - P.x, ey = Q.y - P.y;
-                    if (ex * ex + ey * ey >= kPairCut2) continue;
-                    PairGrad pg;
-                    if (sat_pair_grad(ex, ey, P.z, P.w, Q.z, Q.w, pg)) {
-                        ax += qg(pg.px);
-                        ay += qg(pg.py);
-                        aa += qg(pg.pa);
-                    }
-                }
-            }
-            if (ax | ay | aa) {
-                atomicAdd(&acc[i].x, ax);
-                atomicAdd(&acc[i].y, ay);
-                atomicAdd(&acc[i].z, aa);
-            }
-        }
-        __syncthreads();
-        long long gg = 0, dgg = 0;
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            const int4 a = acc[i], o = gold[i];
-            const long long qx = a.x >> 6, qy = a.y >> 6, qz = a.z >> 6;
-            const long long ox = o.x >> 6, oy = o.y >> 6, oz = o.z >> 6;
-            gg += ox * ox + oy * oy + oz * oz;
-            dgg += (qx - ox) * qx + (qy - oy) * qy + (qz - oz) * qz;
-        }
-        gg = block_sum_ll(gg, red);
-        dgg = block_sum_ll(dgg, red);
-        const float beta = (it == 0 || gg == 0 || it % 25 == 0) ? 0.f : fmaxf(0.f, (float)((double)dgg / (double)gg));
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            const int4 a = acc[i];
-            const float4 d = dir[i];
-            dir[i] = make_float4(-(float)a.x * (1.0f / kQScale) + beta * d.x, -(float)a.y * (1.0f / kQScale) + beta * d.y,
-                                 -(float)a.z * (1.0f / kQScale) + beta * d.z, 0.f);
-            gold[i] = a;
-        }
-        __syncthreads();
-        bool moved = false;
-        float alpha = step;
-        for (int ls = 0; ls < 5 && !moved; ++ls) {
-            for (int i = threadIdx.x; i < n; i += blockDim.x) {
-                const float4 d = dir[i], o = saved[i];
-                const float sx = fminf(0.1f, fmaxf(-0.1f, alpha * d.x));
-                const float sy = fminf(0.1f, fmaxf(-0.1f, alpha * d.y));
-                float a = o.z + fminf(0.1f, fmaxf(-0.1f, alpha * d.z));
-                a = a - kHalfPiF * floorf(a * (1.0f / kHalfPiF));
-                if (!(a >= 0.f && a < kHalfPiF)) a = 0.f;
-                float sn, cs;
-                state_trig(a, &sn, &cs);
-                R.sq[i] = make_float4(o.x + sx, o.y + sy, cs, sn);
-                R.ang[i] = a;
-            }
-            __syncthreads();
-            const long long En = full_energy_cta(R, n, g, L, red);
-            if (En < E && build_cells_cta(R, n, g)) {
-                E = En;
-                step = fminf(0.15f, alpha * 1.25f);
-                moved = true;
-            } else {
-                if (En < E) {  // the better state overflows a cell: lists back to the saved state
-                    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-                        const float4 o = saved[i];
-                        float sn, cs;
-                        state_trig(o.z, &sn, &cs);
-                        R.sq[i] = make_float4(o.x, o.y, cs, sn);
-                        R.ang[i] = o.z;
-                    }
-                    __syncthreads();
-                    build_cells_cta(R, n, g);  // the saved state fitted
-                }
-                alpha *= 0.45f;
-            }
-        }
-        if (!moved) {  // back to the saved state (its lists are current); steepest descent, half the step
-            for (int i = threadIdx.x; i < n; i += blockDim.x) {
-                const float4 o = saved[i];
-                float sn, cs;
-                state_trig(o.z, &sn, &cs);
-                R.sq[i] = make_float4(o.x, o.y, cs, sn);
-                R.ang[i] = o.z;
-                dir[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-            }
-            step = fmaxf(1e-7f, step * 0.5f);
-            __syncthreads();
         }
     }
     return E;
@@ -1179,13 +1047,11 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                 if (w == lr && lane == 0) S.qE = E;
                 __syncthreads();
                 const Rep cr = rep_view(dyn + lr * rb, n, jd.Gmax);
-                float4* qs = (int64_t)dyn_bytes >= (int64_t)Rl * rb + 64 * (int64_t)n
+                float4* qs = (int64_t)dyn_bytes >= (int64_t)Rl * rb + 32 * (int64_t)n
                                  ? reinterpret_cast<float4*>(dyn + (int64_t)Rl * rb)
                                  : pos + jd.scr_off;
                 const long long qe_out =
-                    jd.quench_stall == kQuenchCG
-                        ? quench_cg_cta(cr, n, g, S.wside[lr], jd.quench_iters, qs, S.qE, S.red)
-                        : quench_cta(cr, n, g, S.wside[lr], jd.quench_iters, jd.quench_stall, qs, qs + n, S.qE, S.red);
+                    quench_cta(cr, n, g, S.wside[lr], jd.quench_iters, jd.quench_stall, qs, qs + n, S.qE, S.red);
                 if (w == lr) E = qe_out;
                 __syncthreads();
             }
@@ -1199,14 +1065,11 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                 const Rep cr = rep_view(dyn + (cold % Rl) * rb, n, jd.Gmax);
                 // the quench's gradient sums and saved state: in shared memory
                 // after the replicas when the launch left room, else in HBM
-                float4* qs = (int64_t)dyn_bytes >= (int64_t)Rl * rb + 64 * (int64_t)n
+                float4* qs = (int64_t)dyn_bytes >= (int64_t)Rl * rb + 32 * (int64_t)n
                                  ? reinterpret_cast<float4*>(dyn + (int64_t)Rl * rb)
                                  : pos + jd.scr_off;
-                const long long qe_out =
-                    jd.quench_stall == kQuenchCG
-                        ? quench_cg_cta(cr, n, g, S.wside[cold % Rl], jd.quench_iters, qs, S.qE, S.red)
-                        : quench_cta(cr, n, g, S.wside[cold % Rl], jd.quench_iters, jd.quench_stall, qs, qs + n, S.qE,
-                                     S.red);
+                const long long qe_out = quench_cta(cr, n, g, S.wside[cold % Rl], jd.quench_iters, jd.quench_stall, qs,
+                                                    qs + n, S.qE, S.red);
                 if (w == cold % Rl) E = qe_out;
                 __syncthreads();
             }
@@ -1535,10 +1398,10 @@ int launch_anneal(cudaStream_t stream, int njobs, int cs, int Rl, size_t smem, b
 
 // Shared memory of a launch whose largest job needs rb bytes a replica and
 // has n_max squares: the replicas, plus room for the checkpoint quench's
-// scratch (4 n float4) when that fits and keeps as many clusters resident --
+// scratch (2 n float4) when that fits and keeps as many clusters resident --
 // the quench then runs on shared instead of global memory (same results).
 size_t anneal_smem(int cs, int Rl, int64_t rb, int n_max, bool moves) {
-    const size_t base = (size_t)(rb * Rl), with = base + 64 * (size_t)n_max;
+    const size_t base = (size_t)(rb * Rl), with = base + 32 * (size_t)n_max;
     if (with > kAnnealSmemLimit) return base;
     static std::mutex mu;
     static std::map<std::tuple<int, int, int, size_t, size_t, bool>, size_t> memo;
