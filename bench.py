@@ -405,8 +405,8 @@ def run_sqs(args, D: Dist):
         data="synthetic",
         config=dict(workload=f"SAT energy+gradient, {configs} configs x n={n}, FP32 cell list",
                     configs=configs, n=n, seed=SEED, side=float(s32[0]), l2="flushed before every launch",
-                    cta_threads=threads if threads > 0 else 32 * (-threads or 4),
-                    kernel_shape=(f"one warp per configuration, {-threads or 4} per CTA" if threads <= 0 and n <= 256
+                    cta_threads=threads if threads > 0 else 32 * (-threads or 2),
+                    kernel_shape=(f"one warp per configuration, {-threads or 2} per CTA" if threads <= 0 and n <= 256
                                   else "one CTA per configuration"),
                     parallelism=f"replicas x{D.world}", device=name, sm_count=sms),
         e2e=dict(value=e2e_val, unit=UNIT, h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h,
