@@ -299,11 +299,10 @@ __host__ __device__ inline size_t warp_smem_bytes(int n) {
 }
 
 // Pair-gradient sums of the warp kernel: one 32-bit integer per component in
-// units of 2^-19, started from the square's wall gradient.  A pair term is
-// bounded by 2 r_max (|d| + 1/sqrt 2) = 2 * 1.2071 * 2.1213 < 5.13 and a wall
-// term by a few units, so with n <= 256 (at most 255 partners) a sum stays
-// below 2^31 units; every term is rounded once (error < 1e-6) and the sum is
-// exact and order-free.
+// units of 2^-19.  A pair term is bounded by 2 r_max (|d| + 1/sqrt 2) =
+// 2 * 1.2071 * 2.1213 < 5.13, so with n <= 256 (at most 255 partners) a sum
+// stays below 2^31 units; every term is rounded once (error < 1e-6) and the
+// sum is exact and order-free.
 constexpr float kGScale = 524288.0f;
 
 // Energies of the warp kernel are summed as 64-bit integers in units of
@@ -376,11 +375,13 @@ __global__ void __launch_bounds__(W * 32, 28 / W) sat_energy_warp_kernel(int con
             sincosf(pa[k], &ps[k], &pc[k]);
             float gx = 0.f, gy = 0.f, ga = 0.f;
             e_loc += e_units(wall_energy_grad(px[k], py[k], pc[k], ps[k], L, gx, gy, ga));
-            // the wall gradient starts the square's integer sums (|term| < 2^3,
-            // so wall plus pairs stays below 2^31 units); one store at the end
-            gq[3 * i] = gq_units(gx);
-            gq[3 * i + 1] = gq_units(gy);
-            gq[3 * i + 2] = gq_units(ga);
+            if (gdst) {  // the wall term goes straight out (unbounded for squares far outside
+                         // the box); pair terms are added at the end
+                gdst[3 * i] = gx;
+                gdst[3 * i + 1] = gy;
+                gdst[3 * i + 2] = ga;
+            }
+            gq[3 * i] = gq[3 * i + 1] = gq[3 * i + 2] = 0;
             int cx = (int)floorf(px[k] * inv_cell), cy = (int)floorf(py[k] * inv_cell);
             cx = cx < 0 ? 0 : (cx >= G ? G - 1 : cx);
             cy = cy < 0 ? 0 : (cy >= G ? G - 1 : cy);
@@ -504,7 +505,7 @@ __global__ void __launch_bounds__(W * 32, 28 / W) sat_energy_warp_kernel(int con
         if (COUNT) cand[cfg] = cand_loc;
     }
     if (gdst) {
-        for (int k = lane; k < 3 * n; k += 32) gdst[k] = (float)gq[k] * (1.0f / kGScale);
+        for (int k = lane; k < 3 * n; k += 32) gdst[k] += (float)gq[k] * (1.0f / kGScale);
     }
 }
 
