@@ -186,7 +186,9 @@ typedef struct sqs_job {
  * those. */
 #define SQS_JOB_AUTOTUNE 1
 /* Move-set options, each a counterpart of the reference search's moves:
- *  ADAPT       step size per replica scaled by its rung (0.15 .. 2 x sigma
+ *  ADAPT       steps drawn uniform in +-sigma per coordinate and angle (the
+ *              reference's draws; Gaussian of deviation sigma without it),
+ *              step size per replica scaled by its rung (0.15 .. 2 x sigma
  *              from the coldest to the hottest rung), by an adaptation factor
  *              that every 16 proposals moves toward 25% acceptance
  *              (x exp((rate - 0.25) / 2), kept in [0.1, 4]), by 3.5 on every
@@ -225,11 +227,12 @@ typedef struct sqs_job {
  * device_certified_side :175-226; a dilation above 1.008 still rejects).
  * Costs one FP64 side measurement per replica per checkpoint. */
 #define SQS_JOB_CERT_ALL 64
-/* Checkpoint quench budget, k = 1..127: up to 16 k gradient iterations per
- * quench, ending only at zero overlap or when no trial step improves, as the
- * reference's per-epoch polish runs its iterations uninterrupted
- * (seeded.cu:621-713).  k = 0: 64 iterations, also ending after three
- * accepted steps in a row that each gained less than 0.1%. */
+/* Checkpoint quench budget, k = 1..127: up to 16 k conjugate-gradient
+ * iterations per quench, ending only at zero overlap or a zero gradient (a
+ * line search that finds no lower energy drops the direction, halves the
+ * step and goes on), as the reference's per-epoch polish runs its iterations
+ * uninterrupted (seeded.cu:621-713).  k = 0: 64 iterations, also ending
+ * after three accepted steps in a row that each gained less than 0.1%. */
 #define SQS_JOB_QUENCH_STEPS(k) ((int32_t)(k) << 24)
 /* The reference search's target-side ladder (seeded.cu:474-481, 908-943): from
  * the first proposal every rung anneals in its own container below the best

@@ -238,7 +238,7 @@ int main(int argc, char** argv) {
             j.tmin = tmin;
             j.tmax = tmax;
             j.sigma_xy = mv;
-            j.sigma_a = std::min(1.0, 2.5 * mv);
+            j.sigma_a = std::min(1.0, 0.7 * mv);  // theta = 0.7 scale (seeded.cu:510, packing.cu:531)
             j.seed = rng_seed + 0x9E3779B97F4A7C15ull * (unsigned long long)k;
             j.xya = seed.data();
             j.xya_rep = starts.data() + 3 * (size_t)n * 8 * (size_t)k * (size_t)per_job;

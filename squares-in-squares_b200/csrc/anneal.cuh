@@ -13,6 +13,9 @@ constexpr float kCellSide = 1.59f;   // >= sqrt(2.000001) + largest centre move 
 constexpr float kCellSideMax = 2.2f; // largest cell side the autotuner tries
 constexpr float kMaxStep = 0.12f;    // clamp of each proposal coordinate
 constexpr int kMaxN = 1000;
+// float4 scratch per square of one checkpoint quench (gradient sums,
+// previous gradient, direction, saved state)
+constexpr int kQuenchScr = 4;
 // JobDev.quench_stall of SQS_JOB_QUENCH_STEPS jobs: no exit on slow progress.
 constexpr int32_t kQuenchNoStall = 0x7fffffff;
 
@@ -26,7 +29,7 @@ struct JobDev {
     uint64_t seed;
     int64_t pos_off;                  // float4 index of replica 0, square 0
     int64_t best_off;                 // double index of the best state (n x 3)
-    int64_t scr_off;                  // float4 index of the job's quench scratch (2n)
+    int64_t scr_off;                  // float4 index of the job's quench scratch (kQuenchScr n per CTA)
     int64_t props_total;              // proposals per replica in the job's budget
     int64_t xprops;                   // proposals per replica between checkpoints
     int32_t quench_iters, flags;      // gradient steps of a checkpoint quench (at most); kMove* bits

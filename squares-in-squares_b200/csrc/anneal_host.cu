@@ -131,7 +131,8 @@ int prepare_job(const sqs_job& J, int j, JobDev& d, JobMut& m, Plan& p, const Sh
     return SQS_OK;
 }
 
-int64_t job_pos_elems(const sqs_job& J) { return (int64_t)J.replicas * J.n + 2 * (int64_t)J.n; }
+// replicas, then the quench scratch of up to one CTA per replica
+int64_t job_pos_elems(const sqs_job& J) { return (int64_t)J.replicas * J.n * (1 + kQuenchScr); }
 
 int64_t job_props(const sqs_job& J) { return J.sweeps >= 0 ? (int64_t)J.sweeps * J.n : -(int64_t)J.sweeps; }
 

@@ -341,19 +341,35 @@ __device__ long long full_energy_cta(const Rep& R, int n, const Grid& g, float L
 constexpr float kQScale = 1048576.0f;
 __device__ __forceinline__ int qg(float v) { return __float2int_rn(v * kQScale); }
 
+__device__ __forceinline__ long long clamp_q24(int v) { return max(-(1 << 24), min(1 << 24, v)); }
+
 // The checkpoint quench of one replica (the coldest, or each one under
-// SQS_JOB_QUENCH_ALL) by the whole CTA, one thread per (square, neighbouring
-// cell) work item for the gradient and the energies: Jacobi gradient descent
-// on the overlap energy with a backtracking step (up to 6 trials per
-// iteration), at most `iters` iterations, ending early at zero energy, when
-// no trial improves, or after `stall_limit` accepted steps in a row that each
-// gained less than 0.1%.  Gradients and energies are integer sums, so the
-// result does not depend on the CTA's width.
-__device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters, int stall_limit, float4* grad,
-                                float4* saved, long long E, long long* red) {
-    float alpha = 0.05f;
+// SQS_JOB_QUENCH_ALL) by the whole CTA: the reference's conjugate-gradient
+// polish (seeded.cu:621-715) on the overlap energy.  Each iteration takes the
+// gradient (one thread per (square, neighbouring cell) work item), a
+// Polak-Ribiere direction d = -g + beta d (beta = max(0, (g - g_old).g /
+// g_old.g), 0 on the first iteration and every 25th), and a backtracking
+// line search of up to 5 trials from the carried step (x 0.45 per trial).
+// An accepted trial sets the step to min(0.15, 1.25 alpha); when no trial
+// improves, the state goes back, the direction is dropped and the step
+// halves (at least 1e-7) -- the polish goes on, it does not stop there.  It
+// ends at zero energy, at a zero gradient, after `iters` iterations, or after
+// `stall_limit` accepted steps in a row that each gained less than 0.1%.
+// Gradients and their dot products are integer sums, so the result does not
+// depend on the CTA's width.  Scratch: kQuenchScr n float4 (gradient sums,
+// previous gradient, direction, saved state).
+__device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters, int stall_limit, float4* scr,
+                                long long E, long long* red) {
+    int4* acc = reinterpret_cast<int4*>(scr);       // gradient sums of this iteration
+    int4* gold = reinterpret_cast<int4*>(scr + n);  // the previous iteration's
+    float4* dir = scr + 2 * n;                      // search direction
+    float4* saved = scr + 3 * n;                    // state before the line search
+    float step = 0.04f;
     int stall = 0;  // consecutive accepted steps that gained less than 0.1%
-    int4* acc = reinterpret_cast<int4*>(grad);  // the gradient buffer holds the integer sums first
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        gold[i] = make_int4(0, 0, 0, 0);
+        dir[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
     for (int it = 0; it < iters && E > 0; ++it) {
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
             acc[i] = make_int4(0, 0, 0, 0);
@@ -396,10 +412,31 @@ __device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters
             }
         }
         __syncthreads();
+        // Polak-Ribiere: g_old.g_old, (g - g_old).g and g.g as exact integer
+        // sums of components clamped to 2^24 (a gradient of 16; only beta
+        // sees the clamp): 3 n <= 3000 terms below 2^49 each fit 64 bits
+        long long s_oo = 0, s_dg = 0, s_gg = 0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const int4 a = acc[i], o = gold[i];
+            const long long gx = clamp_q24(a.x), gy = clamp_q24(a.y), ga = clamp_q24(a.z);
+            const long long ox = clamp_q24(o.x), oy = clamp_q24(o.y), oa = clamp_q24(o.z);
+            s_oo += ox * ox + oy * oy + oa * oa;
+            s_dg += (gx - ox) * gx + (gy - oy) * gy + (ga - oa) * ga;
+            s_gg += gx * gx + gy * gy + ga * ga;
+        }
+        s_oo = block_sum_ll(s_oo, red);
+        s_dg = block_sum_ll(s_dg, red);
+        s_gg = block_sum_ll(s_gg, red);
+        const float beta =
+            (it == 0 || s_oo == 0 || it % 25 == 0) ? 0.f : fmaxf(0.f, (float)((double)s_dg / (double)s_oo));
+        if (s_gg == 0 && beta == 0.f) break;  // no direction left at the sums' resolution
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
             const int4 a = acc[i];
-            grad[i] = make_float4((float)a.x * (1.0f / kQScale), (float)a.y * (1.0f / kQScale),
-                                  (float)a.z * (1.0f / kQScale), 0.f);
+            const float4 d0 = dir[i];
+            dir[i] = make_float4(__fmaf_rn(beta, d0.x, -(float)a.x * (1.0f / kQScale)),
+                                 __fmaf_rn(beta, d0.y, -(float)a.y * (1.0f / kQScale)),
+                                 __fmaf_rn(beta, d0.z, -(float)a.z * (1.0f / kQScale)), 0.f);
+            gold[i] = a;
         }
         __syncthreads();
         // Trial steps move every coordinate by at most 0.1, so each partner
@@ -407,18 +444,19 @@ __device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters
         // 3 x 3 cells around it on the lists built for the saved state
         // (1.4142 + 0.1 < 1.59 <= cell side): trial energies use those lists,
         // and the lists are rebuilt only for an accepted step.
+        float alpha = step;
         bool moved = false;
-        for (int tries = 0; tries < 6 && !moved; ++tries) {
+        for (int tries = 0; tries < 5 && !moved; ++tries) {
             for (int i = threadIdx.x; i < n; i += blockDim.x) {
-                const float4 d = grad[i], o = saved[i];
+                const float4 d = dir[i], o = saved[i];
                 const float sx = fminf(0.1f, fmaxf(-0.1f, alpha * d.x));
                 const float sy = fminf(0.1f, fmaxf(-0.1f, alpha * d.y));
-                float a = o.z - fminf(0.1f, fmaxf(-0.1f, alpha * d.z));
+                float a = o.z + fminf(0.1f, fmaxf(-0.1f, alpha * d.z));
                 a = a - kHalfPiF * floorf(a * (1.0f / kHalfPiF));
                 if (!(a >= 0.f && a < kHalfPiF)) a = 0.f;
                 float sn, cs;
                 state_trig(a, &sn, &cs);
-                R.sq[i] = make_float4(o.x - sx, o.y - sy, cs, sn);
+                R.sq[i] = make_float4(o.x + sx, o.y + sy, cs, sn);
                 R.ang[i] = a;
             }
             __syncthreads();
@@ -426,7 +464,7 @@ __device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters
             if (En < E && build_cells_cta(R, n, g)) {
                 stall = En > E - E / 1000 ? stall + 1 : 0;  // less than 0.1% gained
                 E = En;
-                alpha = fminf(alpha * 1.3f, 0.2f);
+                step = fminf(0.15f, alpha * 1.25f);
                 moved = true;
             } else {
                 if (En < E) {  // the better state overflows a cell: lists back to the saved state
@@ -440,22 +478,22 @@ __device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters
                     __syncthreads();
                     build_cells_cta(R, n, g);  // the saved state fitted
                 }
-                alpha *= 0.3f;
+                alpha *= 0.45f;
             }
         }
-        if (!moved || stall >= stall_limit) {
-            if (!moved) {  // no improvement: restore the saved state (its lists are current)
-                for (int i = threadIdx.x; i < n; i += blockDim.x) {
-                    const float4 o = saved[i];
-                    float sn, cs;
-                    state_trig(o.z, &sn, &cs);
-                    R.sq[i] = make_float4(o.x, o.y, cs, sn);
-                    R.ang[i] = o.z;
-                }
-                __syncthreads();
+        if (!moved) {  // back to the saved state (its lists are current), direction dropped
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                const float4 o = saved[i];
+                float sn, cs;
+                state_trig(o.z, &sn, &cs);
+                R.sq[i] = make_float4(o.x, o.y, cs, sn);
+                R.ang[i] = o.z;
+                dir[i] = make_float4(0.f, 0.f, 0.f, 0.f);
             }
-            break;
+            step = fmaxf(1e-7f, step * 0.5f);
+            __syncthreads();
         }
+        if (stall >= stall_limit) break;
     }
     return E;
 }
@@ -836,14 +874,22 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                     const U4 ra = philox4x32_10(U4{(uint32_t)ev, (uint32_t)(ev >> 32), (uint32_t)r, 0u}, k0, k1);
                     const U4 rb = philox4x32_10(U4{(uint32_t)ev, (uint32_t)(ev >> 32), (uint32_t)r, 1u}, k0, k1);
                     di = (int)(((uint64_t)ra.x * (uint64_t)n) >> 32);
-                    const float rad1 = sqrtf(-2.f * __logf(u01(ra.y)));
-                    float sn1, cs1;
-                    __sincosf(6.2831853f * u01(ra.z), &sn1, &cs1);
-                    const float rad2 = sqrtf(-2.f * __logf(u01(ra.w)));
-                    const float n2 = rad2 * __cosf(6.2831853f * u01(rb.x));
-                    ddx = jd.sigma_xy * rad1 * cs1;
-                    ddy = jd.sigma_xy * rad1 * sn1;
-                    dda = jd.sigma_a * n2;
+                    if (adaptive) {
+                        // the reference search's steps: uniform in +-sigma
+                        // for each coordinate and the angle (seeded.cu:508-510)
+                        ddx = jd.sigma_xy * (2.f * u01(ra.y) - 1.f);
+                        ddy = jd.sigma_xy * (2.f * u01(ra.z) - 1.f);
+                        dda = jd.sigma_a * (2.f * u01(ra.w) - 1.f);
+                    } else {
+                        const float rad1 = sqrtf(-2.f * __logf(u01(ra.y)));
+                        float sn1, cs1;
+                        __sincosf(6.2831853f * u01(ra.z), &sn1, &cs1);
+                        const float rad2 = sqrtf(-2.f * __logf(u01(ra.w)));
+                        const float n2 = rad2 * __cosf(6.2831853f * u01(rb.x));
+                        ddx = jd.sigma_xy * rad1 * cs1;
+                        ddy = jd.sigma_xy * rad1 * sn1;
+                        dda = jd.sigma_a * n2;
+                    }
                     du = u01(rb.y);
                     if (MOVES && (jd.flags & kMoveCollective)) di |= (int)(rb.z % 7u) << 16;  // move mode
                 }
@@ -1041,17 +1087,20 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
         // the replica on the coldest rung (every replica under
         // SQS_JOB_QUENCH_ALL) is quenched toward zero overlap by every thread
         // of the CTA that holds it
+        // the quench's scratch (kQuenchScr n float4): in shared memory after
+        // the replicas when the launch left room, else this CTA's own block
+        // of the job's scratch in HBM (every CTA may quench at once)
+        float4* qs = (int64_t)dyn_bytes >= (int64_t)Rl * rb + (int64_t)sizeof(float4) * kQuenchScr * n
+                         ? reinterpret_cast<float4*>(dyn + (int64_t)Rl * rb)
+                         : pos + jd.scr_off + (int64_t)rank * kQuenchScr * n;
         if (MOVES && (jd.flags & kMoveQuenchAll) && jd.quench_iters > 0) {
             // every replica of the CTA, one after another, by every thread
             for (int lr = 0; lr < Rl; ++lr) {
                 if (w == lr && lane == 0) S.qE = E;
                 __syncthreads();
                 const Rep cr = rep_view(dyn + lr * rb, n, jd.Gmax);
-                float4* qs = (int64_t)dyn_bytes >= (int64_t)Rl * rb + 32 * (int64_t)n
-                                 ? reinterpret_cast<float4*>(dyn + (int64_t)Rl * rb)
-                                 : pos + jd.scr_off;
                 const long long qe_out =
-                    quench_cta(cr, n, g, S.wside[lr], jd.quench_iters, jd.quench_stall, qs, qs + n, S.qE, S.red);
+                    quench_cta(cr, n, g, S.wside[lr], jd.quench_iters, jd.quench_stall, qs, S.qE, S.red);
                 if (w == lr) E = qe_out;
                 __syncthreads();
             }
@@ -1063,13 +1112,8 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                 if (w == cold % Rl && lane == 0) S.qE = E;
                 __syncthreads();
                 const Rep cr = rep_view(dyn + (cold % Rl) * rb, n, jd.Gmax);
-                // the quench's gradient sums and saved state: in shared memory
-                // after the replicas when the launch left room, else in HBM
-                float4* qs = (int64_t)dyn_bytes >= (int64_t)Rl * rb + 32 * (int64_t)n
-                                 ? reinterpret_cast<float4*>(dyn + (int64_t)Rl * rb)
-                                 : pos + jd.scr_off;
-                const long long qe_out = quench_cta(cr, n, g, S.wside[cold % Rl], jd.quench_iters, jd.quench_stall, qs,
-                                                    qs + n, S.qE, S.red);
+                const long long qe_out =
+                    quench_cta(cr, n, g, S.wside[cold % Rl], jd.quench_iters, jd.quench_stall, qs, S.qE, S.red);
                 if (w == cold % Rl) E = qe_out;
                 __syncthreads();
             }
@@ -1398,10 +1442,10 @@ int launch_anneal(cudaStream_t stream, int njobs, int cs, int Rl, size_t smem, b
 
 // Shared memory of a launch whose largest job needs rb bytes a replica and
 // has n_max squares: the replicas, plus room for the checkpoint quench's
-// scratch (2 n float4) when that fits and keeps as many clusters resident --
+// scratch (kQuenchScr n float4) when that fits and keeps as many clusters resident --
 // the quench then runs on shared instead of global memory (same results).
 size_t anneal_smem(int cs, int Rl, int64_t rb, int n_max, bool moves) {
-    const size_t base = (size_t)(rb * Rl), with = base + 32 * (size_t)n_max;
+    const size_t base = (size_t)(rb * Rl), with = base + sizeof(float4) * kQuenchScr * (size_t)n_max;
     if (with > kAnnealSmemLimit) return base;
     static std::mutex mu;
     static std::map<std::tuple<int, int, int, size_t, size_t, bool>, size_t> memo;

@@ -175,7 +175,7 @@ double seconds_since(std::chrono::steady_clock::time_point t0) {
 // [0, pi/2) in double first -- the host's init_replicas, bit for bit (fmod is
 // exact, the conversions round to nearest) -- and the quench scratch zeroed.
 __global__ void init_replicas_kernel(const double* __restrict__ xya, int n, int R, float4* __restrict__ dst) {
-    const int64_t total = (int64_t)R * n + 2 * (int64_t)n;
+    const int64_t total = (int64_t)R * n * (1 + kQuenchScr);
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
         if (k >= (int64_t)R * n) {
             dst[k] = make_float4(0.f, 0.f, 0.f, 0.f);
