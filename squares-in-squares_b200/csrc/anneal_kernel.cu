@@ -275,12 +275,38 @@ __device__ double cert_side(const Rep& R, int n, const Grid& g, int lane, double
     return fmax(__dsub_rn(bx1, bx0), __dsub_rn(by1, by0));
 }
 
-// ---- CTA-cooperative forms (every thread of the CTA works on one replica)
-__device__ bool build_cells_cta(const Rep& R, int n, const Grid& g) {
-    const int ncell = g.G * g.G, tid = threadIdx.x, nt = blockDim.x;
+__device__ long long block_sum_ll(long long v, long long* red);
+
+// ---- Cooperative forms: a group of threads works on one replica, either
+// the whole CTA (CtaGrp) or one warp (WarpGrp).  Results do not depend on the
+// group: every sum below is an integer sum and slot order within a cell list
+// changes no energy, gradient or decision.
+struct CtaGrp {
+    long long* red;  // one slot per warp of the CTA
+    __device__ __forceinline__ int t() const { return threadIdx.x; }
+    __device__ __forceinline__ int nt() const { return blockDim.x; }
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
+    __device__ __forceinline__ bool sync_or(bool p) const { return __syncthreads_or(p); }
+    __device__ __forceinline__ long long sum(long long v) const { return block_sum_ll(v, red); }
+};
+struct WarpGrp {
+    int lane;
+    __device__ __forceinline__ int t() const { return lane; }
+    __device__ __forceinline__ int nt() const { return 32; }
+    __device__ __forceinline__ void sync() const { __syncwarp(); }
+    __device__ __forceinline__ bool sync_or(bool p) const {
+        __syncwarp();
+        return __any_sync(0xffffffffu, p);
+    }
+    __device__ __forceinline__ long long sum(long long v) const { return warp_sum_ll(v); }
+};
+
+template <class Grp>
+__device__ bool build_cells_grp(const Grp& gp, const Rep& R, int n, const Grid& g) {
+    const int ncell = g.G * g.G, tid = gp.t(), nt = gp.nt();
     for (int c = tid; c < ncell; c += nt) R.cnt[c] = 0;
     for (int k = tid; k < ncell * kCellK; k += nt) R.slot[k] = 0;
-    __syncthreads();
+    gp.sync();
     bool ok = true;
     for (int i = tid; i < n; i += nt) {
         const float4 p = R.sq[i];
@@ -290,11 +316,11 @@ __device__ bool build_cells_cta(const Rep& R, int n, const Grid& g) {
         if (slot_k < (unsigned)kCellK) R.slot[c * kCellK + slot_k] = (uint16_t)i;
         else ok = false;
     }
-    const bool bad = __syncthreads_or(!ok);
+    const bool bad = gp.sync_or(!ok);
     if (bad) {
         for (int c = tid; c < ncell; c += nt)
             if (R.cnt[c] > kCellK) R.cnt[c] = (uint8_t)kCellK;
-        __syncthreads();
+        gp.sync();
     }
     return !bad;
 }
@@ -314,9 +340,10 @@ __device__ long long block_sum_ll(long long v, long long* red) {
 // against the squares listed in cell w % 9 of its 3 x 3 block (each pair
 // counted from its lower index), so a small replica still spreads over
 // many threads.
-__device__ long long full_energy_cta(const Rep& R, int n, const Grid& g, float L, long long* red) {
+template <class Grp>
+__device__ long long full_energy_grp(const Grp& gp, const Rep& R, int n, const Grid& g, float L) {
     long long e = 0;
-    for (int w = threadIdx.x; w < 9 * n; w += blockDim.x) {
+    for (int w = gp.t(); w < 9 * n; w += gp.nt()) {
         const int i = w / 9, c = w - 9 * i;
         const float4 P = R.sq[i];
         if (c == 0) e += qe(wall_e(P.x, P.y, P.z, P.w, L));
@@ -331,7 +358,7 @@ __device__ long long full_energy_cta(const Rep& R, int n, const Grid& g, float L
             if (dx * dx + dy2 * dy2 < kPairCut2) e += qe(sat_pair_energy(dx, dy2, P.z, P.w, Q.z, Q.w));
         }
     }
-    return block_sum_ll(e, red);
+    return gp.sum(e);
 }
 
 // Quench gradient sums: 32-bit integers in units of 2^-20.  A square's 3 x 3
@@ -344,7 +371,7 @@ __device__ __forceinline__ int qg(float v) { return __float2int_rn(v * kQScale);
 __device__ __forceinline__ long long clamp_q24(int v) { return max(-(1 << 24), min(1 << 24, v)); }
 
 // The checkpoint quench of one replica (the coldest, or each one under
-// SQS_JOB_QUENCH_ALL) by the whole CTA: the reference's conjugate-gradient
+// SQS_JOB_QUENCH_ALL) by a group of threads: the reference's conjugate-gradient
 // polish (seeded.cu:621-715) on the overlap energy.  Each iteration takes the
 // gradient (one thread per (square, neighbouring cell) work item), a
 // Polak-Ribiere direction d = -g + beta d (beta = max(0, (g - g_old).g /
@@ -356,28 +383,29 @@ __device__ __forceinline__ long long clamp_q24(int v) { return max(-(1 << 24), m
 // ends at zero energy, at a zero gradient, after `iters` iterations, or after
 // `stall_limit` accepted steps in a row that each gained less than 0.1%.
 // Gradients and their dot products are integer sums, so the result does not
-// depend on the CTA's width.  Scratch: kQuenchScr n float4 (gradient sums,
+// depend on the group's width.  Scratch: kQuenchScr n float4 (gradient sums,
 // previous gradient, direction, saved state).
-__device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters, int stall_limit, float4* scr,
-                                long long E, long long* red) {
+template <class Grp>
+__device__ long long quench_grp(const Grp& gp, const Rep& R, int n, const Grid& g, float L, int iters, int stall_limit,
+                                float4* scr, long long E) {
     int4* acc = reinterpret_cast<int4*>(scr);       // gradient sums of this iteration
     int4* gold = reinterpret_cast<int4*>(scr + n);  // the previous iteration's
     float4* dir = scr + 2 * n;                      // search direction
     float4* saved = scr + 3 * n;                    // state before the line search
     float step = 0.04f;
     int stall = 0;  // consecutive accepted steps that gained less than 0.1%
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    for (int i = gp.t(); i < n; i += gp.nt()) {
         gold[i] = make_int4(0, 0, 0, 0);
         dir[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     for (int it = 0; it < iters && E > 0; ++it) {
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        for (int i = gp.t(); i < n; i += gp.nt()) {
             acc[i] = make_int4(0, 0, 0, 0);
             saved[i] = make_float4(R.sq[i].x, R.sq[i].y, R.ang[i], 0.f);
         }
-        __syncthreads();
+        gp.sync();
         // work item w: square w / 9 against cell w % 9 of its block
-        for (int w = threadIdx.x; w < 9 * n; w += blockDim.x) {
+        for (int w = gp.t(); w < 9 * n; w += gp.nt()) {
             const int i = w / 9, c = w - 9 * i;
             const float4 P = R.sq[i];
             int ax = 0, ay = 0, aa = 0;
@@ -411,12 +439,12 @@ __device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters
                 atomicAdd(&acc[i].z, aa);
             }
         }
-        __syncthreads();
+        gp.sync();
         // Polak-Ribiere: g_old.g_old, (g - g_old).g and g.g as exact integer
         // sums of components clamped to 2^24 (a gradient of 16; only beta
         // sees the clamp): 3 n <= 3000 terms below 2^49 each fit 64 bits
         long long s_oo = 0, s_dg = 0, s_gg = 0;
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        for (int i = gp.t(); i < n; i += gp.nt()) {
             const int4 a = acc[i], o = gold[i];
             const long long gx = clamp_q24(a.x), gy = clamp_q24(a.y), ga = clamp_q24(a.z);
             const long long ox = clamp_q24(o.x), oy = clamp_q24(o.y), oa = clamp_q24(o.z);
@@ -424,13 +452,13 @@ __device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters
             s_dg += (gx - ox) * gx + (gy - oy) * gy + (ga - oa) * ga;
             s_gg += gx * gx + gy * gy + ga * ga;
         }
-        s_oo = block_sum_ll(s_oo, red);
-        s_dg = block_sum_ll(s_dg, red);
-        s_gg = block_sum_ll(s_gg, red);
+        s_oo = gp.sum(s_oo);
+        s_dg = gp.sum(s_dg);
+        s_gg = gp.sum(s_gg);
         const float beta =
             (it == 0 || s_oo == 0 || it % 25 == 0) ? 0.f : fmaxf(0.f, (float)((double)s_dg / (double)s_oo));
         if (s_gg == 0 && beta == 0.f) break;  // no direction left at the sums' resolution
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        for (int i = gp.t(); i < n; i += gp.nt()) {
             const int4 a = acc[i];
             const float4 d0 = dir[i];
             dir[i] = make_float4(__fmaf_rn(beta, d0.x, -(float)a.x * (1.0f / kQScale)),
@@ -438,7 +466,7 @@ __device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters
                                  __fmaf_rn(beta, d0.z, -(float)a.z * (1.0f / kQScale)), 0.f);
             gold[i] = a;
         }
-        __syncthreads();
+        gp.sync();
         // Trial steps move every coordinate by at most 0.1, so each partner
         // within the pair cut-off of a moved square still sits in one of the
         // 3 x 3 cells around it on the lists built for the saved state
@@ -447,7 +475,7 @@ __device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters
         float alpha = step;
         bool moved = false;
         for (int tries = 0; tries < 5 && !moved; ++tries) {
-            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            for (int i = gp.t(); i < n; i += gp.nt()) {
                 const float4 d = dir[i], o = saved[i];
                 const float sx = fminf(0.1f, fmaxf(-0.1f, alpha * d.x));
                 const float sy = fminf(0.1f, fmaxf(-0.1f, alpha * d.y));
@@ -459,30 +487,30 @@ __device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters
                 R.sq[i] = make_float4(o.x + sx, o.y + sy, cs, sn);
                 R.ang[i] = a;
             }
-            __syncthreads();
-            const long long En = full_energy_cta(R, n, g, L, red);
-            if (En < E && build_cells_cta(R, n, g)) {
+            gp.sync();
+            const long long En = full_energy_grp(gp, R, n, g, L);
+            if (En < E && build_cells_grp(gp, R, n, g)) {
                 stall = En > E - E / 1000 ? stall + 1 : 0;  // less than 0.1% gained
                 E = En;
                 step = fminf(0.15f, alpha * 1.25f);
                 moved = true;
             } else {
                 if (En < E) {  // the better state overflows a cell: lists back to the saved state
-                    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                    for (int i = gp.t(); i < n; i += gp.nt()) {
                         const float4 o = saved[i];
                         float sn, cs;
                         state_trig(o.z, &sn, &cs);
                         R.sq[i] = make_float4(o.x, o.y, cs, sn);
                         R.ang[i] = o.z;
                     }
-                    __syncthreads();
-                    build_cells_cta(R, n, g);  // the saved state fitted
+                    gp.sync();
+                    build_cells_grp(gp, R, n, g);  // the saved state fitted
                 }
                 alpha *= 0.45f;
             }
         }
         if (!moved) {  // back to the saved state (its lists are current), direction dropped
-            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            for (int i = gp.t(); i < n; i += gp.nt()) {
                 const float4 o = saved[i];
                 float sn, cs;
                 state_trig(o.z, &sn, &cs);
@@ -491,7 +519,7 @@ __device__ long long quench_cta(const Rep& R, int n, Grid& g, float L, int iters
                 dir[i] = make_float4(0.f, 0.f, 0.f, 0.f);
             }
             step = fmaxf(1e-7f, step * 0.5f);
-            __syncthreads();
+            gp.sync();
         }
         if (stall >= stall_limit) break;
     }
@@ -1084,27 +1112,25 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
         // job's trajectory does not depend on how it is sliced.
         if (p_at != next_cp) break;  // the slice ends between checkpoints
         const bool xpoint = p_at % xp == 0;
-        // the replica on the coldest rung (every replica under
-        // SQS_JOB_QUENCH_ALL) is quenched toward zero overlap by every thread
-        // of the CTA that holds it
-        // the quench's scratch (kQuenchScr n float4): in shared memory after
-        // the replicas when the launch left room, else this CTA's own block
-        // of the job's scratch in HBM (every CTA may quench at once)
-        float4* qs = (int64_t)dyn_bytes >= (int64_t)Rl * rb + (int64_t)sizeof(float4) * kQuenchScr * n
-                         ? reinterpret_cast<float4*>(dyn + (int64_t)Rl * rb)
-                         : pos + jd.scr_off + (int64_t)rank * kQuenchScr * n;
         if (MOVES && (jd.flags & kMoveQuenchAll) && jd.quench_iters > 0) {
-            // every replica of the CTA, one after another, by every thread
-            for (int lr = 0; lr < Rl; ++lr) {
-                if (w == lr && lane == 0) S.qE = E;
-                __syncthreads();
-                const Rep cr = rep_view(dyn + lr * rb, n, jd.Gmax);
-                const long long qe_out =
-                    quench_cta(cr, n, g, S.wside[lr], jd.quench_iters, jd.quench_stall, qs, S.qE, S.red);
-                if (w == lr) E = qe_out;
-                __syncthreads();
+            // every replica at once, each by its own warp; the scratch
+            // (kQuenchScr n float4 a replica) in shared memory after the
+            // replicas when the launch left room for all of them, else the
+            // replica's own block of the job's scratch in HBM
+            if (active) {
+                float4* qw = (int64_t)dyn_bytes >= (int64_t)Rl * (rb + (int64_t)sizeof(float4) * kQuenchScr * n)
+                                 ? reinterpret_cast<float4*>(dyn + (int64_t)Rl * rb) + (int64_t)w * kQuenchScr * n
+                                 : pos + jd.scr_off + ((int64_t)rank * Rl + w) * kQuenchScr * n;
+                E = quench_grp(WarpGrp{lane}, rep, n, g, Lr, jd.quench_iters, jd.quench_stall, qw, E);
             }
+            __syncthreads();
         } else {
+            // the replica on the coldest rung, by every thread of the CTA that
+            // holds it; its scratch in shared memory after the replicas when
+            // the launch left room, else this CTA's block of the job's scratch
+            float4* qs = (int64_t)dyn_bytes >= (int64_t)Rl * rb + (int64_t)sizeof(float4) * kQuenchScr * n
+                             ? reinterpret_cast<float4*>(dyn + (int64_t)Rl * rb)
+                             : pos + jd.scr_off + (int64_t)rank * kQuenchScr * n;
             int cold = 0;
             for (int q = 0; q < R; ++q)
                 if (S.jm.perm[q] == 0) cold = q;
@@ -1112,8 +1138,8 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                 if (w == cold % Rl && lane == 0) S.qE = E;
                 __syncthreads();
                 const Rep cr = rep_view(dyn + (cold % Rl) * rb, n, jd.Gmax);
-                const long long qe_out =
-                    quench_cta(cr, n, g, S.wside[cold % Rl], jd.quench_iters, jd.quench_stall, qs, S.qE, S.red);
+                const long long qe_out = quench_grp(CtaGrp{S.red}, cr, n, g, S.wside[cold % Rl], jd.quench_iters,
+                                                    jd.quench_stall, qs, S.qE);
                 if (w == cold % Rl) E = qe_out;
                 __syncthreads();
             }
@@ -1442,26 +1468,35 @@ int launch_anneal(cudaStream_t stream, int njobs, int cs, int Rl, size_t smem, b
 
 // Shared memory of a launch whose largest job needs rb bytes a replica and
 // has n_max squares: the replicas, plus room for the checkpoint quench's
-// scratch (kQuenchScr n float4) when that fits and keeps as many clusters resident --
-// the quench then runs on shared instead of global memory (same results).
+// scratch (kQuenchScr n float4 per quench) when that fits and keeps as many
+// clusters resident -- the quench then runs on shared instead of global
+// memory (same results).  Launches with the move-set options first try room
+// for every replica's quench (SQS_JOB_QUENCH_ALL quenches them all at once),
+// then for one.
 size_t anneal_smem(int cs, int Rl, int64_t rb, int n_max, bool moves) {
-    const size_t base = (size_t)(rb * Rl), with = base + sizeof(float4) * kQuenchScr * (size_t)n_max;
-    if (with > kAnnealSmemLimit) return base;
+    const size_t base = (size_t)(rb * Rl), q1 = sizeof(float4) * kQuenchScr * (size_t)n_max;
+    const size_t one = base + q1, all = moves ? base + q1 * (size_t)Rl : one;
     static std::mutex mu;
     static std::map<std::tuple<int, int, int, size_t, size_t, bool>, size_t> memo;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return base;
-    const auto key = std::make_tuple(dev, cs, Rl, base, with, moves);
+    const auto key = std::make_tuple(dev, cs, Rl, base, all, moves);
     {
         std::lock_guard<std::mutex> lk(mu);
         auto it = memo.find(key);
         if (it != memo.end()) return it->second;
     }
-    int a = 0, b = 0;
+    int a = 0;
     size_t pick = base;
-    if (anneal_max_clusters(cs, Rl, base, moves, &a) == SQS_OK && anneal_max_clusters(cs, Rl, with, moves, &b) == SQS_OK &&
-        b >= a)
-        pick = with;
+    if (anneal_max_clusters(cs, Rl, base, moves, &a) == SQS_OK) {
+        for (const size_t cand : {all, one}) {
+            int b = 0;
+            if (cand <= kAnnealSmemLimit && anneal_max_clusters(cs, Rl, cand, moves, &b) == SQS_OK && b >= a) {
+                pick = cand;
+                break;
+            }
+        }
+    }
     std::lock_guard<std::mutex> lk(mu);
     memo[key] = pick;
     return pick;
