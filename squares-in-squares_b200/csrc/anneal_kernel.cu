@@ -300,6 +300,35 @@ struct WarpGrp {
     }
     __device__ __forceinline__ long long sum(long long v) const { return warp_sum_ll(v); }
 };
+// `nw` consecutive warps of the CTA (nw >= 2) on named barrier `id` (1..15).
+struct BarGrp {
+    int id, nw, t0;  // barrier, warps, first thread of the group
+    long long* red;  // one slot per warp of the group
+    __device__ __forceinline__ int t() const { return (int)threadIdx.x - t0; }
+    __device__ __forceinline__ int nt() const { return 32 * nw; }
+    __device__ __forceinline__ void sync() const {
+        asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(32 * nw) : "memory");
+    }
+    __device__ __forceinline__ bool sync_or(bool p) const {
+        unsigned r;
+        asm volatile(
+            "{\n\t.reg .pred ip, op;\n\tsetp.ne.u32 ip, %1, 0;\n\tbar.red.or.pred op, %2, %3, ip;\n\t"
+            "selp.u32 %0, 1, 0, op;\n\t}"
+            : "=r"(r)
+            : "r"((unsigned)p), "r"(id), "r"(32 * nw)
+            : "memory");
+        return r != 0;
+    }
+    __device__ __forceinline__ long long sum(long long v) const {
+        v = warp_sum_ll(v);
+        sync();  // every read of the slots by the previous sum is done
+        if ((threadIdx.x & 31) == 0) red[t() >> 5] = v;
+        sync();
+        long long s = 0;
+        for (int k = 0; k < nw; ++k) s += red[k];
+        return s;
+    }
+};
 
 template <class Grp>
 __device__ bool build_cells_grp(const Grp& gp, const Rep& R, int n, const Grid& g) {
@@ -779,6 +808,7 @@ struct CtaShared {
     unsigned long long props[kMaxRl], accs[kMaxRl];
     long long red[kMaxRl];
     long long qE;              // energy of the replica quenched by this CTA
+    long long qEv[kMaxRl];     // each replica's energy through a group quench
 };
 
 // MOVES: whether the move-set options (adaptation, collective moves, kicks)
@@ -1113,15 +1143,29 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
         if (p_at != next_cp) break;  // the slice ends between checkpoints
         const bool xpoint = p_at % xp == 0;
         if (MOVES && (jd.flags & kMoveQuenchAll) && jd.quench_iters > 0) {
-            // every replica at once, each by its own warp; the scratch
-            // (kQuenchScr n float4 a replica) in shared memory after the
-            // replicas when the launch left room for all of them, else the
-            // replica's own block of the job's scratch in HBM
-            if (active) {
-                float4* qw = (int64_t)dyn_bytes >= (int64_t)Rl * (rb + (int64_t)sizeof(float4) * kQuenchScr * n)
-                                 ? reinterpret_cast<float4*>(dyn + (int64_t)Rl * rb) + (int64_t)w * kQuenchScr * n
-                                 : pos + jd.scr_off + ((int64_t)rank * Rl + w) * kQuenchScr * n;
-                E = quench_grp(WarpGrp{lane}, rep, n, g, Lr, jd.quench_iters, jd.quench_stall, qw, E);
+            // every replica at once, each by its own group of gw warps (the
+            // launch gives each replica gw = blockDim / (32 Rl) warps); the
+            // scratch (kQuenchScr n float4 a replica) in shared memory after
+            // the replicas when the launch left room for all of them, else
+            // the replica's own block of the job's scratch in HBM
+            const int gw = (int)(blockDim.x >> 5) / Rl, q = w / gw;
+            const bool smem_scr = (int64_t)dyn_bytes >= (int64_t)Rl * (rb + (int64_t)sizeof(float4) * kQuenchScr * n);
+            float4* qw = smem_scr ? reinterpret_cast<float4*>(dyn + (int64_t)Rl * rb) + (int64_t)q * kQuenchScr * n
+                                  : pos + jd.scr_off + ((int64_t)rank * Rl + q) * kQuenchScr * n;
+            if (gw == 1) {
+                if (active) E = quench_grp(WarpGrp{lane}, rep, n, g, Lr, jd.quench_iters, jd.quench_stall, qw, E);
+            } else {
+                if (active && lane == 0) S.qEv[w] = E;
+                __syncthreads();
+                if (q < Rl) {
+                    const BarGrp gp{1 + q, gw, q * gw * 32, S.red + q * gw};
+                    const Rep cr = rep_view(dyn + q * rb, n, jd.Gmax);
+                    const long long e =
+                        quench_grp(gp, cr, n, g, S.wside[q], jd.quench_iters, jd.quench_stall, qw, S.qEv[q]);
+                    if (gp.t() == 0) S.qEv[q] = e;
+                }
+                __syncthreads();
+                if (active) E = S.qEv[w];
             }
             __syncthreads();
         } else {
@@ -1429,10 +1473,10 @@ int prime_anneal() {
 }
 
 static cudaLaunchConfig_t anneal_config(int clusters, int cs, int Rl, size_t smem, cudaStream_t stream,
-                                        cudaLaunchAttribute* attr) {
+                                        cudaLaunchAttribute* attr, int gw = 1) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(clusters * cs), 1, 1);
-    cfg.blockDim = dim3((unsigned)(Rl * 32), 1, 1);
+    cfg.blockDim = dim3((unsigned)(Rl * 32 * gw), 1, 1);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = stream;
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1444,23 +1488,62 @@ static cudaLaunchConfig_t anneal_config(int clusters, int cs, int Rl, size_t sme
     return cfg;
 }
 
-// Clusters of this shape that can be resident at once (one wave).
-int anneal_max_clusters(int cs, int Rl, size_t smem, bool moves, int* out) {
+// Clusters of this shape (gw warps a replica) that can be resident at once
+// (one wave), memoized per device and shape.
+static int max_clusters_gw(int cs, int Rl, size_t smem, bool moves, int gw, int* out) {
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int, size_t, bool, int>, int> memo;
+    int dev = 0;
+    SQS_CUDA(cudaGetDevice(&dev));
+    const auto key = std::make_tuple(dev, cs, Rl, smem, moves, gw);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = memo.find(key);
+        if (it != memo.end()) {
+            *out = it->second;
+            return SQS_OK;
+        }
+    }
     if (int r = prime_anneal()) return r;
     cudaLaunchAttribute attr[1];
-    const cudaLaunchConfig_t cfg = anneal_config(1, cs, Rl, smem, nullptr, attr);
+    const cudaLaunchConfig_t cfg = anneal_config(1, cs, Rl, smem, nullptr, attr, gw);
     int num = 0;
     if (moves) SQS_CUDA(cudaOccupancyMaxActiveClusters(&num, anneal_kernel<true>, &cfg));
     else SQS_CUDA(cudaOccupancyMaxActiveClusters(&num, anneal_kernel<false>, &cfg));
+    std::lock_guard<std::mutex> lk(mu);
+    memo[key] = num;
     *out = num;
     return SQS_OK;
+}
+
+int anneal_max_clusters(int cs, int Rl, size_t smem, bool moves, int* out) {
+    return max_clusters_gw(cs, Rl, smem, moves, 1, out);
+}
+
+// Warps a replica for a launch of njobs clusters: 1 (the replica's own warp),
+// or with the move-set options the most, up to kMaxRl / Rl, that keep as
+// many of the launch's clusters resident at once.  The extra warps idle
+// while their CTA anneals and join the checkpoint quench, which
+// SQS_JOB_QUENCH_ALL runs for every replica at once (same results: the
+// quench's sums are integers).
+static int quench_warps(int njobs, int cs, int Rl, size_t smem, bool moves) {
+    if (!moves || Rl >= kMaxRl) return 1;
+    int base = 0;
+    if (max_clusters_gw(cs, Rl, smem, moves, 1, &base) != SQS_OK) return 1;
+    const int need = std::min(njobs, base);
+    for (int gw = kMaxRl / Rl; gw > 1; gw /= 2) {
+        int m = 0;
+        if (max_clusters_gw(cs, Rl, smem, moves, gw, &m) == SQS_OK && m >= need) return gw;
+    }
+    return 1;
 }
 
 int launch_anneal(cudaStream_t stream, int njobs, int cs, int Rl, size_t smem, bool moves, const int32_t* job_list,
                   const JobDev* jdev, JobMut* jmut, float4* pos, double* best, int slice) {
     if (int r = prime_anneal()) return r;
     cudaLaunchAttribute attr[1];
-    const cudaLaunchConfig_t cfg = anneal_config(njobs, cs, Rl, smem, stream, attr);
+    const int gw = quench_warps(njobs, cs, Rl, smem, moves);
+    const cudaLaunchConfig_t cfg = anneal_config(njobs, cs, Rl, smem, stream, attr, gw);
     if (moves) SQS_CUDA(cudaLaunchKernelEx(&cfg, anneal_kernel<true>, job_list, jdev, jmut, pos, best, slice, (int)smem));
     else SQS_CUDA(cudaLaunchKernelEx(&cfg, anneal_kernel<false>, job_list, jdev, jmut, pos, best, slice, (int)smem));
     return SQS_OK;
