@@ -232,7 +232,8 @@ typedef struct sqs_job {
  * line search that finds no lower energy drops the direction, halves the
  * step and goes on), as the reference's per-epoch polish runs its iterations
  * uninterrupted (seeded.cu:621-713).  k = 0: 64 iterations, also ending
- * after three accepted steps in a row that each gained less than 0.1%. */
+ * at a line search without a gain or after three accepted steps in a row
+ * that each gained less than 0.1%. */
 #define SQS_JOB_QUENCH_STEPS(k) ((int32_t)(k) << 24)
 /* The reference search's target-side ladder (seeded.cu:474-481, 908-943): from
  * the first proposal every rung anneals in its own container below the best

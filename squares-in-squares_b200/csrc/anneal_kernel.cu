@@ -277,6 +277,29 @@ __device__ double cert_side(const Rep& R, int n, const Grid& g, int lane, double
 
 __device__ long long block_sum_ll(long long v, long long* red);
 
+// Three sums at once over the warps w < nw of a group whose warp partials
+// go to red[3 w .. 3 w + 2]; `sync` orders the slots' writes and reads.
+template <class Sync>
+__device__ __forceinline__ void group_sum3(long long& a, long long& b, long long& c, long long* red, int wg, int nw,
+                                           Sync&& sync) {
+    a = warp_sum_ll(a);
+    b = warp_sum_ll(b);
+    c = warp_sum_ll(c);
+    sync();
+    if ((threadIdx.x & 31) == 0) {
+        red[3 * wg] = a;
+        red[3 * wg + 1] = b;
+        red[3 * wg + 2] = c;
+    }
+    sync();
+    a = b = c = 0;
+    for (int k = 0; k < nw; ++k) {
+        a += red[3 * k];
+        b += red[3 * k + 1];
+        c += red[3 * k + 2];
+    }
+}
+
 // ---- Cooperative forms: a group of threads works on one replica, either
 // the whole CTA (CtaGrp) or one warp (WarpGrp).  Results do not depend on the
 // group: every sum below is an integer sum and slot order within a cell list
@@ -288,6 +311,9 @@ struct CtaGrp {
     __device__ __forceinline__ void sync() const { __syncthreads(); }
     __device__ __forceinline__ bool sync_or(bool p) const { return __syncthreads_or(p); }
     __device__ __forceinline__ long long sum(long long v) const { return block_sum_ll(v, red); }
+    __device__ __forceinline__ void sum3(long long& a, long long& b, long long& c) const {
+        group_sum3(a, b, c, red, (int)threadIdx.x >> 5, (int)(blockDim.x + 31) >> 5, [] { __syncthreads(); });
+    }
 };
 struct WarpGrp {
     int lane;
@@ -299,11 +325,16 @@ struct WarpGrp {
         return __any_sync(0xffffffffu, p);
     }
     __device__ __forceinline__ long long sum(long long v) const { return warp_sum_ll(v); }
+    __device__ __forceinline__ void sum3(long long& a, long long& b, long long& c) const {
+        a = warp_sum_ll(a);
+        b = warp_sum_ll(b);
+        c = warp_sum_ll(c);
+    }
 };
 // `nw` consecutive warps of the CTA (nw >= 2) on named barrier `id` (1..15).
 struct BarGrp {
     int id, nw, t0;  // barrier, warps, first thread of the group
-    long long* red;  // one slot per warp of the group
+    long long* red;  // three slots per warp of the group
     __device__ __forceinline__ int t() const { return (int)threadIdx.x - t0; }
     __device__ __forceinline__ int nt() const { return 32 * nw; }
     __device__ __forceinline__ void sync() const {
@@ -327,6 +358,9 @@ struct BarGrp {
         long long s = 0;
         for (int k = 0; k < nw; ++k) s += red[k];
         return s;
+    }
+    __device__ __forceinline__ void sum3(long long& a, long long& b, long long& c) const {
+        group_sum3(a, b, c, red, t() >> 5, nw, [this] { sync(); });
     }
 };
 
@@ -409,8 +443,9 @@ __device__ __forceinline__ long long clamp_q24(int v) { return max(-(1 << 24), m
 // An accepted trial sets the step to min(0.15, 1.25 alpha); when no trial
 // improves, the state goes back, the direction is dropped and the step
 // halves (at least 1e-7) -- the polish goes on, it does not stop there.  It
-// ends at zero energy, at a zero gradient, after `iters` iterations, or after
-// `stall_limit` accepted steps in a row that each gained less than 0.1%.
+// ends at zero energy, at a zero gradient, after `iters` iterations, or, with
+// a stall limit (not kQuenchNoStall), after `stall_limit` accepted steps in a
+// row that each gained less than 0.1% or at a line search without a gain.
 // Gradients and their dot products are integer sums, so the result does not
 // depend on the group's width.  Scratch: kQuenchScr n float4 (gradient sums,
 // previous gradient, direction, saved state).
@@ -481,9 +516,7 @@ __device__ long long quench_grp(const Grp& gp, const Rep& R, int n, const Grid& 
             s_dg += (gx - ox) * gx + (gy - oy) * gy + (ga - oa) * ga;
             s_gg += gx * gx + gy * gy + ga * ga;
         }
-        s_oo = gp.sum(s_oo);
-        s_dg = gp.sum(s_dg);
-        s_gg = gp.sum(s_gg);
+        gp.sum3(s_oo, s_dg, s_gg);
         const float beta =
             (it == 0 || s_oo == 0 || it % 25 == 0) ? 0.f : fmaxf(0.f, (float)((double)s_dg / (double)s_oo));
         if (s_gg == 0 && beta == 0.f) break;  // no direction left at the sums' resolution
@@ -549,6 +582,7 @@ __device__ long long quench_grp(const Grp& gp, const Rep& R, int n, const Grid& 
             }
             step = fmaxf(1e-7f, step * 0.5f);
             gp.sync();
+            if (stall_limit < kQuenchNoStall) break;  // the library's default quench ends here
         }
         if (stall >= stall_limit) break;
     }
@@ -806,7 +840,7 @@ struct CtaShared {
     int reset0;                // SQS_JOB_TARGETS: the gain resets every rung of ladder 0, not only heads
     float newL;
     unsigned long long props[kMaxRl], accs[kMaxRl];
-    long long red[kMaxRl];
+    long long red[3 * kMaxRl];   // group sums: up to three values a warp
     long long qE;              // energy of the replica quenched by this CTA
     long long qEv[kMaxRl];     // each replica's energy through a group quench
 };
@@ -1158,7 +1192,7 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                 if (active && lane == 0) S.qEv[w] = E;
                 __syncthreads();
                 if (q < Rl) {
-                    const BarGrp gp{1 + q, gw, q * gw * 32, S.red + q * gw};
+                    const BarGrp gp{1 + q, gw, q * gw * 32, S.red + 3 * q * gw};
                     const Rep cr = rep_view(dyn + q * rb, n, jd.Gmax);
                     const long long e =
                         quench_grp(gp, cr, n, g, S.wside[q], jd.quench_iters, jd.quench_stall, qw, S.qEv[q]);
