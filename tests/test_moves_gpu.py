@@ -185,3 +185,20 @@ def test_target_ladders_are_reproducible(ctx):
         assert mixed[k] == alone[k], ("mixed", k)
         assert sliced[k] == alone[k], ("sliced", k)
         assert wide[k] == alone[k], ("cluster 4", k)
+
+
+def test_group_quench_is_width_independent(ctx):
+    """Under SQS_JOB_QUENCH_ALL every replica is quenched at once by a group
+    of warps whose size the launch picks from how many clusters must stay
+    resident: up to four warps a replica for one job alone, fewer when 120
+    copies share the launch.  The quench's sums are integers, so every copy
+    ends exactly where the job alone does."""
+    from sqs.anneal import anneal_batch
+    job = _job(replicas=16, cluster=4, adapt=True, kick=True, quench_all=True, quench_steps=4, cert_all=True)
+    alone = anneal_batch([job], ctx=ctx)[0]
+    assert alone["status"] == 0, alone["reason"]
+    crowd = anneal_batch([job] * 120, ctx=ctx)
+    assert all(r["status"] == 0 for r in crowd)
+    for r in (crowd[0], crowd[57], crowd[-1]):
+        for k in KEYS:
+            assert r[k] == alone[k], k
