@@ -809,7 +809,8 @@ def main():
                       served=lambda: bench_served_sweep(ctx, args.served_rates, args.served_jobs,
                                                         args.served_sweeps, args.served_slice),
                       served_full=lambda: dict(served_10k=bench_served_budget(ctx, 24, 10000),
-                                               served_50k=bench_served_budget(ctx, 8, 50000, n_hi=100)),
+                                               served_50k=bench_served_budget(ctx, 8, 50000, n_hi=100),
+                                               served_50k_full_range=bench_served_budget(ctx, 16, 50000)),
                       plain_pt=lambda: bench_plain_pt(ctx),
                       batched=lambda: bench_batched(ctx, args.batched_sweeps, args.batched_instances),
                       batched_fixed=lambda: bench_batched_fixed(ctx, args.batched_sweeps, args.batched_instances),
