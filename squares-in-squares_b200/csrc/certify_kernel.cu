@@ -262,7 +262,7 @@ __device__ void fix_shfl_min_max(Fix<F>& v, bool& have, bool want_min) {
 
 // One CTA per packing: checks, side measurement, sort and sweep.
 template <int T, int NMAX>
-__global__ void __launch_bounds__(T) cert_packing_kernel(
+__global__ void __launch_bounds__(T, 512 / T) cert_packing_kernel(
     int count, const int32_t* __restrict__ bucket, const int32_t* __restrict__ pk_n,
     const int64_t* __restrict__ pk_sq0, const char* __restrict__ text, const int64_t* __restrict__ raw_off,
     const int32_t* __restrict__ raw_len, Lit* __restrict__ lits, PkOut* __restrict__ out,
