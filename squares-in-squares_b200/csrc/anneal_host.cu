@@ -627,7 +627,8 @@ static int anneal_run(sqs_ctx* ctx, const sqs_job* jobs, int njobs, int slice_sw
         }
         spans.push_back({lists.size(), kv.second.size()});
         lists.insert(lists.end(), kv.second.begin(), kv.second.end());
-        smems.push_back(anneal_smem(std::get<0>(kv.first), std::get<1>(kv.first), rb, nmax, std::get<2>(kv.first) != 0));
+        smems.push_back(anneal_smem(std::get<0>(kv.first), std::get<1>(kv.first), rb, nmax, std::get<2>(kv.first) != 0,
+                                    (int)kv.second.size()));
         keys.push_back(kv.first);
     }
     SQS_CUDA(cudaMemcpyAsync(d_list, lists.data(), sizeof(int32_t) * lists.size(), cudaMemcpyHostToDevice,

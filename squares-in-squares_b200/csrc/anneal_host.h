@@ -45,7 +45,7 @@ int launch_groups(sqs_ctx* ctx, const std::vector<Group>& groups, const JobDev* 
 int anneal_max_clusters(int cs, int Rl, size_t smem, bool moves, int* out);
 // Shared memory to launch with: the replicas, and the quench scratch when it fits
 // without lowering the resident clusters.
-size_t anneal_smem(int cs, int Rl, int64_t rb, int n_max, bool moves);
+size_t anneal_smem(int cs, int Rl, int64_t rb, int n_max, bool moves, int need = 1 << 30);
 int launch_anneal(cudaStream_t stream, int njobs, int cs, int Rl, size_t smem, bool moves, const int32_t* job_list,
                   const JobDev* jdev, JobMut* jmut, float4* pos, double* best, int slice);
 int launch_polish(cudaStream_t stream, int njobs, const int32_t* job_list, const JobDev* jdev, JobMut* jmut,

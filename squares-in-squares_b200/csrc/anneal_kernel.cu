@@ -1589,15 +1589,17 @@ int launch_anneal(cudaStream_t stream, int njobs, int cs, int Rl, size_t smem, b
 // clusters resident -- the quench then runs on shared instead of global
 // memory (same results).  Launches with the move-set options first try room
 // for every replica's quench (SQS_JOB_QUENCH_ALL quenches them all at once),
-// then for one.
-size_t anneal_smem(int cs, int Rl, int64_t rb, int n_max, bool moves) {
+// then for one.  `need` is how many clusters the launch must keep resident:
+// a size is taken when it keeps min(need, the clusters the bare replicas
+// allow) resident, so a launch of a few jobs always gets the room.
+size_t anneal_smem(int cs, int Rl, int64_t rb, int n_max, bool moves, int need) {
     const size_t base = (size_t)(rb * Rl), q1 = sizeof(float4) * kQuenchScr * (size_t)n_max;
     const size_t one = base + q1, all = moves ? base + q1 * (size_t)Rl : one;
     static std::mutex mu;
-    static std::map<std::tuple<int, int, int, size_t, size_t, bool>, size_t> memo;
+    static std::map<std::tuple<int, int, int, size_t, size_t, bool, int>, size_t> memo;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return base;
-    const auto key = std::make_tuple(dev, cs, Rl, base, all, moves);
+    const auto key = std::make_tuple(dev, cs, Rl, base, all, moves, need);
     {
         std::lock_guard<std::mutex> lk(mu);
         auto it = memo.find(key);
@@ -1608,7 +1610,8 @@ size_t anneal_smem(int cs, int Rl, int64_t rb, int n_max, bool moves) {
     if (anneal_max_clusters(cs, Rl, base, moves, &a) == SQS_OK) {
         for (const size_t cand : {all, one}) {
             int b = 0;
-            if (cand <= kAnnealSmemLimit && anneal_max_clusters(cs, Rl, cand, moves, &b) == SQS_OK && b >= a) {
+            if (cand <= kAnnealSmemLimit && anneal_max_clusters(cs, Rl, cand, moves, &b) == SQS_OK &&
+                b >= std::min(need, a)) {
                 pick = cand;
                 break;
             }

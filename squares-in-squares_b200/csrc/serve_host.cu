@@ -481,7 +481,7 @@ int launch_idle(sqs_server* s, const std::vector<int32_t>& fin, int& launched) {
         SQS_CUDA(cudaMemcpyAsync(c->d_list, list.data(), sizeof(int32_t) * (size_t)cnt, cudaMemcpyHostToDevice, c->st));
         if (int r = launch_anneal(c->st, cnt, std::get<0>(o.second), std::get<1>(o.second),
                                   anneal_smem(std::get<0>(o.second), std::get<1>(o.second), rb[o.second],
-                                              nmax[o.second], std::get<2>(o.second) != 0),
+                                              nmax[o.second], std::get<2>(o.second) != 0, cnt),
                                   std::get<2>(o.second) != 0, c->d_list,
                                   s->d_jd, s->d_jm, (float4*)s->arena, (double*)s->arena, std::max(1, s->slice)))
             return r;
