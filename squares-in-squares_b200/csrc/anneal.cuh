@@ -14,8 +14,9 @@ constexpr float kCellSideMax = 2.2f; // largest cell side the autotuner tries
 constexpr float kMaxStep = 0.12f;    // clamp of each proposal coordinate
 constexpr int kMaxN = 1000;
 // float4 scratch per square of one checkpoint quench (gradient sums,
-// previous gradient, direction, saved state)
-constexpr int kQuenchScr = 4;
+// previous gradient, direction, saved state, and 8 words a square for the
+// line search's pair list)
+constexpr int kQuenchScr = 6;
 // JobDev.quench_stall of SQS_JOB_QUENCH_STEPS jobs: no exit on slow progress.
 constexpr int32_t kQuenchNoStall = 0x7fffffff;
 

@@ -431,6 +431,31 @@ __device__ long long full_energy_grp(const Grp& gp, const Rep& R, int n, const G
 constexpr float kQScale = 1048576.0f;
 __device__ __forceinline__ int qg(float v) { return __float2int_rn(v * kQScale); }
 
+// Line-search pair list.  A trial moves every centre coordinate by at most
+// kListStep from the saved state; then a pair within the cut-off at the trial
+// was at most 1.4142 + 2 kListStep < 1.59 (the smallest cell side) apart per
+// axis at the saved state, so it sits in the saved 3 x 3 cell blocks, and at
+// most sqrt(kPairCut2) + 2 sqrt(2) kListStep = 1.6546 apart: the pairs of
+// those blocks closer than sqrt(kListCut2) = 1.6583 hold every pair with a
+// non-zero trial energy, and the list's energy equals the full one exactly.
+constexpr float kListStep = 0.085f, kListCut2 = 2.75f;
+
+template <class Grp>
+__device__ long long list_energy(const Grp& gp, const Rep& R, int n, float L, const uint32_t* pl, int cnt) {
+    long long e = 0;
+    for (int i = gp.t(); i < n; i += gp.nt()) {
+        const float4 P = R.sq[i];
+        e += qe(wall_e(P.x, P.y, P.z, P.w, L));
+    }
+    for (int k = gp.t(); k < cnt; k += gp.nt()) {
+        const uint32_t pr = pl[k];
+        const float4 P = R.sq[pr & 0xffffu], Q = R.sq[pr >> 16];
+        const float dx = Q.x - P.x, dy = Q.y - P.y;
+        if (dx * dx + dy * dy < kPairCut2) e += qe(sat_pair_energy(dx, dy, P.z, P.w, Q.z, Q.w));
+    }
+    return gp.sum(e);
+}
+
 __device__ __forceinline__ long long clamp_q24(int v) { return max(-(1 << 24), min(1 << 24, v)); }
 
 // The checkpoint quench of one replica (the coldest, or each one under
@@ -448,7 +473,8 @@ __device__ __forceinline__ long long clamp_q24(int v) { return max(-(1 << 24), m
 // row that each gained less than 0.1% or at a line search without a gain.
 // Gradients and their dot products are integer sums, so the result does not
 // depend on the group's width.  Scratch: kQuenchScr n float4 (gradient sums,
-// previous gradient, direction, saved state).
+// previous gradient, direction, saved state, pair list: a counter, the
+// largest direction component and up to 8 n - 2 pairs).
 template <class Grp>
 __device__ long long quench_grp(const Grp& gp, const Rep& R, int n, const Grid& g, float L, int iters, int stall_limit,
                                 float4* scr, long long E) {
@@ -456,6 +482,8 @@ __device__ long long quench_grp(const Grp& gp, const Rep& R, int n, const Grid& 
     int4* gold = reinterpret_cast<int4*>(scr + n);  // the previous iteration's
     float4* dir = scr + 2 * n;                      // search direction
     float4* saved = scr + 3 * n;                    // state before the line search
+    uint32_t* plist = reinterpret_cast<uint32_t*>(scr + 4 * n);  // [0] count, [1] max |d|, pairs
+    const int pcap = 8 * n - 2;
     float step = 0.04f;
     int stall = 0;  // consecutive accepted steps that gained less than 0.1%
     for (int i = gp.t(); i < n; i += gp.nt()) {
@@ -467,8 +495,13 @@ __device__ long long quench_grp(const Grp& gp, const Rep& R, int n, const Grid& 
             acc[i] = make_int4(0, 0, 0, 0);
             saved[i] = make_float4(R.sq[i].x, R.sq[i].y, R.ang[i], 0.f);
         }
+        if (gp.t() == 0) {
+            plist[0] = 0u;
+            plist[1] = 0u;
+        }
         gp.sync();
-        // work item w: square w / 9 against cell w % 9 of its block
+        // work item w: square w / 9 against cell w % 9 of its block; it also
+        // lists the block's pairs (i < j) closer than sqrt(kListCut2)
         for (int w = gp.t(); w < 9 * n; w += gp.nt()) {
             const int i = w / 9, c = w - 9 * i;
             const float4 P = R.sq[i];
@@ -488,7 +521,12 @@ __device__ long long quench_grp(const Grp& gp, const Rep& R, int n, const Grid& 
                     if (j == i) continue;
                     const float4 Q = R.sq[j];
                     const float ex = Q.x - P.x, ey = Q.y - P.y;
-                    if (ex * ex + ey * ey >= kPairCut2) continue;
+                    const float d2 = ex * ex + ey * ey;
+                    if (j > i && d2 < kListCut2) {
+                        const uint32_t slot = atomicAdd(&plist[0], 1u);
+                        if (slot < (uint32_t)pcap) plist[2 + slot] = (uint32_t)i | ((uint32_t)j << 16);
+                    }
+                    if (d2 >= kPairCut2) continue;
                     PairGrad pg;
                     if (sat_pair_grad(ex, ey, P.z, P.w, Q.z, Q.w, pg)) {
                         ax += qg(pg.px);
@@ -520,20 +558,29 @@ __device__ long long quench_grp(const Grp& gp, const Rep& R, int n, const Grid& 
         const float beta =
             (it == 0 || s_oo == 0 || it % 25 == 0) ? 0.f : fmaxf(0.f, (float)((double)s_dg / (double)s_oo));
         if (s_gg == 0 && beta == 0.f) break;  // no direction left at the sums' resolution
+        uint32_t dmax_bits = 0u;  // largest |d.x|, |d.y| (bits of non-negative floats order as integers)
         for (int i = gp.t(); i < n; i += gp.nt()) {
             const int4 a = acc[i];
             const float4 d0 = dir[i];
-            dir[i] = make_float4(__fmaf_rn(beta, d0.x, -(float)a.x * (1.0f / kQScale)),
-                                 __fmaf_rn(beta, d0.y, -(float)a.y * (1.0f / kQScale)),
-                                 __fmaf_rn(beta, d0.z, -(float)a.z * (1.0f / kQScale)), 0.f);
+            const float4 d1 = make_float4(__fmaf_rn(beta, d0.x, -(float)a.x * (1.0f / kQScale)),
+                                          __fmaf_rn(beta, d0.y, -(float)a.y * (1.0f / kQScale)),
+                                          __fmaf_rn(beta, d0.z, -(float)a.z * (1.0f / kQScale)), 0.f);
+            dir[i] = d1;
             gold[i] = a;
+            dmax_bits = max(dmax_bits, __float_as_uint(fmaxf(fabsf(d1.x), fabsf(d1.y))));
         }
+        dmax_bits = __reduce_max_sync(0xffffffffu, dmax_bits);
+        if ((threadIdx.x & 31) == 0) atomicMax(&plist[1], dmax_bits);
         gp.sync();
+        const int npairs = (int)plist[0];
+        const float dmax = __uint_as_float(plist[1]);
         // Trial steps move every coordinate by at most 0.1, so each partner
         // within the pair cut-off of a moved square still sits in one of the
         // 3 x 3 cells around it on the lists built for the saved state
         // (1.4142 + 0.1 < 1.59 <= cell side): trial energies use those lists,
-        // and the lists are rebuilt only for an accepted step.
+        // and the lists are rebuilt only for an accepted step.  A trial whose
+        // largest centre step is at most kListStep sums the pair list instead
+        // (the same energy, without the cell scan).
         float alpha = step;
         bool moved = false;
         for (int tries = 0; tries < 5 && !moved; ++tries) {
@@ -550,7 +597,8 @@ __device__ long long quench_grp(const Grp& gp, const Rep& R, int n, const Grid& 
                 R.ang[i] = a;
             }
             gp.sync();
-            const long long En = full_energy_grp(gp, R, n, g, L);
+            const bool by_list = npairs <= pcap && alpha * dmax <= kListStep;
+            const long long En = by_list ? list_energy(gp, R, n, L, plist + 2, npairs) : full_energy_grp(gp, R, n, g, L);
             if (En < E && build_cells_grp(gp, R, n, g)) {
                 stall = En > E - E / 1000 ? stall + 1 : 0;  // less than 0.1% gained
                 E = En;
