@@ -486,6 +486,7 @@ __device__ long long quench_grp(const Grp& gp, const Rep& R, int n, const Grid& 
     const int pcap = 8 * n - 2;
     float step = 0.04f;
     int stall = 0;  // consecutive accepted steps that gained less than 0.1%
+    float drift = 1e30f;  // bound on any centre's per-axis move since the pair list was built (none yet)
     for (int i = gp.t(); i < n; i += gp.nt()) {
         gold[i] = make_int4(0, 0, 0, 0);
         dir[i] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -495,14 +496,51 @@ __device__ long long quench_grp(const Grp& gp, const Rep& R, int n, const Grid& 
             acc[i] = make_int4(0, 0, 0, 0);
             saved[i] = make_float4(R.sq[i].x, R.sq[i].y, R.ang[i], 0.f);
         }
+        // the pair list stays exact while no centre has moved more than
+        // kListStep per axis since it was built; past that it is rebuilt
+        const bool rebuild = !(drift <= kListStep);
         if (gp.t() == 0) {
-            plist[0] = 0u;
+            if (rebuild) plist[0] = 0u;
             plist[1] = 0u;
         }
         gp.sync();
+        if (!rebuild) {
+            // gradient over the list: walls, then both sides of every pair
+            // within the cut-off (the cell scan's operations and sums)
+            for (int i = gp.t(); i < n; i += gp.nt()) {
+                const float4 P = R.sq[i];
+                float wx = 0.f, wy = 0.f, wa = 0.f;
+                wall_energy_grad(P.x, P.y, P.z, P.w, L, wx, wy, wa);
+                const int ax = qg(wx), ay = qg(wy), aa = qg(wa);
+                if (ax | ay | aa) {
+                    atomicAdd(&acc[i].x, ax);
+                    atomicAdd(&acc[i].y, ay);
+                    atomicAdd(&acc[i].z, aa);
+                }
+            }
+            const int np = (int)plist[0];
+            for (int k = gp.t(); k < np; k += gp.nt()) {
+                const uint32_t pr = plist[2 + k];
+                const int i = (int)(pr & 0xffffu), j = (int)(pr >> 16);
+                const float4 P = R.sq[i], Q = R.sq[j];
+                const float ex = Q.x - P.x, ey = Q.y - P.y;
+                if (ex * ex + ey * ey >= kPairCut2) continue;
+                PairGrad pg;
+                if (sat_pair_grad(ex, ey, P.z, P.w, Q.z, Q.w, pg)) {
+                    atomicAdd(&acc[i].x, qg(pg.px));
+                    atomicAdd(&acc[i].y, qg(pg.py));
+                    atomicAdd(&acc[i].z, qg(pg.pa));
+                }
+                if (sat_pair_grad(P.x - Q.x, P.y - Q.y, Q.z, Q.w, P.z, P.w, pg)) {
+                    atomicAdd(&acc[j].x, qg(pg.px));
+                    atomicAdd(&acc[j].y, qg(pg.py));
+                    atomicAdd(&acc[j].z, qg(pg.pa));
+                }
+            }
+        }
         // work item w: square w / 9 against cell w % 9 of its block; it also
         // lists the block's pairs (i < j) closer than sqrt(kListCut2)
-        for (int w = gp.t(); w < 9 * n; w += gp.nt()) {
+        for (int w = gp.t(); rebuild && w < 9 * n; w += gp.nt()) {
             const int i = w / 9, c = w - 9 * i;
             const float4 P = R.sq[i];
             int ax = 0, ay = 0, aa = 0;
@@ -542,6 +580,7 @@ __device__ long long quench_grp(const Grp& gp, const Rep& R, int n, const Grid& 
             }
         }
         gp.sync();
+        if (rebuild) drift = plist[0] <= (uint32_t)pcap ? 0.f : 1e30f;  // an overflowed list is not used
         // Polak-Ribiere: g_old.g_old, (g - g_old).g and g.g as exact integer
         // sums of components clamped to 2^24 (a gradient of 16; only beta
         // sees the clamp): 3 n <= 3000 terms below 2^49 each fit 64 bits
@@ -578,9 +617,10 @@ __device__ long long quench_grp(const Grp& gp, const Rep& R, int n, const Grid& 
         // within the pair cut-off of a moved square still sits in one of the
         // 3 x 3 cells around it on the lists built for the saved state
         // (1.4142 + 0.1 < 1.59 <= cell side): trial energies use those lists,
-        // and the lists are rebuilt only for an accepted step.  A trial whose
-        // largest centre step is at most kListStep sums the pair list instead
-        // (the same energy, without the cell scan).
+        // and the lists are rebuilt only for an accepted step.  A trial that
+        // keeps every centre within kListStep per axis of where the pair list
+        // was built sums the list instead (the same energy, without the cell
+        // scan).
         float alpha = step;
         bool moved = false;
         for (int tries = 0; tries < 5 && !moved; ++tries) {
@@ -597,12 +637,13 @@ __device__ long long quench_grp(const Grp& gp, const Rep& R, int n, const Grid& 
                 R.ang[i] = a;
             }
             gp.sync();
-            const bool by_list = npairs <= pcap && alpha * dmax <= kListStep;
+            const bool by_list = npairs <= pcap && drift + alpha * dmax <= kListStep;
             const long long En = by_list ? list_energy(gp, R, n, L, plist + 2, npairs) : full_energy_grp(gp, R, n, g, L);
             if (En < E && build_cells_grp(gp, R, n, g)) {
                 stall = En > E - E / 1000 ? stall + 1 : 0;  // less than 0.1% gained
                 E = En;
                 step = fminf(0.15f, alpha * 1.25f);
+                drift += fminf(0.1f, alpha * dmax);  // every centre moved at most this far per axis
                 moved = true;
             } else {
                 if (En < E) {  // the better state overflows a cell: lists back to the saved state
