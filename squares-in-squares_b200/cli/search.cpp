@@ -223,10 +223,10 @@ int main(int argc, char** argv) {
                 j.sweeps = (int)std::max<long long>(-2000000000LL, -std::max(1LL, proposals_per_chain));
                 j.exchange_every = -std::max(1, steps);
                 j.flags |= SQS_JOB_TARGETS | SQS_JOB_LADDERS(lad);
-                // without the tuner, the widest cluster (up to 16 CTAs): the
-                // checkpoint quenches a CTA's replicas one after another, so
-                // fewer replicas per CTA finish an epoch sooner, as the
-                // reference polishes its chains on separate blocks
+                // without the tuner, the widest cluster (up to 16 CTAs): fewer
+                // replicas per CTA leave each replica more warps for its
+                // checkpoint quench, as the reference polishes its chains on
+                // separate blocks
                 if (!autotune) j.flags |= SQS_JOB_CLUSTER(std::min(16, 8 * lad));
                 j.shrink = std::min(0.1 / 20.0, shrink / L);
             } else {
@@ -244,6 +244,16 @@ int main(int argc, char** argv) {
             j.xya_rep = starts.data() + 3 * (size_t)n * 8 * (size_t)k * (size_t)per_job;
             ptrs[(size_t)k] = outs[(size_t)k].data();
         }
+        // Untimed warm-up of one proposal a replica: the first call loads the
+        // kernels and allocates the device buffers, which the reference does
+        // before it starts its clock (its allocations, copies and first
+        // launches precede `start`, seeded.cu:887-906).
+        std::vector<sqs_job> warm = jobs;
+        for (sqs_job& w : warm) {
+            w.sweeps = targets ? -1 : 1;
+            w.exchange_every = targets ? -1 : 1;
+        }
+        (void)sqs_anneal_batch(ctx, warm.data(), njobs, 0, ptrs.data(), res.data());
         const auto t0 = std::chrono::steady_clock::now();
         const int rc = sqs_anneal_batch(ctx, jobs.data(), njobs, 0, ptrs.data(), res.data());
         seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
