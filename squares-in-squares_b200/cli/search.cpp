@@ -52,7 +52,9 @@
 // "target_L" is the FP64 dilation-certified side of the best state and "q"
 // that state (the packing the interval certifier accepted); when no ladder
 // finds a certified state the seed is reported with its side, as the
-// reference does.
+// reference does.  "seconds" times the search call after an untimed call of
+// one proposal a replica has loaded the kernels and allocated the buffers,
+// as the reference's clock starts after its own set-up.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
