@@ -191,10 +191,8 @@ typedef struct sqs_job {
  *              step size per replica scaled by its rung (0.15 .. 2 x sigma
  *              from the coldest to the hottest rung), by an adaptation factor
  *              that every 16 proposals moves toward 25% acceptance
- *              (x exp((rate - 0.25) / 2), kept in [0.1, 4]) and restarts at 1
- *              with every exchange interval, as the reference's restarts with
- *              every epoch, by 3.5 on every 16th proposal of an interval, and
- *              a cooling cycle of 200 exchange rounds that
+ *              (x exp((rate - 0.25) / 2), kept in [0.1, 4]), by 3.5 on every
+ *              16th proposal, and a cooling cycle of 200 exchange rounds that
  *              scales temperatures by 0.002^(k/199) and steps by its square
  *              root (seeded.cu:493-494, 506-507, 614-618);
  *  COLLECTIVE  6 proposals in 7 move a set of squares around the drawn one:

@@ -1040,7 +1040,6 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
     const int64_t p_end = min(P_total, p_at + (int64_t)(jd.slice > 0 ? jd.slice : slice_sweeps) * n);
     while (p_at < p_end) {
         const int64_t next_cp = min(P_total, (p_at / xp + 1) * xp);
-        const uint64_t cp0 = (uint64_t)((p_at / xp) * xp);  // first proposal of this checkpoint interval
         const int64_t stop = min(next_cp, p_end);
         if (active) {
             for (int64_t base = p_at; base < stop; base += 32) {
@@ -1104,7 +1103,7 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                     const uint64_t pidx = (uint64_t)(base + q);
                     if (adaptive) {
                         sc = step_scale(jd, adapt, S.jm.perm[r], cool);
-                        if (((pidx - cp0) & 15u) == 0) sc *= 3.5f;  // the interval's 16th proposals
+                        if ((pidx & 15u) == 0) sc *= 3.5f;
                     }
                     const float dx = fminf(kMaxStep, fmaxf(-kMaxStep, sdx * sc));
                     const float dy = fminf(kMaxStep, fmaxf(-kMaxStep, sdy * sc));
@@ -1151,7 +1150,7 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                     }
                     if (adaptive) {  // every 16 proposals: steer toward 25% acceptance
                         win += acc;
-                        if (((pidx - cp0 + 1u) & 15u) == 0) {
+                        if (((pidx + 1u) & 15u) == 0) {
                             adapt = fmaxf(0.1f, fminf(4.0f, adapt * expf(((float)win / 16.f - 0.25f) * 0.5f)));
                             win = 0;
                         }
@@ -1419,7 +1418,6 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
             cluster.sync();
         }
         const bool regrid = S.newL < L;
-        bool was_reset = false;  // this replica restarted from the new best
         if (regrid || targets) {
             const float f = S.newL / L;
             if (regrid) {
@@ -1431,7 +1429,6 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
                 const float Ln = rung_side(jd, L, rung);
                 const int RL = rungs_per_ladder(jd);
                 const bool reset = targets && S.decision_win >= 0 && (rung % RL == 0 || (S.reset0 && rung < RL));
-                was_reset = reset;
                 if (reset) {
                     // ladder head: the new best, scaled into its own side (seeded.cu:928-936)
                     const double* src = best + jd.best_off;
@@ -1479,18 +1476,9 @@ __global__ void __launch_bounds__(32 * kMaxRl) anneal_kernel(const int32_t* __re
             __syncthreads();
         }
         // overlapped replicas are kicked (the round just completed decides
-        // whether the worst square is also moved); a replica just restarted
-        // from the new best is not: the reference kicks its chains inside the
-        // epoch's kernel and restarts the ladder heads after it, on the host
-        // (seeded.cu:721-778, 926-936)
-        if (MOVES && active && (jd.flags & kMoveKick) && !was_reset && E > qe(1e-12f))
+        // whether the worst square is also moved)
+        if (MOVES && active && (jd.flags & kMoveKick) && E > qe(1e-12f))
             E = kick_replica(rep, g, n, Lr, lane, r, S.jm.xround, k0, k1, E, save);
-        // the step adaptation restarts with every interval, as the reference
-        // restarts it with every epoch (seeded.cu:477-478)
-        if (adaptive) {
-            adapt = 1.f;
-            win = 0;
-        }
     }
 
     // ---- write the slice back
